@@ -1,0 +1,355 @@
+"""Benchmark of the LD hot path (AND+popcount counts + fused r^2) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload single_region|all_pairs] [--kernel auto|popc|mma]
+
+Workload (default): the dataset-shaped single region -- 29,817 SNPs x 16,622
+haploid sequences (K = 260 words per SNP), allele frequencies Beta(0.1, 1)
+clipped to >= 1/16,622, haplotype-copying model (20 founders, recombination
+blocks of 50-500 SNPs, 1% per-site mutation), lower-triangular FP32 r^2.
+Seeded synthetic data of that shape stands in for the dataset.
+
+A step is one pass of the hot path over the region: counts + r^2 for all
+M(M-1)/2 SNP pairs (the kernel also fills the diagonal).  `value` is
+SNP-pairs/s with the packed table resident in HBM (device-to-device call,
+output to HBM), timed per step with CUDA events on the launching stream after
+an L2 flush (a 512 MB write); `e2e` is the same metric through the host-buffer
+C-ABI call (qld_cuda_ld): pinned host table -> device, counts + r^2, lower
+triangle -> pinned host memory, all inside the timed region.
+
+With --gpus N (torchrun) every rank processes its own region of the same shape
+(no data-path collective; weak scaling); timing is the max over ranks.
+`--impl reference` times the reference's CPU path (its bin_gemm_2x2
+micro-kernel in a BLIS-style loop plus its get_pairwise_ld_score, built from
+the qLD sources into oracle/_ref) with all host threads on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "r2 SNP-pairs/s (counts + fused r2 epilogue)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="single_region", choices=["single_region", "all_pairs"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(name):
+    if name == "single_region":
+        return dict(workload="single_region_29817x16622_lower_triangle", snps=29_817,
+                    haplotypes=16_622, words_per_snp=260, model="copying(20 founders)",
+                    freq="Beta(0.1,1) clipped >= 1/16622", output="fp32 lower triangle")
+    return dict(workload="all_pairs_2048x4096_symmetric", snps=2048, haplotypes=4096,
+                words_per_snp=64, model="iid Bernoulli", freq="Uniform(0.05,0.5)",
+                output="fp32 lower triangle")
+
+
+def make_table(name, device, seed_offset=0):
+    from qld_b200 import synth
+    if name == "single_region":
+        return synth.single_region_workload(device=device, seed=2 + seed_offset)
+    return synth.all_pairs_workload(device=device, seed=1 + seed_offset)
+
+
+# ------------------------------------------------------------------ clocks --
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------ reference CPU --
+
+def cpu_reference_rate(T_np, S, seconds_target=12.0, threads=None):
+    """Reference CPU path (bin_gemm_2x2 loop + get_pairwise_ld_score) on the
+    first Ms SNPs of the table, single region; Ms chosen so the timed sample
+    takes ~seconds_target.  Returns (pairs/s, cores, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import oracle
+    threads = threads or os.cpu_count()
+
+    def run(ms):
+        A = np.ascontiguousarray(T_np[:ms])
+        bc = oracle.bitcounts(A)
+        t0 = time.perf_counter()
+        C = oracle.ref_counts_ukr(A, None, lower_only=True, threads=threads)
+        oracle.ref_ld_score(bc, bc, C, S, threads=threads)
+        return time.perf_counter() - t0
+
+    m = T_np.shape[0]
+    ms = min(m, 1024)
+    t = run(ms)
+    while t < seconds_target / 8 and ms < m:
+        ms = min(m, ms * 2)
+        t = run(ms)
+    if t < seconds_target / 2 and ms < m:
+        ms = min(m, int(ms * (seconds_target / max(t, 1e-3)) ** 0.5))
+        t = run(ms)
+    pairs = ms * (ms - 1) / 2
+    return pairs / t, threads, f"first {ms} SNPs of the region, all {ms*(ms-1)//2} pairs, {t:.2f} s"
+
+
+def reference_arm(args, rank, world):
+    import numpy as np
+    cfg = workload_config(args.workload)
+    if rank != 0:
+        return
+    T, S = make_table(args.workload, "cpu")
+    T_np = T.numpy().view(np.uint64)
+    for _ in range(args.warmup):
+        cpu_reference_rate(T_np, S, seconds_target=2.0)
+    vals = []
+    desc = ""
+    cores = os.cpu_count()
+    for _ in range(args.steps):
+        v, cores, desc = cpu_reference_rate(T_np, S, seconds_target=6.0)
+        vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64 popcount / f32 r2", "data": "synthetic",
+            "config": cfg,
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "reference",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------------- ours --
+
+def lower_tri_d2h_bytes(m, tile=128):
+    total = 0
+    for r0 in range(0, m, tile):
+        rows = min(tile, m - r0)
+        total += rows * (m - r0) * 4
+    return total
+
+
+def ours_arm(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from qld_b200 import api, synth
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    cfg = workload_config(args.workload)
+    cfg["parallelism"] = f"replicas x{world} (independent regions, no collective)"
+    cfg["l2"] = "512 MB flush write between timed steps"
+
+    T, S = make_table(args.workload, dev, seed_offset=rank)
+    m, K = T.shape
+    lda = K + (K & 1)
+    Tp = torch.zeros(m, lda, dtype=torch.int64, device=dev)
+    Tp[:, :K] = T
+    bc = synth.popcount_rows(T).to(torch.int32)
+    out = torch.empty(m, m, dtype=torch.float32, device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+
+    ctx = api.Context(local_rank)
+    kern = {"auto": api.KERNEL_AUTO, "popc": api.KERNEL_POPC, "mma": api.KERNEL_MMA}[args.kernel]
+    ctx.set_option(api.OPT_KERNEL, kern)
+    ctx.set_option(api.OPT_PROFILE, 1)
+    st = torch.cuda.current_stream()
+
+    def step():
+        ctx.ld_device(Tp, bc, m, lda, Tp, bc, m, lda, K, S, True, out, m, stream=st)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    ctx.sync(stream=st)
+    ctx.stats(reset=True)
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(st)
+            step()
+            ev[i][1].record(st)
+        ctx.sync(stream=st)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    stats = ctx.stats(reset=True)
+    clocks = clk.summary()
+
+    pairs = m * (m - 1) / 2
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms_max = float(t.item())
+    value = pairs * args.steps * world / (total_ms_max * 1e-3)
+
+    # roofline of the counts kernel
+    kern_ms = stats.counts_kernel_ms / max(1, stats.counts_launches)
+    bitops = pairs * 64 * K
+    variant = stats.last_kernel
+    popc_peak = ctx.measure_popc_peak()
+    if variant == api.KERNEL_MMA:
+        a = torch.randint(-2, 2, (8192, 8192), dtype=torch.int8, device=dev)
+        b = torch.randint(-2, 2, (8192, 8192), dtype=torch.int8, device=dev).t()
+        for _ in range(3):
+            torch._int_mm(a, b)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            torch._int_mm(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        i8_tops = 2 * 8192 ** 3 * 10 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+        achieved = 2 * bitops / (kern_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": i8_tops, "unit": "TOPS (int8)",
+                "frac": achieved / i8_tops, "peak_source": "measured: torch._int_mm int8 8192^3"}
+    else:
+        achieved = bitops / (kern_ms * 1e-3) / 1e12
+        roof = {"bound": "popc", "achieved": achieved, "peak": popc_peak / 1e12,
+                "unit": "Tbit-op/s", "frac": achieved / (popc_peak / 1e12),
+                "peak_source": "measured: qld_cuda_measure_popc_peak (register-only AND+POPC)"}
+    alg_bytes = m * K * 8 * 2 + pairs * 4
+    roof["traffic"] = None
+    roof["algorithmic_bytes_per_launch"] = alg_bytes
+    roof["kernel_ms"] = kern_ms
+    roof["hbm_frac_of_measured"] = (alg_bytes / (kern_ms * 1e-3) / 1e9) / 6538.9
+
+    line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64 popcount / f32 r2", "data": "synthetic", "config": cfg,
+            "bitops_per_s": bitops * args.steps * world / (total_ms_max * 1e-3),
+            "gpu_launches": stats.kernel_launches, "kernel_variant": variant,
+            "roofline": roof, "clocks": clocks}
+
+    # ---- e2e through the host-buffer C-ABI call
+    if not args.no_e2e:
+        Th = ctx.pinned_empty((m, K), np.uint64)
+        Th[:] = T.cpu().numpy().view(np.uint64)
+        bch = ctx.pinned_empty((m,), np.uint32)
+        bch[:] = bc.cpu().numpy().view(np.uint32)
+        outh = ctx.pinned_empty((m, m), np.float32)
+        for _ in range(max(1, args.warmup)):
+            ctx.ld(Th, bch, S=S, r2_out=outh)
+        if world > 1:
+            dist.barrier()
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            ctx.ld(Th, bch, S=S, r2_out=outh)
+            ts.append(time.perf_counter() - t0)
+        tt = torch.tensor([sum(ts)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        line["e2e"] = {"value": pairs * args.steps * world / float(tt.item()), "unit": "pairs/s",
+                       "h2d_bytes_per_step": m * K * 8 + m * 4,
+                       "d2h_bytes_per_step": lower_tri_d2h_bytes(m),
+                       "api": "qld_cuda_ld (pinned host buffers)"}
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, desc = cpu_reference_rate(T.cpu().numpy().view(np.uint64), S)
+        line["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": cores, "kind": "reference",
+                                "sample": desc}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        ours_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

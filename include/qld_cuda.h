@@ -1,0 +1,148 @@
+/*
+ * qld_cuda.h -- C ABI of libqld_cuda, the sm_100a (B200) LD hot path of
+ * qLD-compute: pairwise AND+popcount counts over packed 64-bit MDF rows and
+ * the fused r^2 epilogue.
+ *
+ * Plain C types only (no CUDA or torch types): a C caller such as
+ * qLD-compute's per-task driver links it directly; other hosts bind it
+ * through their FFI.  Every function returns QLD_OK (0) or a negative
+ * QLD_ERR_* code and never exits the process; qld_cuda_last_error() gives the
+ * message of the last failure on a context.
+ *
+ * Data layout (as qLD's table_x64, src/correlator/include/correlate_MEM.h:66-75):
+ *   A, B     row-major SNP tables, K uint64 words per row, MSB-first packing
+ *            (sample s is bit 63 - s%64 of word s/64), zero tail bits.
+ *   bcA, bcB per-row popcounts (the MDF BC field, BCtable).
+ *   r2_out   n x m float, B-major: r2_out[i*m + j] is the r^2 of B row i and
+ *            A row j -- the reference's results[] (gemm_cpu.c:357-388).
+ *   counts   n x m uint32 with the same indexing, i.e. the reference's
+ *            column-major m x n C matrix (gemm_cpu.c:203-236) narrowed to 32 bit.
+ *   symmetric  single-region task (the reference's posWset2 == 0): B is A and
+ *            only entries with j >= i (A index >= B index: the lower triangle of
+ *            C including its diagonal, what cblas_dsyrk(CblasLower) fills) are
+ *            defined on return; the entries with j < i are unspecified (the
+ *            reference leaves values there that its writer never reads).
+ *
+ * r^2 modes (per entry, cA = bcA[j], cB = bcB[i], c = count, S = snp_size):
+ *   QLD_R2_EXACT      r^2 = D^2 / (cA(S-cA) cB(S-cB)) with the exact integer
+ *                     D = S*c - cA*cB, evaluated in FP64 and rounded once to
+ *                     FP32 (relative error <= 2^-24 against an FP64 oracle).
+ *   QLD_R2_REFERENCE  bit-identical to get_pairwise_ld_score()
+ *                     (gemm_cpu.c:343-404): FP32 frequencies, FP32 numerator,
+ *                     FP64 denominator, no fused multiply-add.
+ *   Both: r^2 = 0 when cA == 0 or cB == 0; r^2 > 1.0001 becomes 123.456;
+ *   0/0 (an all-ones SNP) stays NaN.
+ */
+#ifndef QLD_CUDA_H
+#define QLD_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QLD_CUDA_ABI_VERSION 1
+
+/* status codes */
+#define QLD_OK               0
+#define QLD_ERR_INVALID     -1  /* bad argument                                  */
+#define QLD_ERR_CUDA        -2  /* a CUDA runtime/driver call failed             */
+#define QLD_ERR_NOMEM       -3  /* device or pinned host allocation failed       */
+#define QLD_ERR_NODEVICE    -4  /* no usable sm_100 device                       */
+#define QLD_ERR_TIMEOUT     -5  /* a kernel's bounded wait gave up               */
+#define QLD_ERR_BUSY        -6  /* admission refused (serving)                   */
+#define QLD_ERR_UNSUPPORTED -7  /* shape/option not supported by this kernel     */
+
+/* r^2 evaluation modes */
+#define QLD_R2_EXACT      0
+#define QLD_R2_REFERENCE  1
+
+/* counts-kernel variants */
+#define QLD_KERNEL_AUTO   0  /* per-shape choice                                 */
+#define QLD_KERNEL_POPC   1  /* LOP3 + POPC on the CUDA cores                     */
+#define QLD_KERNEL_MMA    2  /* bit -> int8 unpack + tcgen05 i8 MMA (TMEM)        */
+
+/* qld_cuda_set_option() keys */
+#define QLD_OPT_KERNEL    1  /* QLD_KERNEL_*                                      */
+#define QLD_OPT_R2_MODE   2  /* QLD_R2_*                                          */
+#define QLD_OPT_PROFILE   3  /* 1: time every counts-kernel launch with events    */
+#define QLD_OPT_BAND_ROWS 4  /* B rows per streamed output band (host-buffer calls) */
+
+typedef struct qld_ctx qld_ctx;
+
+/*
+ * Context lifecycle.  Replaces gpu_init()/gpu_release() (qLD
+ * src/correlator/include/gemm_gpu.h:52-54, called from
+ * correlate_our_kernel.c:593-596,626-629).  One context per host thread;
+ * a context is not re-entrant.
+ */
+int qld_cuda_init(int device, qld_ctx **ctx_out);
+int qld_cuda_release(qld_ctx *ctx);
+const char *qld_cuda_last_error(const qld_ctx *ctx);
+int qld_cuda_set_option(qld_ctx *ctx, int option, long long value);
+
+/*
+ * One LD task from host memory: the counts + r^2 part of correlate()
+ * (gemm_cpu.c:420-623: blis_gemm()/gemm() at :517-547 and
+ * get_pairwise_ld_score() at :557-563), with qLD-compute's argument meaning:
+ * m = tableAsize, n = tableBsize, K = compressed_snp_size, S = snp_size,
+ * symmetric = (posWset2 == 0).  B/bcB are ignored when symmetric (n must
+ * equal m).  counts_out may be NULL.  Host buffers may be pageable or pinned
+ * (qld_cuda_host_alloc); pinned ones let the copies overlap the kernels.
+ * Synchronous: returns when r2_out (and counts_out) hold the results.
+ */
+int qld_cuda_ld(qld_ctx *ctx,
+                const uint64_t *A, const uint32_t *bcA, int m,
+                const uint64_t *B, const uint32_t *bcB, int n,
+                int K, int S, int symmetric,
+                float *r2_out, uint32_t *counts_out);
+
+/*
+ * The same task on device-resident buffers, enqueued on `stream`
+ * (a cudaStream_t; NULL = the context's stream), asynchronous.
+ *   lda/ldb   words between consecutive rows in device memory (>= K, even;
+ *             row starts 16-byte aligned).  Words past K are never read.
+ *   ldr/ldc   elements between consecutive B rows of r2 / counts (>= m).
+ * Call qld_cuda_sync() to wait and collect the kernel status.
+ */
+typedef struct qld_ld_args {
+    const uint64_t *A; const uint32_t *bcA; int m; long long lda;
+    const uint64_t *B; const uint32_t *bcB; int n; long long ldb;
+    int K; int S; int symmetric;
+    float *r2; long long ldr;
+    uint32_t *counts; long long ldc;
+} qld_ld_args;
+
+int qld_cuda_ld_device(qld_ctx *ctx, const qld_ld_args *args, void *stream);
+int qld_cuda_sync(qld_ctx *ctx, void *stream);
+
+/* Pinned host memory for tables and results (the -cuda reader allocates its
+ * tables here so the host<->device copies run asynchronously). */
+int qld_cuda_host_alloc(qld_ctx *ctx, size_t bytes, void **ptr);
+int qld_cuda_host_free(qld_ctx *ctx, void *ptr);
+
+/* Counters since the last reset: counts-kernel launches, all launches of
+ * this library's kernels, and (with QLD_OPT_PROFILE) the summed event time
+ * of the counts-kernel launches in milliseconds. */
+typedef struct qld_stats {
+    long long counts_launches;
+    long long kernel_launches;
+    double counts_kernel_ms;
+    int last_kernel;           /* QLD_KERNEL_* used by the last call */
+} qld_stats;
+
+int qld_cuda_get_stats(qld_ctx *ctx, qld_stats *out, int reset);
+
+/* Measured peak of the popcount pipe on this device, in bit-ops/s (one POPC
+ * of an ANDed 32-bit word = 32 bit-ops): the compute roofline of the
+ * QLD_KERNEL_POPC variant.  Runs a register-only kernel for ~0.1 s.
+ * No counterpart in the reference (its roofline is not measured). */
+int qld_cuda_measure_popc_peak(qld_ctx *ctx, double *bitops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QLD_CUDA_H */

@@ -1,0 +1,266 @@
+/*
+ * qld_oracle.c -- CPU restatement of qLD-compute's LD hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA path is
+ * compared against; nothing in the shipped library links, loads or calls it.
+ * Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use it.
+ *
+ * What is restated (reference file:line, paths inside the qLD project):
+ *   qo_counts          <- blis_gemm() / gemm() + bin_gemm_2x2()
+ *                         src/correlator/src/gemm_cpu.c:125-341,
+ *                         blis/config/binary_gemm/kernels/3/bin_gemm.c:4-141
+ *                         C[a + b*m] = sum_k popcount(A[a*K+k] & B[b*K+k]),
+ *                         column-major m x n; the single-region (SYRK, CblasLower)
+ *                         form fills only a >= b and leaves the rest 0
+ *                         (gemm_cpu.c:226-236 and the zeroing at :479-483).
+ *   qo_r2_reference    <- get_pairwise_ld_score()  gemm_cpu.c:343-404, with the
+ *                         same float/double mix, written out operation by
+ *                         operation so the rounding is explicit.
+ *   qo_r2_exact        FP64 oracle: r2 = D^2 / (cA(S-cA) cB(S-cB)) with the exact
+ *                         integer D = S*cAB - cA*cB, and the reference's special
+ *                         cases (zero popcount -> 0, > 1.0001 -> 123.456).
+ *   qo_write_results   <- writeResultsHeader()/writeResults() correlate_IO.c:378-429
+ *   qo_fprint_f        <- fprint_f()/reverse()  fast_print.c:21-103
+ *
+ * Build with -ffp-contract=off: every fused multiply-add below is written as
+ * an explicit fmaf() so the rounding never depends on compiler flags.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define QO_EXPORT __attribute__((visibility("default")))
+
+/* ---------------------------------------------------------------- counts -- */
+
+QO_EXPORT void qo_counts(const uint64_t *A, int m, const uint64_t *B, int n,
+                         int K, int lower_only, uint32_t *C)
+{
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int b = 0; b < n; b++) {
+        const uint64_t *rb = B + (size_t)b * K;
+        for (int a = 0; a < m; a++) {
+            uint32_t c = 0;
+            if (!lower_only || a >= b) {
+                const uint64_t *ra = A + (size_t)a * K;
+                for (int k = 0; k < K; k++)
+                    c += (uint32_t)__builtin_popcountll(ra[k] & rb[k]);
+            }
+            C[(size_t)a + (size_t)b * m] = c;
+        }
+    }
+}
+
+/* Row popcounts: the MDF "BC" field / BCtable (snip_processing.c:805). */
+QO_EXPORT void qo_bitcounts(const uint64_t *A, int m, int K, uint32_t *bc)
+{
+    for (int a = 0; a < m; a++) {
+        uint32_t c = 0;
+        for (int k = 0; k < K; k++)
+            c += (uint32_t)__builtin_popcountll(A[(size_t)a * K + k]);
+        bc[a] = c;
+    }
+}
+
+/* ------------------------------------------------------------ r2 epilogue -- */
+
+/*
+ * get_pairwise_ld_score (gemm_cpu.c:343-404), entry (i over B, j over A):
+ *   val_1 = (float)bcA[j] / S; val_2 = (float)bcB[i] / S; val_3 = (float)C / S
+ *   r  = (val_3 - val_1*val_2)^2                        (float)
+ *   r /= (val_1*val_2*(1.0-val_1)*(1.0-val_2))           (double denominator)
+ *   r > 1.0001 -> 123.456
+ * `fma_contract` selects whether val_3 - val_1*val_2 is one fused operation
+ * (what gcc emits for the reference's -O3 -march=native build on FMA hosts)
+ * or a rounded product followed by a rounded subtraction.
+ */
+static inline float ref_entry(uint32_t cA, uint32_t cB, uint32_t cAB, int S,
+                              int fma_contract)
+{
+    if (cB == 0 || cA == 0)
+        return 0.0f;
+    float fs = (float)S;
+    float v1 = (float)cA / fs;
+    float v2 = (float)cB / fs;
+    float v3 = (float)cAB / fs;
+    float d;
+    if (fma_contract) {
+        d = fmaf(-v1, v2, v3);
+    } else {
+        volatile float p = v1 * v2;
+        d = v3 - p;
+    }
+    float r = d * d;
+    float p12 = v1 * v2;
+    double den = (double)p12 * (1.0 - (double)v1);
+    den = den * (1.0 - (double)v2);
+    r = (float)((double)r / den);
+    if ((double)r > 1.0001)
+        r = 123.456f;
+    return r;
+}
+
+/* out[i*m + j] for i < n (B rows), j < m (A rows); C column-major m x n. */
+QO_EXPORT void qo_r2_reference(const uint32_t *bcA, int m, const uint32_t *bcB,
+                               int n, const uint32_t *C, int S,
+                               int fma_contract, float *out)
+{
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < m; j++)
+            out[(size_t)i * m + j] =
+                ref_entry(bcA[j], bcB[i], C[(size_t)j + (size_t)i * m], S,
+                          fma_contract);
+}
+
+static inline double exact_entry(uint32_t cA, uint32_t cB, uint32_t cAB, int S)
+{
+    if (cB == 0 || cA == 0)
+        return 0.0;
+    long long D = (long long)S * cAB - (long long)cA * cB;
+    long long vA = (long long)cA * ((long long)S - cA);
+    long long vB = (long long)cB * ((long long)S - cB);
+    long double num = (long double)D * (long double)D;
+    long double den = (long double)vA * (long double)vB;
+    double r = (double)(num / den);
+    if (r > 1.0001)
+        r = 123.456;
+    return r;
+}
+
+/* FP64 oracle; out64 and/or out32 (its float rounding) may be NULL. */
+QO_EXPORT void qo_r2_exact(const uint32_t *bcA, int m, const uint32_t *bcB,
+                           int n, const uint32_t *C, int S, double *out64,
+                           float *out32)
+{
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < m; j++) {
+            double r = exact_entry(bcA[j], bcB[i], C[(size_t)j + (size_t)i * m], S);
+            if (out64)
+                out64[(size_t)i * m + j] = r;
+            if (out32)
+                out32[(size_t)i * m + j] = (r == 123.456) ? 123.456f : (float)r;
+        }
+}
+
+/* ------------------------------------------------------------ text report -- */
+
+typedef struct {
+    char *buf;
+    size_t len, cap;
+} qo_sink;
+
+static void sink_putc(qo_sink *s, char c)
+{
+    if (s->len < s->cap)
+        s->buf[s->len] = c;
+    s->len++;
+}
+
+static void sink_puts(qo_sink *s, const char *str)
+{
+    while (*str)
+        sink_putc(s, *str++);
+}
+
+/* reverse() of fast_print.c:21-33: reverses the decimal digits of a positive
+ * value in place and returns their count; a value <= 0 becomes 0. */
+static unsigned rev_digits(long *num)
+{
+    unsigned digits = 0;
+    long rev = 0;
+    while (*num > 0) {
+        digits++;
+        rev = rev * 10 + (*num) % 10;
+        *num /= 10;
+    }
+    *num = rev;
+    return digits;
+}
+
+/* fprint_f (fast_print.c:35-103): the scaled value is formed in float and
+ * truncated, never rounded; a zero fraction prints as "<int>." */
+static void fmt_f(qo_sink *s, float val, int precision)
+{
+    unsigned long power10 = 1;
+    for (int j = 0; j < precision; j++)
+        power10 *= 10;
+    long scaled = (long)(val * (float)power10);
+    long ipart = (long)val;
+    scaled = (long)((unsigned long)scaled - (unsigned long)ipart * power10);
+    unsigned i_digits = rev_digits(&ipart);
+    unsigned d_digits = rev_digits(&scaled);
+    if (ipart == 0) {
+        sink_putc(s, '0');
+    } else {
+        unsigned printed = 0;
+        while (ipart != 0) {
+            sink_putc(s, (char)('0' + ipart % 10));
+            ipart /= 10;
+            printed++;
+        }
+        for (unsigned j = 0; j < i_digits - printed; j++)
+            sink_putc(s, '0');
+    }
+    sink_putc(s, '.');
+    if (scaled == 0)
+        return;
+    for (unsigned j = 0; j < (unsigned)precision - d_digits; j++)
+        sink_putc(s, '0');
+    for (unsigned j = 0; j < d_digits; j++) {
+        sink_putc(s, (char)('0' + scaled % 10));
+        scaled /= 10;
+    }
+}
+
+QO_EXPORT size_t qo_fprint_f(char *buf, size_t cap, float val, int precision)
+{
+    qo_sink s = {buf, 0, cap};
+    fmt_f(&s, val, precision);
+    return s.len;
+}
+
+/*
+ * Report body of writeResults (correlate_IO.c:384-429), preceded by the
+ * header line of writeResultsHeader (:378-381) when with_header != 0.
+ * Returns the number of bytes the report needs; writes at most cap bytes.
+ */
+QO_EXPORT size_t qo_write_results(char *buf, size_t cap, int with_header,
+                                  const uint32_t *posA, const char *const *idA,
+                                  const uint32_t *bcA, int m,
+                                  const uint32_t *posB, const char *const *idB,
+                                  const uint32_t *bcB, int n, int S,
+                                  const float *results, float r2limit,
+                                  int posWset2)
+{
+    qo_sink s = {buf, 0, cap};
+    char num[32];
+    if (with_header)
+        sink_puts(&s, "POS2\tPOS1\tID2\tID1\tfreq[2]\tfreq[1]\tLD\n");
+    int cnt = 0;
+    for (int i = 0; i < n; i++) {
+        if (posWset2 == 0)
+            cnt++;
+        for (int j = cnt; j < m; j++) {
+            float v = results[(size_t)i * m + j];
+            if (v >= r2limit && v < 100) {
+                snprintf(num, sizeof num, "%u\t%u\t", posB[i], posA[j]);
+                sink_puts(&s, num);
+                sink_puts(&s, idB[i]);
+                sink_putc(&s, '\t');
+                sink_puts(&s, idA[j]);
+                sink_putc(&s, '\t');
+                fmt_f(&s, 1.0f * (float)bcB[i] / (float)S, 9);
+                sink_putc(&s, '\t');
+                fmt_f(&s, 1.0f * (float)bcA[j] / (float)S, 9);
+                sink_putc(&s, '\t');
+                fmt_f(&s, v, 9);
+                sink_putc(&s, '\n');
+            }
+        }
+    }
+    return s.len;
+}

@@ -1,0 +1,222 @@
+"""Python binding of libqld_cuda's C ABI (include/qld_cuda.h).
+
+This is the host-side mirror of qLD-compute's compute entry point for the
+tests and the benchmark: ``Context.ld`` takes the same arguments as the
+reference's ``correlate()`` compute part (src/correlator/include/gemm_cpu.h:24-38:
+table A + bit counts + size, table B + bit counts + size, compressed snip size
+K, snip size S, posWset2) and returns its ``results`` array.  Errors surface as
+``QldError`` carrying the library's status code and message -- the library
+never exits the process.
+
+The library must be built (``python -m qld_b200.build``); there is no fallback
+path: loading fails loudly when the CUDA library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libqld_cuda.so")
+
+OK = 0
+ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NODEVICE, ERR_TIMEOUT, ERR_BUSY, ERR_UNSUPPORTED = (
+    -1, -2, -3, -4, -5, -6, -7)
+R2_EXACT, R2_REFERENCE = 0, 1
+KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA = 0, 1, 2
+OPT_KERNEL, OPT_R2_MODE, OPT_PROFILE, OPT_BAND_ROWS = 1, 2, 3, 4
+
+EXPORTED = (
+    "qld_cuda_init", "qld_cuda_release", "qld_cuda_last_error", "qld_cuda_set_option",
+    "qld_cuda_ld", "qld_cuda_ld_device", "qld_cuda_sync", "qld_cuda_host_alloc",
+    "qld_cuda_host_free", "qld_cuda_get_stats", "qld_cuda_measure_popc_peak",
+)
+
+
+class QldError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class _LdArgs(ct.Structure):
+    _fields_ = [
+        ("A", ct.c_void_p), ("bcA", ct.c_void_p), ("m", ct.c_int), ("lda", ct.c_longlong),
+        ("B", ct.c_void_p), ("bcB", ct.c_void_p), ("n", ct.c_int), ("ldb", ct.c_longlong),
+        ("K", ct.c_int), ("S", ct.c_int), ("symmetric", ct.c_int),
+        ("r2", ct.c_void_p), ("ldr", ct.c_longlong),
+        ("counts", ct.c_void_p), ("ldc", ct.c_longlong),
+    ]
+
+
+class _Stats(ct.Structure):
+    _fields_ = [("counts_launches", ct.c_longlong), ("kernel_launches", ct.c_longlong),
+                ("counts_kernel_ms", ct.c_double), ("last_kernel", ct.c_int)]
+
+
+@dataclass
+class Stats:
+    counts_launches: int
+    kernel_launches: int
+    counts_kernel_ms: float
+    last_kernel: int
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ct.CDLL:
+    """Load libqld_cuda.so (raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built; run `python -m qld_b200.build`")
+    lib = ct.CDLL(path)
+    vp, i, ll = ct.c_void_p, ct.c_int, ct.c_longlong
+    lib.qld_cuda_init.argtypes = [i, ct.POINTER(vp)]
+    lib.qld_cuda_release.argtypes = [vp]
+    lib.qld_cuda_last_error.argtypes = [vp]
+    lib.qld_cuda_last_error.restype = ct.c_char_p
+    lib.qld_cuda_set_option.argtypes = [vp, i, ll]
+    lib.qld_cuda_ld.argtypes = [vp, vp, vp, i, vp, vp, i, i, i, i, vp, vp]
+    lib.qld_cuda_ld_device.argtypes = [vp, ct.POINTER(_LdArgs), vp]
+    lib.qld_cuda_sync.argtypes = [vp, vp]
+    lib.qld_cuda_host_alloc.argtypes = [vp, ct.c_size_t, ct.POINTER(vp)]
+    lib.qld_cuda_host_free.argtypes = [vp, vp]
+    lib.qld_cuda_get_stats.argtypes = [vp, ct.POINTER(_Stats), i]
+    lib.qld_cuda_measure_popc_peak.argtypes = [vp, ct.POINTER(ct.c_double)]
+    _lib = lib
+    return lib
+
+
+def _ptr(a) -> int | None:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor
+
+
+class Context:
+    """One libqld_cuda context (one per host thread), bound to a device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = ct.c_void_p()
+        rc = self.lib.qld_cuda_init(int(device), ct.byref(h))
+        if rc != OK:
+            raise QldError(rc, f"qld_cuda_init(device={device}) failed")
+        self.h = h
+        self.device = device
+        self._pinned: dict[int, int] = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            for p in list(self._pinned):
+                self.lib.qld_cuda_host_free(self.h, ct.c_void_p(p))
+            self._pinned.clear()
+            self.lib.qld_cuda_release(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != OK:
+            raise QldError(rc, self.lib.qld_cuda_last_error(self.h).decode(errors="replace"))
+
+    def set_option(self, option: int, value: int):
+        self._check(self.lib.qld_cuda_set_option(self.h, option, int(value)))
+
+    def stats(self, reset: bool = False) -> Stats:
+        s = _Stats()
+        self._check(self.lib.qld_cuda_get_stats(self.h, ct.byref(s), int(reset)))
+        return Stats(s.counts_launches, s.kernel_launches, s.counts_kernel_ms, s.last_kernel)
+
+    def measure_popc_peak(self) -> float:
+        """Measured popcount-pipe peak in bit-ops/s."""
+        v = ct.c_double()
+        self._check(self.lib.qld_cuda_measure_popc_peak(self.h, ct.byref(v)))
+        return v.value
+
+    # -------------------------------------------------------------- host --
+    def pinned_empty(self, shape, dtype) -> np.ndarray:
+        """numpy array in pinned host memory owned by this context."""
+        dtype = np.dtype(dtype)
+        nbytes = int(np.prod(shape)) * dtype.itemsize
+        p = ct.c_void_p()
+        self._check(self.lib.qld_cuda_host_alloc(self.h, max(nbytes, 1), ct.byref(p)))
+        self._pinned[p.value] = nbytes
+        buf = (ct.c_byte * max(nbytes, 1)).from_address(p.value)
+        return np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+    def ld(self, A, bcA, B=None, bcB=None, *, S: int, symmetric: bool | None = None,
+           r2_out=None, counts: bool | np.ndarray = False):
+        """One LD task from host arrays; returns r2 (n, m) [and counts (n, m)].
+
+        A, B: (rows, K) uint64 (or int64 bit patterns); bcA, bcB: uint32.
+        symmetric defaults to B is None (single region).
+        """
+        if symmetric is None:
+            symmetric = B is None
+        A = np.ascontiguousarray(A).view(np.uint64) if A.dtype != np.uint64 else np.ascontiguousarray(A)
+        bcA = np.ascontiguousarray(bcA, dtype=np.uint32)
+        m, K = A.shape
+        if symmetric:
+            B, bcB, n = A, bcA, m
+        else:
+            B = np.ascontiguousarray(B).view(np.uint64) if B.dtype != np.uint64 else np.ascontiguousarray(B)
+            bcB = np.ascontiguousarray(bcB, dtype=np.uint32)
+            n = B.shape[0]
+            if B.shape[1] != K:
+                raise ValueError("A and B must have the same number of words per row")
+        if r2_out is None:
+            r2_out = np.empty((n, m), np.float32)
+        cnt = None
+        if isinstance(counts, np.ndarray):
+            cnt = counts
+        elif counts:
+            cnt = np.empty((n, m), np.uint32)
+        self._check(self.lib.qld_cuda_ld(self.h, _ptr(A), _ptr(bcA), m, _ptr(B), _ptr(bcB), n,
+                                         K, int(S), int(bool(symmetric)), _ptr(r2_out), _ptr(cnt)))
+        return (r2_out, cnt) if cnt is not None else r2_out
+
+    # ------------------------------------------------------------ device --
+    def ld_device(self, A, bcA, m, lda, B, bcB, n, ldb, K, S, symmetric, r2, ldr,
+                  counts=None, ldc=0, stream=None):
+        """Enqueue one task on device buffers (torch tensors or raw pointers)."""
+        a = _LdArgs(_p(A), _p(bcA), int(m), int(lda), _p(B), _p(bcB), int(n), int(ldb), int(K),
+                    int(S), int(bool(symmetric)), _p(r2), int(ldr), _p(counts), int(ldc))
+        self._check(self.lib.qld_cuda_ld_device(self.h, ct.byref(a), _stream(stream)))
+
+    def sync(self, stream=None):
+        self._check(self.lib.qld_cuda_sync(self.h, _stream(stream)))
+
+
+def _p(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return _ptr(x)
+
+
+def _stream(s):
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return s
+    return s.cuda_stream  # torch.cuda.Stream

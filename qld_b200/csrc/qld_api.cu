@@ -1,0 +1,439 @@
+// qld_api.cu -- the C ABI of libqld_cuda (declared in include/qld_cuda.h).
+//
+// Host-buffer calls (qld_cuda_ld) stage the packed tables into device memory
+// with one pitched copy each (the device pitch is K rounded up to an even
+// word count so every row starts 16-byte aligned for TMA), then walk the B
+// rows in bands: band t's kernel writes its r^2 rows into one of two device
+// band buffers while the copy stream moves band t-1's rows to the caller's
+// buffer, so the device->host stream overlaps the counts kernels.
+#include <cudaTypedefs.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <utility>
+#include <vector>
+
+#include "qld_cuda.h"
+#include "qld_kernels.h"
+
+using namespace qld;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct qld_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;   // kernels and host->device copies
+    cudaStream_t copy = nullptr;     // device->host result copies
+    unsigned *d_status = nullptr;
+    unsigned *h_status = nullptr;    // pinned mirror of d_status
+    char err[512] = {0};
+    int kernel = QLD_KERNEL_AUTO;
+    int r2_mode = QLD_R2_EXACT;
+    int profile = 0;
+    int band_rows = 4096;
+    long long timeout_cycles = 4000000000LL;  // ~2 s at boost clock
+    DevBuf dA, dB, dbcA, dbcB, dOut[2], dCnt[2];
+    cudaEvent_t ev_band[2] = {nullptr, nullptr};
+    cudaEvent_t ev_copy[2] = {nullptr, nullptr};
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
+    size_t prof_used = 0;
+    qld_stats stats{};
+    PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+};
+
+namespace {
+
+int set_err(qld_ctx *c, int code, const char *fmt, ...) {
+    if (c) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(c->err, sizeof c->err, fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+#define CUDA_TRY(ctx, expr)                                                              \
+    do {                                                                                 \
+        cudaError_t e_ = (expr);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return set_err((ctx), QLD_ERR_CUDA, "%s failed: %s", #expr,                  \
+                           cudaGetErrorString(e_));                                      \
+    } while (0)
+
+int ensure(qld_ctx *c, DevBuf &b, size_t bytes) {
+    if (bytes <= b.bytes) return QLD_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    size_t want = bytes + bytes / 8;  // headroom so nearby sizes reuse the buffer
+    if (cudaMalloc(&b.p, want) != cudaSuccess) {
+        cudaGetLastError();
+        if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            return set_err(c, QLD_ERR_NOMEM, "cudaMalloc(%zu) failed", bytes);
+        }
+        want = bytes;
+    }
+    b.bytes = want;
+    return QLD_OK;
+}
+
+// Tensor map over a row-major table of `rows` rows, K uint64 words used per
+// row, `ld` words between rows; box = box_words x box_rows, 128-byte swizzle.
+int make_tmap(qld_ctx *c, CUtensorMap *tm, const void *base, int rows, int K, long long ld,
+              const KernelShape &ks) {
+    cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 8};
+    cuuint32_t box[2] = {(cuuint32_t)ks.box_words, (cuuint32_t)ks.box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = c->encode(tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, const_cast<void *>(base), dims,
+                           strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return set_err(c, QLD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d): rows=%d K=%d ld=%lld",
+                       (int)r, rows, K, ld);
+    return QLD_OK;
+}
+
+struct Task {
+    const uint64_t *A; const uint32_t *bcA; int m; long long lda;
+    const uint64_t *B; const uint32_t *bcB; int n; long long ldb;
+    int K, S, symmetric;
+};
+
+int choose_kernel(qld_ctx *c, const Task &) {
+    (void)c;
+    return QLD_KERNEL_POPC;
+}
+
+// Launch the counts kernel over B tile rows [tb0, tb0 + tiles_b), writing
+// r2/counts rows relative to out_row0.
+int launch_counts(qld_ctx *c, const Task &t, const CUtensorMap &tmA, const CUtensorMap &tmB,
+                  int tb0, int tiles_b, float *r2, long long ldr, uint32_t *cnt, long long ldc,
+                  int out_row0, cudaStream_t st) {
+    const int variant = c->kernel == QLD_KERNEL_AUTO ? choose_kernel(c, t) : c->kernel;
+    if (variant != QLD_KERNEL_POPC)
+        return set_err(c, QLD_ERR_UNSUPPORTED, "kernel variant %d is not available", variant);
+    const KernelShape &ks = kPopcShape;
+    LdParams p{};
+    p.m = t.m; p.n = t.n; p.K = t.K; p.S = t.S;
+    p.symmetric = t.symmetric;
+    p.nk = (t.K + ks.box_words - 1) / ks.box_words;
+    p.bcA = t.bcA; p.bcB = t.bcB;
+    p.r2 = r2; p.ldr = ldr; p.counts = cnt; p.ldc = ldc; p.out_row0 = out_row0;
+    p.status = c->d_status;
+    p.timeout_cycles = c->timeout_cycles;
+    for (int done = 0; done < tiles_b; done += 65535) {
+        const int nb = tiles_b - done < 65535 ? tiles_b - done : 65535;
+        p.tb0 = tb0 + done;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (c->profile) {
+            if (c->prof_used == c->prof.size()) {
+                cudaEvent_t a, b;
+                CUDA_TRY(c, cudaEventCreate(&a));
+                CUDA_TRY(c, cudaEventCreate(&b));
+                c->prof.emplace_back(a, b);
+            }
+            e0 = c->prof[c->prof_used].first;
+            e1 = c->prof[c->prof_used].second;
+            ++c->prof_used;
+            CUDA_TRY(c, cudaEventRecord(e0, st));
+        }
+        cudaError_t e = launch_popc(tmA, tmB, p, nb, c->r2_mode, st);
+        if (e != cudaSuccess)
+            return set_err(c, QLD_ERR_CUDA, "counts kernel launch failed: %s", cudaGetErrorString(e));
+        if (c->profile) CUDA_TRY(c, cudaEventRecord(e1, st));
+        c->stats.counts_launches++;
+        c->stats.kernel_launches++;
+    }
+    c->stats.last_kernel = variant;
+    return QLD_OK;
+}
+
+// Wait for `st`, fold the profiled kernel times in, and read/clear the status.
+int finish(qld_ctx *c, cudaStream_t st) {
+    CUDA_TRY(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(unsigned),
+                                cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(c, cudaStreamSynchronize(st));
+    for (size_t i = 0; i < c->prof_used; ++i) {
+        float ms = 0.f;
+        CUDA_TRY(c, cudaEventElapsedTime(&ms, c->prof[i].first, c->prof[i].second));
+        c->stats.counts_kernel_ms += ms;
+    }
+    c->prof_used = 0;
+    const unsigned st_bits = *c->h_status;
+    if (st_bits) {
+        CUDA_TRY(c, cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), st));
+        CUDA_TRY(c, cudaStreamSynchronize(st));
+        return set_err(c, QLD_ERR_TIMEOUT, "a counts kernel gave up a bounded wait (status 0x%x)",
+                       st_bits);
+    }
+    return QLD_OK;
+}
+
+bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace
+
+// ================================================================== C ABI ==
+
+extern "C" {
+
+int qld_cuda_init(int device, qld_ctx **ctx_out) {
+    if (!ctx_out) return QLD_ERR_INVALID;
+    *ctx_out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return QLD_ERR_NODEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10)
+        return QLD_ERR_NODEVICE;
+    qld_ctx *c = new (std::nothrow) qld_ctx();
+    if (!c) return QLD_ERR_NOMEM;
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    if (const char *s = getenv("QLD_TIMEOUT_CYCLES")) c->timeout_cycles = atoll(s);
+    int rc = QLD_OK;
+    do {
+        if (cudaSetDevice(device) != cudaSuccess) { rc = QLD_ERR_CUDA; break; }
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
+            rc = QLD_ERR_CUDA; break;
+        }
+        for (int i = 0; i < 2; ++i)
+            if (cudaEventCreateWithFlags(&c->ev_band[i], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->ev_copy[i], cudaEventDisableTiming) != cudaSuccess) {
+                rc = QLD_ERR_CUDA; break;
+            }
+        if (rc) break;
+        if (cudaMalloc(&c->d_status, sizeof(unsigned)) != cudaSuccess ||
+            cudaMemset(c->d_status, 0, sizeof(unsigned)) != cudaSuccess ||
+            cudaMallocHost(&c->h_status, sizeof(unsigned)) != cudaSuccess) {
+            rc = QLD_ERR_NOMEM; break;
+        }
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+                cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
+            rc = QLD_ERR_CUDA; break;
+        }
+        c->encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    } while (0);
+    if (rc) {
+        cudaGetLastError();
+        qld_cuda_release(c);
+        return rc;
+    }
+    *ctx_out = c;
+    return QLD_OK;
+}
+
+int qld_cuda_release(qld_ctx *c) {
+    if (!c) return QLD_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copy) cudaStreamSynchronize(c->copy);
+    DevBuf *bufs[] = {&c->dA, &c->dB, &c->dbcA, &c->dbcB, &c->dOut[0], &c->dOut[1],
+                      &c->dCnt[0], &c->dCnt[1]};
+    for (DevBuf *b : bufs)
+        if (b->p) cudaFree(b->p);
+    for (auto &e : c->prof) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    for (int i = 0; i < 2; ++i) {
+        if (c->ev_band[i]) cudaEventDestroy(c->ev_band[i]);
+        if (c->ev_copy[i]) cudaEventDestroy(c->ev_copy[i]);
+    }
+    if (c->d_status) cudaFree(c->d_status);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->copy) cudaStreamDestroy(c->copy);
+    delete c;
+    return QLD_OK;
+}
+
+const char *qld_cuda_last_error(const qld_ctx *c) { return c ? c->err : "no context"; }
+
+int qld_cuda_set_option(qld_ctx *c, int option, long long value) {
+    if (!c) return QLD_ERR_INVALID;
+    switch (option) {
+    case QLD_OPT_KERNEL:
+        if (value < QLD_KERNEL_AUTO || value > QLD_KERNEL_MMA)
+            return set_err(c, QLD_ERR_INVALID, "bad kernel variant %lld", value);
+        c->kernel = (int)value;
+        return QLD_OK;
+    case QLD_OPT_R2_MODE:
+        if (value != QLD_R2_EXACT && value != QLD_R2_REFERENCE)
+            return set_err(c, QLD_ERR_INVALID, "bad r2 mode %lld", value);
+        c->r2_mode = (int)value;
+        return QLD_OK;
+    case QLD_OPT_PROFILE:
+        c->profile = value ? 1 : 0;
+        return QLD_OK;
+    case QLD_OPT_BAND_ROWS:
+        if (value < 128 || value > (1 << 24))
+            return set_err(c, QLD_ERR_INVALID, "band rows %lld out of range", value);
+        c->band_rows = (int)((value + 127) / 128 * 128);
+        return QLD_OK;
+    default:
+        return set_err(c, QLD_ERR_INVALID, "unknown option %d", option);
+    }
+}
+
+int qld_cuda_get_stats(qld_ctx *c, qld_stats *out, int reset) {
+    if (!c) return QLD_ERR_INVALID;
+    if (out) *out = c->stats;
+    if (reset) {
+        const int last = c->stats.last_kernel;
+        c->stats = qld_stats{};
+        c->stats.last_kernel = last;
+    }
+    return QLD_OK;
+}
+
+int qld_cuda_host_alloc(qld_ctx *c, size_t bytes, void **ptr) {
+    if (!c || !ptr) return QLD_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (cudaMallocHost(ptr, bytes ? bytes : 1) != cudaSuccess) {
+        cudaGetLastError();
+        *ptr = nullptr;
+        return set_err(c, QLD_ERR_NOMEM, "cudaMallocHost(%zu) failed", bytes);
+    }
+    return QLD_OK;
+}
+
+int qld_cuda_host_free(qld_ctx *c, void *ptr) {
+    if (!c) return QLD_ERR_INVALID;
+    if (ptr) CUDA_TRY(c, cudaFreeHost(ptr));
+    return QLD_OK;
+}
+
+int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const uint64_t *B,
+                const uint32_t *bcB, int n, int K, int S, int symmetric, float *r2_out,
+                uint32_t *counts_out) {
+    if (!c) return QLD_ERR_INVALID;
+    if (symmetric) { B = A; bcB = bcA; n = m; }
+    if (m < 0 || n < 0 || K < 1 || S < 1)
+        return set_err(c, QLD_ERR_INVALID, "bad sizes m=%d n=%d K=%d S=%d", m, n, K, S);
+    if (m == 0 || n == 0) return QLD_OK;
+    if (!A || !bcA || !B || !bcB || !r2_out)
+        return set_err(c, QLD_ERR_INVALID, "NULL table, bit-count or output pointer");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const KernelShape &ks = kPopcShape;
+    const long long Kp = K + (K & 1);
+    int rc;
+    if ((rc = ensure(c, c->dA, (size_t)m * Kp * 8)) || (rc = ensure(c, c->dbcA, (size_t)m * 4)))
+        return rc;
+    CUDA_TRY(c, cudaMemcpy2DAsync(c->dA.p, Kp * 8, A, (size_t)K * 8, (size_t)K * 8, m,
+                                  cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->dbcA.p, bcA, (size_t)m * 4, cudaMemcpyHostToDevice, c->stream));
+    const uint64_t *dB = static_cast<const uint64_t *>(c->dA.p);
+    const uint32_t *dbcB = static_cast<const uint32_t *>(c->dbcA.p);
+    if (!symmetric) {
+        if ((rc = ensure(c, c->dB, (size_t)n * Kp * 8)) || (rc = ensure(c, c->dbcB, (size_t)n * 4)))
+            return rc;
+        CUDA_TRY(c, cudaMemcpy2DAsync(c->dB.p, Kp * 8, B, (size_t)K * 8, (size_t)K * 8, n,
+                                      cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(c->dbcB.p, bcB, (size_t)n * 4, cudaMemcpyHostToDevice,
+                                    c->stream));
+        dB = static_cast<const uint64_t *>(c->dB.p);
+        dbcB = static_cast<const uint32_t *>(c->dbcB.p);
+    }
+    Task t{static_cast<const uint64_t *>(c->dA.p), static_cast<const uint32_t *>(c->dbcA.p), m, Kp,
+           dB, dbcB, n, Kp, K, S, symmetric};
+    CUtensorMap tmA, tmB;
+    if ((rc = make_tmap(c, &tmA, t.A, m, K, Kp, ks)) || (rc = make_tmap(c, &tmB, t.B, n, K, Kp, ks)))
+        return rc;
+
+    const int band = c->band_rows;  // multiple of 128 == ks.bn
+    const int nbands = (n + band - 1) / band;
+    const size_t slot_rows = (size_t)(n < band ? n : band);
+    for (int s = 0; s < 2 && s < nbands; ++s) {
+        if ((rc = ensure(c, c->dOut[s], slot_rows * m * 4))) return rc;
+        if (counts_out && (rc = ensure(c, c->dCnt[s], slot_rows * m * 4))) return rc;
+    }
+    for (int bi = 0; bi < nbands; ++bi) {
+        const int s = bi & 1;
+        const int b0 = bi * band, b1 = b0 + band < n ? b0 + band : n;
+        if (bi >= 2) CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_copy[s], 0));
+        float *r2s = static_cast<float *>(c->dOut[s].p);
+        uint32_t *cs = counts_out ? static_cast<uint32_t *>(c->dCnt[s].p) : nullptr;
+        if ((rc = launch_counts(c, t, tmA, tmB, b0 / ks.bn, (b1 - b0 + ks.bn - 1) / ks.bn, r2s, m,
+                                cs, m, b0, c->stream)))
+            return rc;
+        CUDA_TRY(c, cudaEventRecord(c->ev_band[s], c->stream));
+        CUDA_TRY(c, cudaStreamWaitEvent(c->copy, c->ev_band[s], 0));
+        if (!symmetric) {
+            CUDA_TRY(c, cudaMemcpyAsync(r2_out + (size_t)b0 * m, r2s, (size_t)(b1 - b0) * m * 4,
+                                        cudaMemcpyDeviceToHost, c->copy));
+            if (cs)
+                CUDA_TRY(c, cudaMemcpyAsync(counts_out + (size_t)b0 * m, cs,
+                                            (size_t)(b1 - b0) * m * 4, cudaMemcpyDeviceToHost,
+                                            c->copy));
+        } else {
+            // Per 128-row tile row: columns [r0, m) hold every entry j >= i.
+            for (int r0 = b0; r0 < b1; r0 += ks.bn) {
+                const int r1 = r0 + ks.bn < b1 ? r0 + ks.bn : b1;
+                if (r0 >= m) break;
+                const size_t w = (size_t)(m - r0) * 4;
+                CUDA_TRY(c, cudaMemcpy2DAsync(r2_out + (size_t)r0 * m + r0, (size_t)m * 4,
+                                              r2s + (size_t)(r0 - b0) * m + r0, (size_t)m * 4, w,
+                                              r1 - r0, cudaMemcpyDeviceToHost, c->copy));
+                if (cs)
+                    CUDA_TRY(c, cudaMemcpy2DAsync(counts_out + (size_t)r0 * m + r0, (size_t)m * 4,
+                                                  cs + (size_t)(r0 - b0) * m + r0, (size_t)m * 4,
+                                                  w, r1 - r0, cudaMemcpyDeviceToHost, c->copy));
+            }
+        }
+        CUDA_TRY(c, cudaEventRecord(c->ev_copy[s], c->copy));
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(c->copy));
+    return finish(c, c->stream);
+}
+
+int qld_cuda_ld_device(qld_ctx *c, const qld_ld_args *a, void *stream) {
+    if (!c || !a) return QLD_ERR_INVALID;
+    Task t{a->A, a->bcA, a->m, a->lda, a->B, a->bcB, a->n, a->ldb, a->K, a->S, a->symmetric};
+    if (t.symmetric) { t.B = t.A; t.bcB = t.bcA; t.n = t.m; t.ldb = t.lda; }
+    if (t.m < 0 || t.n < 0 || t.K < 1 || t.S < 1 || t.lda < t.K || t.ldb < t.K || (t.lda & 1) ||
+        (t.ldb & 1) || a->ldr < t.m || (a->counts && a->ldc < t.m))
+        return set_err(c, QLD_ERR_INVALID, "bad sizes/strides m=%d n=%d K=%d lda=%lld ldb=%lld",
+                       t.m, t.n, t.K, t.lda, t.ldb);
+    if (t.m == 0 || t.n == 0) return QLD_OK;
+    if (!t.A || !t.B || !t.bcA || !t.bcB || !a->r2 || !aligned16(t.A) || !aligned16(t.B))
+        return set_err(c, QLD_ERR_INVALID, "NULL or misaligned device pointer");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const KernelShape &ks = kPopcShape;
+    CUtensorMap tmA, tmB;
+    int rc;
+    if ((rc = make_tmap(c, &tmA, t.A, t.m, t.K, t.lda, ks)) ||
+        (rc = make_tmap(c, &tmB, t.B, t.n, t.K, t.ldb, ks)))
+        return rc;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    return launch_counts(c, t, tmA, tmB, 0, (t.n + ks.bn - 1) / ks.bn, a->r2, a->ldr, a->counts,
+                         a->ldc, 0, st);
+}
+
+int qld_cuda_sync(qld_ctx *c, void *stream) {
+    if (!c) return QLD_ERR_INVALID;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    return finish(c, stream ? static_cast<cudaStream_t>(stream) : c->stream);
+}
+
+}  // extern "C"

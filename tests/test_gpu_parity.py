@@ -1,0 +1,161 @@
+"""GPU parity of the counts kernels + fused r^2 epilogue against the oracle
+and the reference's golden vectors, through the C ABI.
+
+Bars: counts bit-exact; r^2 in QLD_R2_REFERENCE mode bit-identical to the
+reference's get_pairwise_ld_score(); r^2 in QLD_R2_EXACT mode within 1e-6
+relative of the FP64 oracle (special values exact).
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import assert_r2_close, golden_names, load_golden, lower_mask
+from qld_b200 import api, synth
+
+pytestmark = pytest.mark.gpu
+
+KERNELS = [api.KERNEL_POPC]
+
+
+def _check_task(ctx, A, B, S, symmetric, kernel):
+    ctx.set_option(api.OPT_KERNEL, kernel)
+    bcA = oracle.bitcounts(A)
+    Bx = A if symmetric else B
+    bcB = oracle.bitcounts(Bx)
+    want_c = oracle.counts(A, Bx)
+    mask = lower_mask(*want_c.shape) if symmetric else None
+    sel = (lambda x: x[mask]) if symmetric else (lambda x: x)
+
+    ctx.set_option(api.OPT_R2_MODE, api.R2_EXACT)
+    r2, cnt = ctx.ld(A, bcA, None if symmetric else B, None if symmetric else bcB, S=S,
+                     symmetric=symmetric, counts=True)
+    assert np.array_equal(sel(cnt), sel(want_c)), "counts differ"
+    want64 = oracle.r2_exact(bcA, bcB, want_c, S)
+    err = assert_r2_close(r2, want64, mask=mask)
+
+    ctx.set_option(api.OPT_R2_MODE, api.R2_REFERENCE)
+    r2r = ctx.ld(A, bcA, None if symmetric else B, None if symmetric else bcB, S=S,
+                 symmetric=symmetric)
+    want_ref = oracle.r2_reference(bcA, bcB, want_c, S, fma_contract=False)
+    assert np.array_equal(sel(r2r).view(np.uint32), sel(want_ref).view(np.uint32)), \
+        "reference-mode r2 not bit-identical"
+    ctx.set_option(api.OPT_R2_MODE, api.R2_EXACT)
+    return err
+
+
+SHAPES = [
+    # m, n, samples, symmetric
+    (1, 1, 1, False),
+    (5, 3, 64, False),
+    (129, 77, 450, False),
+    (300, 200, 1000, False),
+    (257, 257, 16622, True),
+    (1000, 1000, 4096, True),
+    (640, 1300, 130, False),
+    (130, 130, 2049, True),
+    (2048, 2048, 4096, True),       # the all-pairs workload's size
+]
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("m,n,N,sym", SHAPES)
+def test_random_shapes(gpu_ctx, kernel, m, n, N, sym):
+    t, _ = synth.all_pairs_workload(m=m + (0 if sym else n), n=N, seed=m * 7 + n)
+    T = t.numpy().view(np.uint64)
+    A = T[:m]
+    B = None if sym else T[m:]
+    _check_task(gpu_ctx, A, B, N, sym, kernel)
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("name", golden_names())
+def test_golden(gpu_ctx, kernel, name):
+    g = load_golden(name)
+    gpu_ctx.set_option(api.OPT_KERNEL, kernel)
+    sym = g["symmetric"]
+    mask = lower_mask(*g["counts"].shape) if sym else np.ones(g["counts"].shape, bool)
+    gpu_ctx.set_option(api.OPT_R2_MODE, api.R2_REFERENCE)
+    r2, cnt = gpu_ctx.ld(g["A"], g["bcA"], None if sym else g["B"], None if sym else g["bcB"],
+                         S=g["S"], symmetric=sym, counts=True)
+    gpu_ctx.set_option(api.OPT_R2_MODE, api.R2_EXACT)
+    assert np.array_equal(cnt[mask], g["counts"][mask])
+    assert np.array_equal(r2[mask].view(np.uint32), g["r2_ref"][mask].view(np.uint32))
+    # the report written from the GPU results is the reference's, byte for byte
+    if sym:
+        r2 = np.where(mask, r2, g["r2_ref"])
+    rep = oracle.write_results(g["posA"], g["idA"], g["bcA"], g["posB"], g["idB"], g["bcB"],
+                               g["S"], r2, g["r2limit"], 0 if sym else 1)
+    assert rep == g["report"]
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_device_resident_call(gpu_ctx, kernel):
+    """qld_cuda_ld_device on torch buffers with padded pitches."""
+    gpu_ctx.set_option(api.OPT_KERNEL, kernel)
+    m, n, N = 700, 300, 3000
+    t, _ = synth.all_pairs_workload(m=m + n, n=N, seed=4)
+    K = t.shape[1]
+    lda = K + 6
+    dev = torch.device("cuda", 0)
+    At = torch.zeros(m, lda, dtype=torch.int64, device=dev)
+    Bt = torch.zeros(n, lda, dtype=torch.int64, device=dev)
+    At[:, :K] = t[:m].to(dev)
+    Bt[:, :K] = t[m:].to(dev)
+    At[:, K:] = -1   # words past K must never be read
+    Bt[:, K:] = -1
+    A = t[:m].numpy().view(np.uint64)
+    B = t[m:].numpy().view(np.uint64)
+    bcA = torch.from_numpy(oracle.bitcounts(A).view(np.int32)).to(dev)
+    bcB = torch.from_numpy(oracle.bitcounts(B).view(np.int32)).to(dev)
+    ldr = m + 13
+    r2 = torch.full((n, ldr), -7.0, dtype=torch.float32, device=dev)
+    cnt = torch.zeros((n, ldr), dtype=torch.int32, device=dev)
+    st = torch.cuda.current_stream()
+    gpu_ctx.ld_device(At, bcA, m, lda, Bt, bcB, n, lda, K, N, False, r2, ldr, cnt, ldr, stream=st)
+    gpu_ctx.sync(stream=st)
+    want_c = oracle.counts(A, B)
+    got_c = cnt[:, :m].cpu().numpy().view(np.uint32)
+    assert np.array_equal(got_c, want_c)
+    assert torch.all(r2[:, m:] == -7.0), "wrote past m in a padded row"
+    assert_r2_close(r2[:, :m].cpu().numpy(), oracle.r2_exact(oracle.bitcounts(A), oracle.bitcounts(B), want_c, N))
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_streamed_bands(gpu_ctx, kernel):
+    """Host-buffer call with several output bands (band rows < n)."""
+    gpu_ctx.set_option(api.OPT_KERNEL, kernel)
+    gpu_ctx.set_option(api.OPT_BAND_ROWS, 256)
+    try:
+        T1 = synth.all_pairs_workload(m=1100, n=1500, seed=9)[0].numpy().view(np.uint64)
+        err = _check_task(gpu_ctx, T1, None, 1500, True, kernel)
+        t, _ = synth.all_pairs_workload(m=1700, n=777, seed=10)
+        T = t.numpy().view(np.uint64)
+        _check_task(gpu_ctx, T[:600], T[600:], 777, False, kernel)
+    finally:
+        gpu_ctx.set_option(api.OPT_BAND_ROWS, 4096)
+    assert err[0] <= 1e-6
+
+
+def test_pinned_buffers(gpu_ctx):
+    m, N = 900, 5000
+    t, _ = synth.all_pairs_workload(m=m, n=N, seed=21)
+    A = gpu_ctx.pinned_empty(t.shape, np.uint64)
+    A[:] = t.numpy().view(np.uint64)
+    bc = gpu_ctx.pinned_empty((m,), np.uint32)
+    bc[:] = oracle.bitcounts(A)
+    out = gpu_ctx.pinned_empty((m, m), np.float32)
+    gpu_ctx.ld(A, bc, S=N, r2_out=out)
+    want = oracle.r2_exact(bc, bc, oracle.counts(A), N)
+    assert_r2_close(out, want, mask=lower_mask(m, m))
+
+
+def test_invalid_arguments_return_codes(gpu_ctx):
+    A = np.zeros((4, 2), np.uint64)
+    bc = np.zeros(4, np.uint32)
+    with pytest.raises(api.QldError) as e:
+        gpu_ctx.ld(A, bc, S=0)
+    assert e.value.code == api.ERR_INVALID
+    with pytest.raises(api.QldError) as e:
+        gpu_ctx.set_option(api.OPT_KERNEL, 99)
+    assert e.value.code == api.ERR_INVALID

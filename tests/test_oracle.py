@@ -1,0 +1,89 @@
+"""CPU tests: the oracle against the reference's golden vectors (and against
+the reference library itself when it is built)."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden_names, load_golden, lower_mask
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_counts_match_golden(name):
+    g = load_golden(name)
+    C = oracle.counts(g["A"], g["B"])
+    assert np.array_equal(C, g["counts"])
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_bitcounts_match_golden(name):
+    g = load_golden(name)
+    assert np.array_equal(oracle.bitcounts(g["A"]), g["bcA"])
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_r2_reference_semantics_bit_exact(name):
+    g = load_golden(name)
+    r = oracle.r2_reference(g["bcA"], g["bcB"], g["counts"], g["S"], fma_contract=False)
+    assert np.array_equal(r.view(np.uint32), g["r2_ref"].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_report_bytes_match_golden(name):
+    g = load_golden(name)
+    rep = oracle.write_results(g["posA"], g["idA"], g["bcA"], g["posB"], g["idB"], g["bcB"],
+                               g["S"], g["r2_ref"], g["r2limit"], 0 if g["symmetric"] else 1)
+    assert rep == g["report"]
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_exact_oracle_agrees_where_reference_is_well_conditioned(name):
+    """The FP64 oracle and the reference agree to float precision wherever the
+    reference's FP32 numerator does not cancel (r^2 > 1e-2)."""
+    g = load_golden(name)
+    e = oracle.r2_exact(g["bcA"], g["bcB"], g["counts"], g["S"])
+    r = g["r2_ref"].astype(np.float64)
+    sel = np.isfinite(e) & (e > 1e-2) & (e < 100)
+    if g["symmetric"]:
+        sel &= lower_mask(*e.shape)
+    if sel.any():
+        rel = np.abs(r[sel] - e[sel]) / e[sel]
+        assert rel.max() < 1e-3
+
+
+def test_fprint_f_truncates_like_reference():
+    assert oracle.fprint_f(0.0) == "0."
+    assert oracle.fprint_f(1.0) == "1."
+    assert oracle.fprint_f(0.5) == "0.500000000"
+    assert oracle.fprint_f(0.25) == "0.250000000"
+    # float32(0.1) * 1e9 in float -> 100000000 exactly -> "0.100000000"
+    assert oracle.fprint_f(0.1) == "0.100000000"
+    # float32(1/3) * 1e9 rounds to 333333344 in float before truncation
+    assert oracle.fprint_f(1.0 / 3.0) == "0.333333344"
+    assert oracle.fprint_f(123.456).startswith("123.")
+
+
+def test_symmetric_counts_lower_triangle():
+    rng = np.random.default_rng(3)
+    A = rng.integers(0, 2**63, size=(40, 5), dtype=np.uint64)
+    full = oracle.counts(A)
+    low = oracle.counts(A, lower_only=True)
+    mask = lower_mask(40, 40)
+    assert np.array_equal(full[mask], low[mask])
+    assert np.all(low[~mask] == 0)
+    assert np.array_equal(full, full.T)
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref not built")
+def test_restatement_matches_reference_library_random():
+    rng = np.random.default_rng(5)
+    for (m, n, K) in [(1, 1, 1), (17, 9, 3), (150, 131, 7)]:
+        A = rng.integers(0, 2**64 - 1, size=(m, K), dtype=np.uint64)
+        B = rng.integers(0, 2**64 - 1, size=(n, K), dtype=np.uint64)
+        C = oracle.counts(A, B)
+        assert np.array_equal(C.astype(np.uint64), oracle.ref_counts_gemm(A, B))
+        assert np.array_equal(C.astype(np.uint64), oracle.ref_counts_ukr(A, B, threads=2))
+        S = 64 * K
+        bcA, bcB = oracle.bitcounts(A), oracle.bitcounts(B)
+        r_ref = oracle.ref_ld_score(bcA, bcB, C.astype(np.uint64), S)
+        r_me = oracle.r2_reference(bcA, bcB, C, S, fma_contract=False)
+        assert np.array_equal(r_ref.view(np.uint32), r_me.view(np.uint32))
