@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--snps", type=int, default=0,
+                    help="use only the first N SNPs of the workload (profiling captures)")
     return ap.parse_args()
 
 
@@ -206,6 +208,10 @@ def ours_arm(args, rank, world, local_rank):
     cfg["l2"] = "512 MB flush write between timed steps"
 
     T, S = make_table(args.workload, dev, seed_offset=rank)
+    if args.snps:
+        T = T[:args.snps].contiguous()
+        cfg["snps"] = T.shape[0]
+        cfg["workload"] += f"_first{T.shape[0]}"
     m, K = T.shape
     lda = K + (K & 1)
     Tp = torch.zeros(m, lda, dtype=torch.int64, device=dev)
