@@ -196,7 +196,7 @@ cudaError_t launch_mode(const CUtensorMap &tmA, const CUtensorMap &tmB, const Ld
 
 }  // namespace
 
-const KernelShape kPopcShape = {BM, BN, KC, 128};
+const KernelShape kPopcShape = {BM, BN, KC, BM, BN, 128};
 
 cudaError_t launch_popc(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
                         int tiles_b, int r2_mode, cudaStream_t st) {

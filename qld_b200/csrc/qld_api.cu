@@ -93,15 +93,16 @@ int ensure(qld_ctx *c, DevBuf &b, size_t bytes) {
 // Tensor map over a row-major table of `rows` rows, K uint64 words used per
 // row, `ld` words between rows; box = box_words x box_rows, 128-byte swizzle.
 int make_tmap(qld_ctx *c, CUtensorMap *tm, const void *base, int rows, int K, long long ld,
-              const KernelShape &ks) {
+              int box_words, int box_rows, int swizzle) {
     cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)ld * 8};
-    cuuint32_t box[2] = {(cuuint32_t)ks.box_words, (cuuint32_t)ks.box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)box_words, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
+    const CUtensorMapSwizzle sw =
+        swizzle == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
     CUresult r = c->encode(tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, const_cast<void *>(base), dims,
-                           strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                           strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
         return set_err(c, QLD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d): rows=%d K=%d ld=%lld",
                        (int)r, rows, K, ld);
@@ -119,15 +120,23 @@ int choose_kernel(qld_ctx *c, const Task &) {
     return QLD_KERNEL_POPC;
 }
 
-// Launch the counts kernel over B tile rows [tb0, tb0 + tiles_b), writing
-// r2/counts rows relative to out_row0.
-int launch_counts(qld_ctx *c, const Task &t, const CUtensorMap &tmA, const CUtensorMap &tmB,
-                  int tb0, int tiles_b, float *r2, long long ldr, uint32_t *cnt, long long ldc,
-                  int out_row0, cudaStream_t st) {
+const KernelShape &shape_of(int variant) {
+    return variant == QLD_KERNEL_MMA ? kMmaShape : kPopcShape;
+}
+
+// Launch the counts kernel over B rows [b0, b1) (b0 a multiple of 256),
+// writing r2/counts rows relative to out_row0.
+int launch_counts(qld_ctx *c, const Task &t, int b0, int b1, float *r2, long long ldr,
+                  uint32_t *cnt, long long ldc, int out_row0, cudaStream_t st) {
     const int variant = c->kernel == QLD_KERNEL_AUTO ? choose_kernel(c, t) : c->kernel;
-    if (variant != QLD_KERNEL_POPC)
-        return set_err(c, QLD_ERR_UNSUPPORTED, "kernel variant %d is not available", variant);
-    const KernelShape &ks = kPopcShape;
+    const KernelShape &ks = shape_of(variant);
+    CUtensorMap tmA, tmB;
+    int rc;
+    if ((rc = make_tmap(c, &tmA, t.A, t.m, t.K, t.lda, ks.box_words, ks.box_rows_a, ks.swizzle)) ||
+        (rc = make_tmap(c, &tmB, t.B, t.n, t.K, t.ldb, ks.box_words, ks.box_rows_b, ks.swizzle)))
+        return rc;
+    const int tb0 = b0 / ks.bn;
+    const int tiles_b = (b1 - b0 + ks.bn - 1) / ks.bn;
     LdParams p{};
     p.m = t.m; p.n = t.n; p.K = t.K; p.S = t.S;
     p.symmetric = t.symmetric;
@@ -152,7 +161,8 @@ int launch_counts(qld_ctx *c, const Task &t, const CUtensorMap &tmA, const CUten
             ++c->prof_used;
             CUDA_TRY(c, cudaEventRecord(e0, st));
         }
-        cudaError_t e = launch_popc(tmA, tmB, p, nb, c->r2_mode, st);
+        cudaError_t e = variant == QLD_KERNEL_MMA ? launch_mma(tmA, tmB, p, nb, c->r2_mode, st)
+                                                  : launch_popc(tmA, tmB, p, nb, c->r2_mode, st);
         if (e != cudaSuccess)
             return set_err(c, QLD_ERR_CUDA, "counts kernel launch failed: %s", cudaGetErrorString(e));
         if (c->profile) CUDA_TRY(c, cudaEventRecord(e1, st));
@@ -287,9 +297,9 @@ int qld_cuda_set_option(qld_ctx *c, int option, long long value) {
         c->profile = value ? 1 : 0;
         return QLD_OK;
     case QLD_OPT_BAND_ROWS:
-        if (value < 128 || value > (1 << 24))
+        if (value < 256 || value > (1 << 24))
             return set_err(c, QLD_ERR_INVALID, "band rows %lld out of range", value);
-        c->band_rows = (int)((value + 127) / 128 * 128);
+        c->band_rows = (int)((value + 255) / 256 * 256);
         return QLD_OK;
     default:
         return set_err(c, QLD_ERR_INVALID, "unknown option %d", option);
@@ -335,7 +345,6 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
     if (!A || !bcA || !B || !bcB || !r2_out)
         return set_err(c, QLD_ERR_INVALID, "NULL table, bit-count or output pointer");
     CUDA_TRY(c, cudaSetDevice(c->device));
-    const KernelShape &ks = kPopcShape;
     const long long Kp = K + (K & 1);
     int rc;
     if ((rc = ensure(c, c->dA, (size_t)m * Kp * 8)) || (rc = ensure(c, c->dbcA, (size_t)m * 4)))
@@ -357,11 +366,8 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
     }
     Task t{static_cast<const uint64_t *>(c->dA.p), static_cast<const uint32_t *>(c->dbcA.p), m, Kp,
            dB, dbcB, n, Kp, K, S, symmetric};
-    CUtensorMap tmA, tmB;
-    if ((rc = make_tmap(c, &tmA, t.A, m, K, Kp, ks)) || (rc = make_tmap(c, &tmB, t.B, n, K, Kp, ks)))
-        return rc;
 
-    const int band = c->band_rows;  // multiple of 128 == ks.bn
+    const int band = c->band_rows;  // multiple of 256: whole tile rows of every variant
     const int nbands = (n + band - 1) / band;
     const size_t slot_rows = (size_t)(n < band ? n : band);
     for (int s = 0; s < 2 && s < nbands; ++s) {
@@ -374,9 +380,7 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
         if (bi >= 2) CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_copy[s], 0));
         float *r2s = static_cast<float *>(c->dOut[s].p);
         uint32_t *cs = counts_out ? static_cast<uint32_t *>(c->dCnt[s].p) : nullptr;
-        if ((rc = launch_counts(c, t, tmA, tmB, b0 / ks.bn, (b1 - b0 + ks.bn - 1) / ks.bn, r2s, m,
-                                cs, m, b0, c->stream)))
-            return rc;
+        if ((rc = launch_counts(c, t, b0, b1, r2s, m, cs, m, b0, c->stream))) return rc;
         CUDA_TRY(c, cudaEventRecord(c->ev_band[s], c->stream));
         CUDA_TRY(c, cudaStreamWaitEvent(c->copy, c->ev_band[s], 0));
         if (!symmetric) {
@@ -387,9 +391,9 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
                                             (size_t)(b1 - b0) * m * 4, cudaMemcpyDeviceToHost,
                                             c->copy));
         } else {
-            // Per 128-row tile row: columns [r0, m) hold every entry j >= i.
-            for (int r0 = b0; r0 < b1; r0 += ks.bn) {
-                const int r1 = r0 + ks.bn < b1 ? r0 + ks.bn : b1;
+            // Per 128 rows: columns [r0, m) hold every entry j >= i.
+            for (int r0 = b0; r0 < b1; r0 += 128) {
+                const int r1 = r0 + 128 < b1 ? r0 + 128 : b1;
                 if (r0 >= m) break;
                 const size_t w = (size_t)(m - r0) * 4;
                 CUDA_TRY(c, cudaMemcpy2DAsync(r2_out + (size_t)r0 * m + r0, (size_t)m * 4,
@@ -419,15 +423,8 @@ int qld_cuda_ld_device(qld_ctx *c, const qld_ld_args *a, void *stream) {
     if (!t.A || !t.B || !t.bcA || !t.bcB || !a->r2 || !aligned16(t.A) || !aligned16(t.B))
         return set_err(c, QLD_ERR_INVALID, "NULL or misaligned device pointer");
     CUDA_TRY(c, cudaSetDevice(c->device));
-    const KernelShape &ks = kPopcShape;
-    CUtensorMap tmA, tmB;
-    int rc;
-    if ((rc = make_tmap(c, &tmA, t.A, t.m, t.K, t.lda, ks)) ||
-        (rc = make_tmap(c, &tmB, t.B, t.n, t.K, t.ldb, ks)))
-        return rc;
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
-    return launch_counts(c, t, tmA, tmB, 0, (t.n + ks.bn - 1) / ks.bn, a->r2, a->ldr, a->counts,
-                         a->ldc, 0, st);
+    return launch_counts(c, t, 0, t.n, a->r2, a->ldr, a->counts, a->ldc, 0, st);
 }
 
 int qld_cuda_sync(qld_ctx *c, void *stream) {

@@ -13,13 +13,20 @@ namespace qld {
 struct KernelShape {
     int bm, bn;       // A rows x B rows per output tile
     int box_words;    // K words per TMA box (one stage)
-    int box_rows;     // rows per TMA box
+    int box_rows_a;   // rows per TMA box of the A map
+    int box_rows_b;   // rows per TMA box of the B map
+    int swizzle;      // TMA swizzle span in bytes (64 or 128)
 };
 
 extern const KernelShape kPopcShape;
+extern const KernelShape kMmaShape;
 
 // Variant (a): tiles_b tile rows starting at p.tb0; p.nk = ceil(K / box_words).
 cudaError_t launch_popc(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
                         int tiles_b, int r2_mode, cudaStream_t st);
+
+// Variant (b): p.nk unused (the kernel derives its stages from K).
+cudaError_t launch_mma(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
+                       int tiles_b, int r2_mode, cudaStream_t st);
 
 }  // namespace qld

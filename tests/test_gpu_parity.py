@@ -15,7 +15,7 @@ from qld_b200 import api, synth
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = [api.KERNEL_POPC]
+KERNELS = [api.KERNEL_POPC, api.KERNEL_MMA]
 
 
 def _check_task(ctx, A, B, S, symmetric, kernel):
@@ -96,7 +96,7 @@ def test_device_resident_call(gpu_ctx, kernel):
     m, n, N = 700, 300, 3000
     t, _ = synth.all_pairs_workload(m=m + n, n=N, seed=4)
     K = t.shape[1]
-    lda = K + 6
+    lda = K + 6 + (K & 1)   # even pitch (16-byte aligned rows), padded
     dev = torch.device("cuda", 0)
     At = torch.zeros(m, lda, dtype=torch.int64, device=dev)
     Bt = torch.zeros(n, lda, dtype=torch.int64, device=dev)
