@@ -224,7 +224,10 @@ def ours_arm(args, rank, world, local_rank):
     kern = {"auto": api.KERNEL_AUTO, "popc": api.KERNEL_POPC, "mma": api.KERNEL_MMA}[args.kernel]
     ctx.set_option(api.OPT_KERNEL, kern)
     ctx.set_option(api.OPT_PROFILE, 1)
-    st = torch.cuda.current_stream()
+    # A dedicated stream: torch's default stream is the legacy NULL stream,
+    # which the C ABI reads as "the context's own stream".
+    st = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(st)
 
     def step():
         ctx.ld_device(Tp, bc, m, lda, Tp, bc, m, lda, K, S, True, out, m, stream=st)
@@ -241,11 +244,13 @@ def ours_arm(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local_rank) as clk:
+        torch.cuda.nvtx.range_push("qld_timed")
         for i in range(args.steps):
             flush.zero_()
             ev[i][0].record(st)
             step()
             ev[i][1].record(st)
+        torch.cuda.nvtx.range_pop()
         ctx.sync(stream=st)
         torch.cuda.synchronize()
     if world > 1:

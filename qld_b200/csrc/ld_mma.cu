@@ -1,31 +1,37 @@
-// ld_mma.cu -- counts kernel, variant (b): bits unpacked to int8 {0,1} in
-// shared memory, contracted by the 5th-generation tensor cores
+// ld_mma.cu -- counts kernel, variant (b): bits unpacked to 8-bit {0, 0x80}
+// in shared memory and contracted by the 5th-generation tensor cores
 // (tcgen05.mma.kind::i8, unsigned 8-bit operands, s32 accumulators in TMEM).
-// Exact: every product is 0 or 1 and a count is at most the sample size
-// (< 2^31).  The r^2 epilogue (qLD gemm_cpu.c:343-404) runs on the
-// accumulators as they leave TMEM.  Same contraction as variant (a):
-// qLD's blis_gemm()/bin_gemm_2x2 (gemm_cpu.c:125-341,
-// blis/config/binary_gemm/kernels/3/bin_gemm.c:4-141).
+// Every product is 0 or 0x80 * 0x80 = 2^14, so an accumulator holds exactly
+// 2^14 * count, which fits in s32 while the sample count is below 2^17
+// (the host routes larger K to variant (a)).  The r^2 epilogue (qLD
+// gemm_cpu.c:343-404) runs on the accumulators as they leave TMEM.  Same
+// contraction as variant (a): qLD's blis_gemm()/bin_gemm_2x2
+// (gemm_cpu.c:125-341, blis/config/binary_gemm/kernels/3/bin_gemm.c:4-141).
 //
-// One CTA computes a 128 (A rows) x 256 (B rows) output tile.  Warp roles:
-//   warp 0       TMA producer: per packed stage, 8 words (512 samples) of the
-//                128 A rows and of the 256 B rows (64-byte swizzle), into a
-//                ring of PST stages.
-//   warp 1       TMEM allocation (256 columns) and the single MMA-issuing
-//                thread: per unpacked stage (128 samples) 4 MMAs of
-//                128 x 256 x 32, then tcgen05.commit to free the stage.
+// Persistent: one CTA per SM walks a static list of 128 (A rows) x 256
+// (B rows) output tiles; tiles of a launch are ordered B-tile-row first so
+// the CTAs running at the same time share B panels in L2.  Warp roles:
+//   warp 0       TMA producer: per packed stage 8 words (512 samples) of the
+//                tile's 128 A rows and 256 B rows (64-byte swizzle).
+//   warp 1       TMEM owner (512 columns = two 128 x 256 s32 accumulators)
+//                and the MMA-issuing thread: per unpacked stage (128
+//                samples) 4 MMAs of 128 x 256 x 32 into the tile's
+//                accumulator, tcgen05.commit frees the stage; after the
+//                tile, a commit hands the accumulator to the epilogue.
 //   warps 2-9    unpack: each packed stage gives 4 unpacked stages of
-//                128 A + 256 B rows x 128 bytes, written in the canonical
-//                K-major 128-byte-swizzled layout the MMA descriptors name;
-//                then the epilogue: tcgen05.ld of the accumulators, r^2,
-//                coalesced stores (32 lanes = 32 consecutive A rows).
+//                128 + 256 rows x 128 bytes in the canonical K-major
+//                128-byte-swizzled layout the MMA descriptors name.
+//   warps 10-13  epilogue: tcgen05.ld of the finished accumulator (warp w
+//                reads TMEM lanes 32*(w%4)..), r^2, coalesced stores
+//                (32 lanes = 32 consecutive A rows), then release the
+//                accumulator -- overlapping the next tile's MMAs.
 //
 // Unpack mapping.  The 16 packed bytes of a row for one unpacked stage are
 // four 32-bit words w0..w3; output 16-byte chunk c (c = 0..7) holds the
-// words ((w0 >> c) & 0x01010101, ..., (w3 >> c) & 0x01010101), i.e. byte b of
-// its word j is bit c + 8b of w_j.  This is a fixed permutation of the 128
-// samples, the same for A and B, so sum_k a_k b_k is unchanged: one shift and
-// one AND per 4 output bytes.
+// words ((w0 << (7-c)) & 0x80808080, ..., (w3 << (7-c)) & 0x80808080), i.e.
+// byte b of its word j carries bit c + 8b of w_j.  This is a fixed
+// permutation of the 128 samples, the same for A and B, so the contraction
+// is unchanged: one shift (IMAD pipe) and one AND (ALU pipe) per 4 bytes.
 #include "qld_device.cuh"
 #include "qld_kernels.h"
 
@@ -36,28 +42,34 @@ namespace {
 constexpr int BM = 128, BN = 256;
 constexpr int PW = 8;                    // packed words per row per packed stage
 constexpr int SUB = PW / 2;              // unpacked stages (128 samples) per packed stage
-constexpr int PST = 4;                   // packed ring depth
-constexpr int UST = 2;                   // unpacked ring depth
+constexpr int PST = 3;                   // packed ring depth
+constexpr int UST = 3;                   // unpacked ring depth
 constexpr int PA_BYTES = BM * PW * 8;    // 8 KB
 constexpr int PB_BYTES = BN * PW * 8;    // 16 KB
 constexpr int UA_BYTES = BM * 128;       // 16 KB
 constexpr int UB_BYTES = BN * 128;       // 32 KB
 constexpr int UNPACK_WARPS = 8;
 constexpr int UNPACK_THREADS = UNPACK_WARPS * 32;
-constexpr int THREADS = 64 + UNPACK_THREADS;
-constexpr uint32_t TMEM_COLS = 256;
+constexpr int EPI_WARPS = 4;
+constexpr int EPI_THREADS = EPI_WARPS * 32;
+constexpr int FIRST_UNPACK_WARP = 2;
+constexpr int FIRST_EPI_WARP = FIRST_UNPACK_WARP + UNPACK_WARPS;
+constexpr int THREADS = (FIRST_EPI_WARP + EPI_WARPS) * 32;   // 448
+constexpr uint32_t TMEM_COLS = 512;                          // two accumulators
+constexpr int COUNT_SHIFT = 14;                              // log2(0x80 * 0x80)
 
 // smem map (offsets from a 1024-byte aligned base)
 constexpr int OFF_UA = 0;
 constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
 constexpr int OFF_PA = OFF_UB + UST * UB_BYTES;
 constexpr int OFF_PB = OFF_PA + PST * PA_BYTES;
-constexpr int OFF_BAR = OFF_PB + PST * PB_BYTES;
-constexpr int NBARS = 2 * PST + 2 * UST + 1;
-constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
-constexpr int OFF_ROWS = (OFF_TMEM + 16 + 15) / 16 * 16;        // per-B-row epilogue factors
+constexpr int OFF_ROWS = OFF_PB + PST * PB_BYTES;            // per-B-row epilogue factors
 constexpr int ROWS_BYTES = BN * (8 + 4 + 4);
-constexpr int SMEM_BYTES = OFF_ROWS + ROWS_BYTES + 1024;
+constexpr int OFF_BAR = OFF_ROWS + ROWS_BYTES;
+constexpr int NBARS = 2 * PST + 2 * UST + 2 + 2 + 1;
+constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
+constexpr int SMEM_BYTES = OFF_TMEM + 16 + 1024;
+static_assert(SMEM_BYTES <= 232448, "shared memory budget");
 
 // Instruction descriptor, kind::i8: D = s32 (bits 4-5 = 2), A and B unsigned
 // 8-bit (bits 7-9, 10-12 = 0), both K-major (bits 15, 16 = 0),
@@ -123,35 +135,68 @@ __device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
 }
 
 __device__ __forceinline__ uint4 unpack_chunk(const uint4 &w, int c) {
-    const uint32_t M = 0x01010101u;
-    return make_uint4((w.x >> c) & M, (w.y >> c) & M, (w.z >> c) & M, (w.w >> c) & M);
+    const uint32_t M = 0x80808080u;
+    const int s = 7 - c;
+    return make_uint4((w.x << s) & M, (w.y << s) & M, (w.z << s) & M, (w.w << s) & M);
 }
+
+// Tile list of one launch: B tile rows tb in [tb0, tb0 + tiles_b), and in
+// each the A tiles ta in [ta_lo(tb), TA) -- all of them for two regions,
+// those reaching the diagonal (a >= b somewhere) for a single region.
+struct TileList {
+    int TA, tb0, tiles_b, symmetric;
+    __device__ __forceinline__ int ta_lo(int tb) const {
+        return symmetric ? (tb * BN) / BM : 0;
+    }
+    __device__ __forceinline__ int count() const {
+        int n = 0;
+        for (int t = 0; t < tiles_b; ++t) {
+            const int c = TA - ta_lo(tb0 + t);
+            n += c > 0 ? c : 0;
+        }
+        return n;
+    }
+    __device__ __forceinline__ void decode(int idx, int &ta, int &tb) const {
+        for (int t = 0; t < tiles_b; ++t) {
+            const int lo = ta_lo(tb0 + t);
+            const int c = TA - lo > 0 ? TA - lo : 0;
+            if (idx < c) {
+                ta = lo + idx;
+                tb = tb0 + t;
+                return;
+            }
+            idx -= c;
+        }
+        ta = tb = -1;
+    }
+};
 
 template <int MODE>
 __global__ void __launch_bounds__(THREADS, 1)
 k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-         const LdParams p) {
+         const LdParams p, const int tiles_b) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + OFF_BAR);
     uint64_t *pfull = bars, *pempty = bars + PST;
     uint64_t *ufull = bars + 2 * PST, *uempty = bars + 2 * PST + UST;
-    uint64_t *accf = bars + 2 * PST + 2 * UST;
+    uint64_t *accfull = bars + 2 * PST + 2 * UST;
+    uint64_t *accempty = accfull + 2;
+    uint64_t *mma_done = accempty + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + OFF_TMEM);
     double *rowd = reinterpret_cast<double *>(smem + OFF_ROWS);
     uint32_t *rowc = reinterpret_cast<uint32_t *>(smem + OFF_ROWS + BN * 8);
     float *rowv = reinterpret_cast<float *>(smem + OFF_ROWS + BN * 12);
 
-    const int ta = blockIdx.x;
-    const int tb = p.tb0 + blockIdx.y;
-    if (p.symmetric && ta * BM + BM - 1 < tb * BN) return;
     if (grid_failed(p.status)) return;
+    const TileList tl{(p.m + BM - 1) / BM, p.tb0, tiles_b, p.symmetric};
+    const int ntiles = tl.count();
+    if ((int)blockIdx.x >= ntiles) return;
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int np = (p.K + PW - 1) / PW;      // packed stages
-    const int nu = np * SUB;                 // unpacked stages
+    const int np = (p.K + PW - 1) / PW;      // packed stages per tile
 
     if (tid == 0) {
         for (int s = 0; s < PST; ++s) {
@@ -162,7 +207,11 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
             mbar_init(smem_u32(&ufull[s]), UNPACK_WARPS);
             mbar_init(smem_u32(&uempty[s]), 1);
         }
-        mbar_init(smem_u32(accf), 1);
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(smem_u32(&accfull[s]), 1);
+            mbar_init(smem_u32(&accempty[s]), EPI_WARPS);
+        }
+        mbar_init(smem_u32(mma_done), 1);
         fence_barrier_init();
     }
     if (warp == 1) {
@@ -178,167 +227,211 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0) {
-        // --------------------------------------------------------- producer --
+        // ------------------------------------------------------- producer --
         if (lane == 0) {
             prefetch_tmap(&tmA);
             prefetch_tmap(&tmB);
-            int issued = 0;
-            for (int kp = 0; kp < np; ++kp) {
-                const int s = kp % PST;
-                if (kp >= PST && !mbar_wait(smem_u32(&pempty[s]), ((kp / PST) - 1) & 1,
-                                            p.timeout_cycles, p.status)) {
-                    flag_error(p.status, ST_TIMEOUT_EMPTY);
-                    break;
+            int gp = 0;   // packed stages issued so far (ring position)
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                int ta, tb;
+                tl.decode(tile, ta, tb);
+                for (int kp = 0; kp < np; ++kp, ++gp) {
+                    const int s = gp % PST;
+                    if (gp >= PST && !mbar_wait(smem_u32(&pempty[s]), ((gp / PST) - 1) & 1,
+                                                p.timeout_cycles, p.status)) {
+                        flag_error(p.status, ST_TIMEOUT_EMPTY);
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t fb = smem_u32(&pfull[s]);
+                    mbar_arrive_expect_tx(fb, PA_BYTES + PB_BYTES);
+                    tma_load_2d(smem_u32(smem + OFF_PA + s * PA_BYTES), &tmA, kp * PW, ta * BM, fb);
+                    tma_load_2d(smem_u32(smem + OFF_PB + s * PB_BYTES), &tmB, kp * PW, tb * BN, fb);
                 }
-                const uint32_t fb = smem_u32(&pfull[s]);
-                mbar_arrive_expect_tx(fb, PA_BYTES + PB_BYTES);
-                tma_load_2d(smem_u32(smem + OFF_PA + s * PA_BYTES), &tmA, kp * PW, ta * BM, fb);
-                tma_load_2d(smem_u32(smem + OFF_PB + s * PB_BYTES), &tmB, kp * PW, tb * BN, fb);
-                ++issued;
             }
-            for (int kp = issued > PST ? issued - PST : 0; kp < issued; ++kp)
-                if (!mbar_wait(smem_u32(&pfull[kp % PST]), (kp / PST) & 1, p.timeout_cycles,
+            // Drain: this CTA's copies must land before it retires.
+            for (int g = gp > PST ? gp - PST : 0; g < gp; ++g)
+                if (!mbar_wait(smem_u32(&pfull[g % PST]), (g / PST) & 1, p.timeout_cycles,
                                nullptr)) {
                     flag_error(p.status, ST_TIMEOUT_DRAIN);
                     break;
                 }
         }
     } else if (warp == 1) {
-        // ------------------------------------------------------ MMA issuer --
+        // ----------------------------------------------------- MMA issuer --
         if (lane == 0) {
-            for (int u = 0; u < nu; ++u) {
-                const int s = u % UST;
-                if (!mbar_wait(smem_u32(&ufull[s]), (u / UST) & 1, p.timeout_cycles, p.status)) {
-                    flag_error(p.status, ST_TIMEOUT_UNPACK);
+            int gu = 0, it = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
+                const int ab = it & 1;
+                if (it >= 2 && !mbar_wait(smem_u32(&accempty[ab]), ((it >> 1) - 1) & 1,
+                                          p.timeout_cycles, p.status)) {
+                    flag_error(p.status, ST_TIMEOUT_MMA);
                     break;
                 }
                 tc_fence_after();
-                const uint32_t a0 = smem_u32(smem + OFF_UA + s * UA_BYTES);
-                const uint32_t b0 = smem_u32(smem + OFF_UB + s * UB_BYTES);
+                const uint32_t d = tmem + (uint32_t)(ab * BN);
+                for (int u = 0; u < np * SUB; ++u, ++gu) {
+                    const int s = gu % UST;
+                    if (!mbar_wait(smem_u32(&ufull[s]), (gu / UST) & 1, p.timeout_cycles,
+                                   p.status)) {
+                        flag_error(p.status, ST_TIMEOUT_UNPACK);
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a0 = smem_u32(smem + OFF_UA + s * UA_BYTES);
+                    const uint32_t b0 = smem_u32(smem + OFF_UB + s * UB_BYTES);
 #pragma unroll
-                for (int kk = 0; kk < 4; ++kk)
-                    tc_mma_i8(tmem, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), IDESC,
-                              (u > 0 || kk > 0) ? 1u : 0u);
-                tc_commit(smem_u32(&uempty[s]));
+                    for (int kk = 0; kk < 4; ++kk)
+                        tc_mma_i8(d, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), IDESC,
+                                  (u > 0 || kk > 0) ? 1u : 0u);
+                    tc_commit(smem_u32(&uempty[s]));
+                }
+                tc_commit(smem_u32(&accfull[ab]));   // also on the error path
             }
-            // Fires once every MMA issued above has completed (also on the
-            // error path, so TMEM is never released under a running MMA).
-            tc_commit(smem_u32(accf));
+            tc_commit(smem_u32(mma_done));           // every MMA above has completed
         }
-    } else {
+    } else if (warp < FIRST_EPI_WARP) {
         // --------------------------------------------------------- unpack --
-        const int ut = tid - 64;
-        // B-row epilogue factors for this tile, computed while data streams.
-        {
-            const int b = tb * BN + ut;
-            const uint32_t c = b < p.n ? p.bcB[b] : 0u;
-            rowc[ut] = c;
-            if (MODE == R2_EXACT) {
-                rowd[ut] = row_exact(c, p.S).inv_var;
-            } else {
-                const RowRef r = row_ref(c, p.S);
-                rowv[ut] = r.v;
-                rowd[ut] = r.one_minus;
-            }
-        }
+        const int ut = tid - FIRST_UNPACK_WARP * 32;
+        int gp = 0, gu = 0;
         bool ok = true;
-        for (int kp = 0; kp < np && ok; ++kp) {
-            const int ps = kp % PST;
-            // Wait outcomes are made warp-uniform so the warp never splits.
-            const bool got = mbar_wait(smem_u32(&pfull[ps]), (kp / PST) & 1, p.timeout_cycles,
-                                       p.status);
-            if (!__all_sync(0xffffffffu, got)) {
-                if (lane == 0) flag_error(p.status, ST_TIMEOUT_FULL);
-                ok = false;
-                break;
-            }
-            const uint8_t *pa = smem + OFF_PA + ps * PA_BYTES;
-            const uint8_t *pb = smem + OFF_PB + ps * PB_BYTES;
-            for (int sub = 0; sub < SUB; ++sub) {
-                const int u = kp * SUB + sub;
-                const int us = u % UST;
-                const bool freed = u < UST || mbar_wait(smem_u32(&uempty[us]), ((u / UST) - 1) & 1,
-                                                        p.timeout_cycles, p.status);
-                if (!__all_sync(0xffffffffu, freed)) {
-                    if (lane == 0) flag_error(p.status, ST_TIMEOUT_MMA);
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            for (int kp = 0; kp < np && ok; ++kp, ++gp) {
+                const int ps = gp % PST;
+                // Wait outcomes are made warp-uniform so the warp never splits.
+                const bool got = mbar_wait(smem_u32(&pfull[ps]), (gp / PST) & 1,
+                                           p.timeout_cycles, p.status);
+                if (!__all_sync(0xffffffffu, got)) {
+                    if (lane == 0) flag_error(p.status, ST_TIMEOUT_FULL);
                     ok = false;
                     break;
                 }
-                uint8_t *ua = smem + OFF_UA + us * UA_BYTES;
-                uint8_t *ub = smem + OFF_UB + us * UB_BYTES;
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const int t = ut + j * UNPACK_THREADS;   // 768 tasks: (row, half)
-                    const int row = t >> 1, half = t & 1;
-                    const bool isA = row < BM;
-                    const int r = isA ? row : row - BM;
-                    // packed row r: 64 bytes, 64-byte swizzle (16-byte chunk ^= (r>>1)&3)
-                    const uint8_t *src = (isA ? pa : pb) + r * 64 + ((sub ^ ((r >> 1) & 3)) << 4);
-                    const uint4 w = *reinterpret_cast<const uint4 *>(src);
-                    uint8_t *dst = (isA ? ua : ub) + r * 128;
-#pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        const int c = half * 4 + cc;
-                        *reinterpret_cast<uint4 *>(dst + ((c ^ (r & 7)) << 4)) = unpack_chunk(w, c);
+                const uint8_t *pa = smem + OFF_PA + ps * PA_BYTES;
+                const uint8_t *pb = smem + OFF_PB + ps * PB_BYTES;
+                for (int sub = 0; sub < SUB; ++sub, ++gu) {
+                    const int us = gu % UST;
+                    const bool freed = gu < UST || mbar_wait(smem_u32(&uempty[us]),
+                                                             ((gu / UST) - 1) & 1,
+                                                             p.timeout_cycles, p.status);
+                    if (!__all_sync(0xffffffffu, freed)) {
+                        if (lane == 0) flag_error(p.status, ST_TIMEOUT_MMA);
+                        ok = false;
+                        break;
                     }
-                }
-                fence_proxy_async_smem();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(smem_u32(&ufull[us]));
-            }
-            if (!ok) break;
-            __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&pempty[ps]));
-        }
-
-        // -------------------------------------------------------- epilogue --
-        named_bar_sync(1, UNPACK_THREADS);   // row factors visible to all unpack warps
-        bool ready = ok && mbar_wait(smem_u32(accf), 0, p.timeout_cycles, p.status);
-        ready = __all_sync(0xffffffffu, ready);
-        if (ready) {
-            __syncwarp();
-            tc_fence_after();
-            const int q = warp & 3;                  // TMEM lane quarter of this warp
-            const int h = (warp - 2) >> 2;           // column half
-            const int a = ta * BM + q * 32 + lane;
-            const bool a_ok = a < p.m;
-            const uint32_t ca = a_ok ? p.bcA[a] : 0u;
-            RowExact ra_e;
-            RowRef ra_r;
-            if (MODE == R2_EXACT) ra_e = row_exact(ca, p.S);
-            else ra_r = row_ref(ca, p.S);
-#pragma unroll 1
-            for (int cb = 0; cb < 4; ++cb) {
-                uint32_t v[32];
-                const int col0 = h * 128 + cb * 32;
-                __syncwarp();
-                tc_ld_32x32b_x32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col0, v);
+                    uint8_t *ua = smem + OFF_UA + us * UA_BYTES;
+                    uint8_t *ub = smem + OFF_UB + us * UB_BYTES;
 #pragma unroll
-                for (int t = 0; t < 32; ++t) {
-                    const int bl = col0 + t;
-                    const int b = tb * BN + bl;
-                    if (b < p.n && a_ok && (!p.symmetric || a >= b)) {
-                        float r2;
-                        if (MODE == R2_EXACT) {
-                            RowExact rb;
-                            rb.c = rowc[bl];
-                            rb.inv_var = rowd[bl];
-                            r2 = r2_exact(v[t], ra_e, rb, p.S);
-                        } else {
-                            RowRef rb;
-                            rb.c = rowc[bl];
-                            rb.v = rowv[bl];
-                            rb.one_minus = rowd[bl];
-                            r2 = r2_reference(v[t], ra_r, rb, p.S);
+                    for (int j = 0; j < 3; ++j) {
+                        const int t = ut + j * UNPACK_THREADS;   // 768 tasks: (row, half)
+                        const int row = t >> 1, half = t & 1;
+                        const bool isA = row < BM;
+                        const int r = isA ? row : row - BM;
+                        // packed row r: 64 bytes, 64-byte swizzle (16-byte chunk ^= (r>>1)&3)
+                        const uint8_t *src =
+                            (isA ? pa : pb) + r * 64 + ((sub ^ ((r >> 1) & 3)) << 4);
+                        const uint4 w = *reinterpret_cast<const uint4 *>(src);
+                        uint8_t *dst = (isA ? ua : ub) + r * 128;
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc) {
+                            const int c = half * 4 + cc;
+                            *reinterpret_cast<uint4 *>(dst + ((c ^ (r & 7)) << 4)) =
+                                unpack_chunk(w, c);
                         }
-                        const long long o = (long long)(b - p.out_row0);
-                        p.r2[o * p.ldr + a] = r2;
-                        if (p.counts) p.counts[o * p.ldc + a] = v[t];
                     }
+                    fence_proxy_async_smem();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(smem_u32(&ufull[us]));
+                }
+                if (!ok) break;
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&pempty[ps]));
+            }
+        }
+    } else {
+        // ------------------------------------------------------- epilogue --
+        const int et = tid - FIRST_EPI_WARP * 32;
+        const int q = warp & 3;                  // TMEM lane quarter of this warp
+        bool failed = false;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+            int ta, tb;
+            tl.decode(tile, ta, tb);
+            const int ab = it & 1;
+            // B-row factors of this tile: 2 per thread.
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int bl = et + k * EPI_THREADS;
+                const int b = tb * BN + bl;
+                const uint32_t c = b < p.n ? p.bcB[b] : 0u;
+                rowc[bl] = c;
+                if (MODE == R2_EXACT) {
+                    rowd[bl] = row_exact(c, p.S).inv_var;
+                } else {
+                    const RowRef r = row_ref(c, p.S);
+                    rowv[bl] = r.v;
+                    rowd[bl] = r.one_minus;
                 }
             }
-        } else if (ok && lane == 0) {
-            flag_error(p.status, ST_TIMEOUT_MMA);
+            named_bar_sync(1, EPI_THREADS);
+            // On a failed wait the warp skips the tile but stays in the loop,
+            // so all four epilogue warps keep meeting at the named barrier
+            // (later waits fail fast once the status word is set).
+            bool ready = !failed && mbar_wait(smem_u32(&accfull[ab]), (it >> 1) & 1,
+                                              p.timeout_cycles, p.status);
+            ready = __all_sync(0xffffffffu, ready);
+            if (!ready && !failed) {
+                if (lane == 0) flag_error(p.status, ST_TIMEOUT_MMA);
+                failed = true;
+            }
+            if (ready) {
+                __syncwarp();
+                tc_fence_after();
+                const int a = ta * BM + q * 32 + lane;
+                const bool a_ok = a < p.m;
+                const uint32_t ca = a_ok ? p.bcA[a] : 0u;
+                RowExact ra_e;
+                RowRef ra_r;
+                if (MODE == R2_EXACT) ra_e = row_exact(ca, p.S);
+                else ra_r = row_ref(ca, p.S);
+                const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * BN);
+#pragma unroll 1
+                for (int col0 = 0; col0 < BN; col0 += 32) {
+                    uint32_t v[32];
+                    __syncwarp();
+                    tc_ld_32x32b_x32(tbase + (uint32_t)col0, v);
+#pragma unroll
+                    for (int t = 0; t < 32; ++t) {
+                        const int bl = col0 + t;
+                        const int b = tb * BN + bl;
+                        if (b < p.n && a_ok && (!p.symmetric || a >= b)) {
+                            const uint32_t cnt = v[t] >> COUNT_SHIFT;
+                            float r2;
+                            if (MODE == R2_EXACT) {
+                                RowExact rb;
+                                rb.c = rowc[bl];
+                                rb.inv_var = rowd[bl];
+                                r2 = r2_exact(cnt, ra_e, rb, p.S);
+                            } else {
+                                RowRef rb;
+                                rb.c = rowc[bl];
+                                rb.v = rowv[bl];
+                                rb.one_minus = rowd[bl];
+                                r2 = r2_reference(cnt, ra_r, rb, p.S);
+                            }
+                            const long long o = (long long)(b - p.out_row0);
+                            p.r2[o * p.ldr + a] = r2;
+                            if (p.counts) p.counts[o * p.ldc + a] = cnt;
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&accempty[ab]));
+            }
+            named_bar_sync(1, EPI_THREADS);   // row factors may be rewritten
         }
     }
 
@@ -346,7 +439,7 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
     __syncthreads();
     if (warp == 1) {
         // Every MMA must be complete before TMEM is released.
-        if (!mbar_wait(smem_u32(accf), 0, p.timeout_cycles, nullptr))
+        if (!mbar_wait(smem_u32(mma_done), 0, p.timeout_cycles, nullptr))
             flag_error(p.status, ST_TIMEOUT_MMA);
         __syncwarp();
         tc_fence_after();
@@ -356,6 +449,8 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
     }
 }
 
+int g_sm_count = 0;
+
 template <int MODE>
 cudaError_t launch_mode(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
                         int tiles_b, cudaStream_t st) {
@@ -363,8 +458,23 @@ cudaError_t launch_mode(const CUtensorMap &tmA, const CUtensorMap &tmB, const Ld
     cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     if (e != cudaSuccess) return e;
-    dim3 grid((p.m + BM - 1) / BM, tiles_b);
-    kern<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p);
+    if (g_sm_count == 0) {
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev)) !=
+            cudaSuccess)
+            return e;
+    }
+    // Host-side count of the launch's tiles (same rule as TileList).
+    const long long TA = (p.m + BM - 1) / BM;
+    long long ntiles = 0;
+    for (int t = 0; t < tiles_b; ++t) {
+        const long long lo = p.symmetric ? ((long long)(p.tb0 + t) * BN) / BM : 0;
+        ntiles += TA - lo > 0 ? TA - lo : 0;
+    }
+    if (ntiles == 0) return cudaSuccess;
+    const int grid = (int)(ntiles < g_sm_count ? ntiles : g_sm_count);
+    kern<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p, tiles_b);
     return cudaGetLastError();
 }
 
@@ -373,6 +483,7 @@ cudaError_t launch_mode(const CUtensorMap &tmA, const CUtensorMap &tmB, const Ld
 // Both tensor maps use box_words = PW (64 bytes, 64-byte swizzle); A's box
 // has BM rows, B's BN rows.
 const KernelShape kMmaShape = {BM, BN, PW, BM, BN, 64};
+const int kMmaMaxSamples = (1 << (31 - COUNT_SHIFT)) - 1;
 
 cudaError_t launch_mma(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
                        int tiles_b, int r2_mode, cudaStream_t st) {

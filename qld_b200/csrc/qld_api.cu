@@ -115,9 +115,13 @@ struct Task {
     int K, S, symmetric;
 };
 
-int choose_kernel(qld_ctx *c, const Task &) {
+bool mma_exact_for(const Task &t) { return (long long)t.K * 64 <= kMmaMaxSamples; }
+
+// Per-shape variant: the tensor-core kernel wherever its s32 accumulators
+// stay exact, the popcount kernel otherwise.
+int choose_kernel(qld_ctx *c, const Task &t) {
     (void)c;
-    return QLD_KERNEL_POPC;
+    return mma_exact_for(t) ? QLD_KERNEL_MMA : QLD_KERNEL_POPC;
 }
 
 const KernelShape &shape_of(int variant) {
@@ -129,6 +133,9 @@ const KernelShape &shape_of(int variant) {
 int launch_counts(qld_ctx *c, const Task &t, int b0, int b1, float *r2, long long ldr,
                   uint32_t *cnt, long long ldc, int out_row0, cudaStream_t st) {
     const int variant = c->kernel == QLD_KERNEL_AUTO ? choose_kernel(c, t) : c->kernel;
+    if (variant == QLD_KERNEL_MMA && !mma_exact_for(t))
+        return set_err(c, QLD_ERR_UNSUPPORTED,
+                       "tensor-core kernel needs K*64 <= %d samples (K=%d)", kMmaMaxSamples, t.K);
     const KernelShape &ks = shape_of(variant);
     CUtensorMap tmA, tmB;
     int rc;

@@ -80,13 +80,16 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long lo
                                           const unsigned *status) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
-    unsigned spins = 0;
-    while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > limit) return false;
-        if ((++spins & 1023u) == 0u && status && *((volatile const unsigned *)status) != 0u)
-            return false;
+    // try_wait itself suspends the thread for a while; the clock and the
+    // status word are only looked at every 64 polls to keep spinning warps
+    // off the issue slots the working warps need.
+    for (unsigned spins = 1;; ++spins) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((spins & 63u) == 0u) {
+            if (clock64() - t0 > limit) return false;
+            if (status && *((volatile const unsigned *)status) != 0u) return false;
+        }
     }
-    return true;
 }
 
 __device__ __forceinline__ bool grid_failed(const unsigned *status) {

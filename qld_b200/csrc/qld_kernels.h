@@ -25,7 +25,9 @@ extern const KernelShape kMmaShape;
 cudaError_t launch_popc(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
                         int tiles_b, int r2_mode, cudaStream_t st);
 
-// Variant (b): p.nk unused (the kernel derives its stages from K).
+// Variant (b): p.nk unused (the kernel derives its stages from K).  Exact
+// while K * 64 <= kMmaMaxSamples.
+extern const int kMmaMaxSamples;
 cudaError_t launch_mma(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
                        int tiles_b, int r2_mode, cudaStream_t st);
 
