@@ -75,7 +75,10 @@ def make_table(name, device, seed_offset=0):
 # ------------------------------------------------------------------ clocks --
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi samples every 50 ms from before warm-up to after the timed
+    region; summary() keeps the samples whose timestamps fall inside
+    [mark_start(), mark_end()] (all samples if none do)."""
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -83,6 +86,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -90,14 +94,24 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            deadline = time.time() + 10
+            while time.time() < deadline and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)
         except FileNotFoundError:
             self.proc = None
         return self
 
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+
     def __exit__(self, *exc):
         if self.proc:
+            time.sleep(0.1)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -105,22 +119,33 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        import datetime
         rows = []
         if self.path and os.path.exists(self.path):
             for line in open(self.path):
                 parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
+                if len(parts) >= 10:
                     rows.append(parts)
             os.unlink(self.path)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+
+        def ts(r):
+            try:
+                return datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                return None
+        inside = [r for r in rows if self.t0 and self.t1 and ts(r) is not None
+                  and self.t0 - 0.05 <= ts(r) <= self.t1 + 0.05]
+        use = inside or rows
+        sm = [float(r[2]) for r in use if r[2].replace(".", "").isdigit()]
+        smax = [float(r[3]) for r in use if r[3].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        reasons = sorted({names[k] for r in use for k in range(4) if r[6 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(use),
+                "window": "timed region" if inside else "whole run (no sample inside the region)"}
 
 
 # ------------------------------------------------------------ reference CPU --
@@ -244,6 +269,7 @@ def ours_arm(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local_rank) as clk:
+        clk.mark_start()
         torch.cuda.nvtx.range_push("qld_timed")
         for i in range(args.steps):
             flush.zero_()
@@ -253,6 +279,7 @@ def ours_arm(args, rank, world, local_rank):
         torch.cuda.nvtx.range_pop()
         ctx.sync(stream=st)
         torch.cuda.synchronize()
+        clk.mark_end()
     if world > 1:
         dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in ev]

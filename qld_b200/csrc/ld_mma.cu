@@ -18,10 +18,10 @@
 //                samples) 4 MMAs of 128 x 256 x 32 into the tile's
 //                accumulator, tcgen05.commit frees the stage; after the
 //                tile, a commit hands the accumulator to the epilogue.
-//   warps 2-9    unpack: each packed stage gives 4 unpacked stages of
+//   warps 2-13   unpack: each packed stage gives 4 unpacked stages of
 //                128 + 256 rows x 128 bytes in the canonical K-major
 //                128-byte-swizzled layout the MMA descriptors name.
-//   warps 10-13  epilogue: tcgen05.ld of the finished accumulator (warp w
+//   warps 14-17  epilogue: tcgen05.ld of the finished accumulator (warp w
 //                reads TMEM lanes 32*(w%4)..), r^2, coalesced stores
 //                (32 lanes = 32 consecutive A rows), then release the
 //                accumulator -- overlapping the next tile's MMAs.
@@ -31,7 +31,9 @@
 // words ((w0 << (7-c)) & 0x80808080, ..., (w3 << (7-c)) & 0x80808080), i.e.
 // byte b of its word j carries bit c + 8b of w_j.  This is a fixed
 // permutation of the 128 samples, the same for A and B, so the contraction
-// is unchanged: one shift (IMAD pipe) and one AND (ALU pipe) per 4 bytes.
+// is unchanged: one shift and one AND per 4 bytes.  The shift is written as
+// a multiply by a per-thread power of two held in a register, so it runs on
+// the IMAD pipe and leaves the ALU pipe to the ANDs.
 #include "qld_device.cuh"
 #include "qld_kernels.h"
 
@@ -48,13 +50,15 @@ constexpr int PA_BYTES = BM * PW * 8;    // 8 KB
 constexpr int PB_BYTES = BN * PW * 8;    // 16 KB
 constexpr int UA_BYTES = BM * 128;       // 16 KB
 constexpr int UB_BYTES = BN * 128;       // 32 KB
-constexpr int UNPACK_WARPS = 8;
+constexpr int UNPACK_WARPS = 12;
 constexpr int UNPACK_THREADS = UNPACK_WARPS * 32;
 constexpr int EPI_WARPS = 4;
 constexpr int EPI_THREADS = EPI_WARPS * 32;
 constexpr int FIRST_UNPACK_WARP = 2;
 constexpr int FIRST_EPI_WARP = FIRST_UNPACK_WARP + UNPACK_WARPS;
-constexpr int THREADS = (FIRST_EPI_WARP + EPI_WARPS) * 32;   // 448
+constexpr int THREADS = (FIRST_EPI_WARP + EPI_WARPS) * 32;   // 576
+constexpr int TASKS = 2 * (BM + BN) / UNPACK_THREADS;           // (row, half) tasks per thread
+static_assert(TASKS * UNPACK_THREADS == 2 * (BM + BN), "unpack tasks must divide evenly");
 constexpr uint32_t TMEM_COLS = 512;                          // two accumulators
 constexpr int COUNT_SHIFT = 14;                              // log2(0x80 * 0x80)
 
@@ -134,11 +138,28 @@ __device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-__device__ __forceinline__ uint4 unpack_chunk(const uint4 &w, int c) {
-    const uint32_t M = 0x80808080u;
-    const int s = 7 - c;
-    return make_uint4((w.x << s) & M, (w.y << s) & M, (w.z << s) & M, (w.w << s) & M);
+__device__ __forceinline__ uint32_t imul(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("mul.lo.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
 }
+
+// chunk = ((w_j << s) & 0x80808080)_j with the shift as a multiply by 2^s.
+__device__ __forceinline__ uint4 unpack_chunk(const uint4 &w, uint32_t pow2) {
+    const uint32_t M = 0x80808080u;
+    return make_uint4(imul(w.x, pow2) & M, imul(w.y, pow2) & M, imul(w.z, pow2) & M,
+                      imul(w.w, pow2) & M);
+}
+
+// One unpack task: half of one packed row (4 of its 8 output chunks).
+struct UnpackTask {
+    uint32_t src;        // smem offset of the row in a packed stage (before stage base)
+    uint32_t xr;         // 64-byte swizzle phase of the packed row
+    uint32_t dst;        // smem offset of the row in an unpacked stage
+    uint32_t is_a;
+    uint32_t chunk_off[4];
+    uint32_t pow2[4];
+};
 
 // Tile list of one launch: B tile rows tb in [tb0, tb0 + tiles_b), and in
 // each the A tiles ta in [ta_lo(tb), TA) -- all of them for two regions,
@@ -296,6 +317,24 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
     } else if (warp < FIRST_EPI_WARP) {
         // --------------------------------------------------------- unpack --
         const int ut = tid - FIRST_UNPACK_WARP * 32;
+        UnpackTask task[TASKS];
+#pragma unroll
+        for (int j = 0; j < TASKS; ++j) {
+            const int t = ut + j * UNPACK_THREADS;   // (row, half) over 128 A + 256 B rows
+            const int row = t >> 1, half = t & 1;
+            const bool isA = row < BM;
+            const int r = isA ? row : row - BM;
+            task[j].is_a = isA;
+            task[j].src = (uint32_t)(r * 64);
+            task[j].xr = (uint32_t)((r >> 1) & 3);
+            task[j].dst = (uint32_t)(r * 128);
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) {
+                const int c = half * 4 + cc;
+                task[j].chunk_off[cc] = (uint32_t)((c ^ (r & 7)) << 4);
+                task[j].pow2[cc] = 1u << (7 - c);
+            }
+        }
         int gp = 0, gu = 0;
         bool ok = true;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
@@ -323,23 +362,18 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
                     }
                     uint8_t *ua = smem + OFF_UA + us * UA_BYTES;
                     uint8_t *ub = smem + OFF_UB + us * UB_BYTES;
+                    uint4 w[TASKS];
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        const int t = ut + j * UNPACK_THREADS;   // 768 tasks: (row, half)
-                        const int row = t >> 1, half = t & 1;
-                        const bool isA = row < BM;
-                        const int r = isA ? row : row - BM;
-                        // packed row r: 64 bytes, 64-byte swizzle (16-byte chunk ^= (r>>1)&3)
-                        const uint8_t *src =
-                            (isA ? pa : pb) + r * 64 + ((sub ^ ((r >> 1) & 3)) << 4);
-                        const uint4 w = *reinterpret_cast<const uint4 *>(src);
-                        uint8_t *dst = (isA ? ua : ub) + r * 128;
+                    for (int j = 0; j < TASKS; ++j)
+                        w[j] = *reinterpret_cast<const uint4 *>(
+                            (task[j].is_a ? pa : pb) + task[j].src + ((sub ^ task[j].xr) << 4));
 #pragma unroll
-                        for (int cc = 0; cc < 4; ++cc) {
-                            const int c = half * 4 + cc;
-                            *reinterpret_cast<uint4 *>(dst + ((c ^ (r & 7)) << 4)) =
-                                unpack_chunk(w, c);
-                        }
+                    for (int j = 0; j < TASKS; ++j) {
+                        uint8_t *dst = (task[j].is_a ? ua : ub) + task[j].dst;
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc)
+                            *reinterpret_cast<uint4 *>(dst + task[j].chunk_off[cc]) =
+                                unpack_chunk(w[j], task[j].pow2[cc]);
                     }
                     fence_proxy_async_smem();
                     __syncwarp();
