@@ -69,6 +69,7 @@ extern "C" {
 #define QLD_OPT_R2_MODE   2  /* QLD_R2_*                                          */
 #define QLD_OPT_PROFILE   3  /* 1: time every counts-kernel launch with events    */
 #define QLD_OPT_BAND_ROWS 4  /* B rows per streamed output band (host-buffer calls) */
+#define QLD_OPT_MMA_TILE  5  /* QLD_KERNEL_MMA output tile rows: 128, 256, 0 = per shape */
 
 typedef struct qld_ctx qld_ctx;
 

@@ -41,6 +41,7 @@ struct qld_ctx {
     int r2_mode = QLD_R2_EXACT;
     int profile = 0;
     int band_rows = 4096;
+    int mma_tile = 0;                 // 0: per shape, else 128 or 256
     long long timeout_cycles = 4000000000LL;  // ~2 s at boost clock
     DevBuf dA, dB, dbcA, dbcB, dOut[2], dCnt[2];
     cudaEvent_t ev_band[2] = {nullptr, nullptr};
@@ -124,8 +125,27 @@ int choose_kernel(qld_ctx *c, const Task &t) {
     return mma_exact_for(t) ? QLD_KERNEL_MMA : QLD_KERNEL_POPC;
 }
 
-const KernelShape &shape_of(int variant) {
-    return variant == QLD_KERNEL_MMA ? kMmaShape : kPopcShape;
+long long tile_count(const Task &t, int bm, int bn, int b0, int b1) {
+    const long long TA = (t.m + bm - 1) / bm;
+    long long n = 0;
+    for (int tb = b0 / bn; tb * bn < b1; ++tb) {
+        const long long lo = t.symmetric ? ((long long)tb * bn) / bm : 0;
+        n += TA - lo > 0 ? TA - lo : 0;
+    }
+    return n;
+}
+
+// The 256 x 256 tile unpacks 2/3 of the bytes per multiply-accumulate but
+// cannot overlap its epilogue; it pays off once there are enough tiles to
+// keep every SM busy for several rounds.
+const KernelShape &mma_shape(qld_ctx *c, const Task &t, int b0, int b1) {
+    if (c->mma_tile == 128) return kMmaShape;
+    if (c->mma_tile == 256) return kMmaWideShape;
+    return tile_count(t, 256, 256, b0, b1) >= 4LL * c->sm_count ? kMmaWideShape : kMmaShape;
+}
+
+const KernelShape &shape_of(qld_ctx *c, int variant, const Task &t, int b0, int b1) {
+    return variant == QLD_KERNEL_MMA ? mma_shape(c, t, b0, b1) : kPopcShape;
 }
 
 // Launch the counts kernel over B rows [b0, b1) (b0 a multiple of 256),
@@ -136,7 +156,7 @@ int launch_counts(qld_ctx *c, const Task &t, int b0, int b1, float *r2, long lon
     if (variant == QLD_KERNEL_MMA && !mma_exact_for(t))
         return set_err(c, QLD_ERR_UNSUPPORTED,
                        "tensor-core kernel needs K*64 <= %d samples (K=%d)", kMmaMaxSamples, t.K);
-    const KernelShape &ks = shape_of(variant);
+    const KernelShape &ks = shape_of(c, variant, t, b0, b1);
     CUtensorMap tmA, tmB;
     int rc;
     if ((rc = make_tmap(c, &tmA, t.A, t.m, t.K, t.lda, ks.box_words, ks.box_rows_a, ks.swizzle)) ||
@@ -168,8 +188,10 @@ int launch_counts(qld_ctx *c, const Task &t, int b0, int b1, float *r2, long lon
             ++c->prof_used;
             CUDA_TRY(c, cudaEventRecord(e0, st));
         }
-        cudaError_t e = variant == QLD_KERNEL_MMA ? launch_mma(tmA, tmB, p, nb, c->r2_mode, st)
-                                                  : launch_popc(tmA, tmB, p, nb, c->r2_mode, st);
+        cudaError_t e =
+            variant != QLD_KERNEL_MMA ? launch_popc(tmA, tmB, p, nb, c->r2_mode, st)
+            : &ks == &kMmaWideShape   ? launch_mma_wide(tmA, tmB, p, nb, c->r2_mode, st)
+                                      : launch_mma(tmA, tmB, p, nb, c->r2_mode, st);
         if (e != cudaSuccess)
             return set_err(c, QLD_ERR_CUDA, "counts kernel launch failed: %s", cudaGetErrorString(e));
         if (c->profile) CUDA_TRY(c, cudaEventRecord(e1, st));
@@ -302,6 +324,11 @@ int qld_cuda_set_option(qld_ctx *c, int option, long long value) {
         return QLD_OK;
     case QLD_OPT_PROFILE:
         c->profile = value ? 1 : 0;
+        return QLD_OK;
+    case QLD_OPT_MMA_TILE:
+        if (value != 0 && value != 128 && value != 256)
+            return set_err(c, QLD_ERR_INVALID, "MMA tile rows must be 0, 128 or 256");
+        c->mma_tile = (int)value;
         return QLD_OK;
     case QLD_OPT_BAND_ROWS:
         if (value < 256 || value > (1 << 24))

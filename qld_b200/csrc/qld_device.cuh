@@ -60,14 +60,18 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t byt
                  : "memory");
 }
 
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+// try_wait with a suspend-time hint: the thread is parked in hardware until
+// the phase completes or ~hint_ns pass, so waiting warps do not spin on the
+// issue slots.
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity,
+                                              uint32_t hint_ns = 20000u) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "r"(hint_ns)
         : "memory");
     return ok != 0;
 }
@@ -80,15 +84,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long lo
                                           const unsigned *status) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
-    // try_wait itself suspends the thread for a while; the clock and the
-    // status word are only looked at every 64 polls to keep spinning warps
-    // off the issue slots the working warps need.
-    for (unsigned spins = 1;; ++spins) {
+    // Each try_wait parks the thread for up to its hint, so the clock and the
+    // status word are looked at on every return.
+    for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((spins & 63u) == 0u) {
-            if (clock64() - t0 > limit) return false;
-            if (status && *((volatile const unsigned *)status) != 0u) return false;
-        }
+        if (clock64() - t0 > limit) return false;
+        if (status && *((volatile const unsigned *)status) != 0u) return false;
     }
 }
 

@@ -19,7 +19,8 @@ struct KernelShape {
 };
 
 extern const KernelShape kPopcShape;
-extern const KernelShape kMmaShape;
+extern const KernelShape kMmaShape;       // 128 x 256 tiles, overlapped epilogue
+extern const KernelShape kMmaWideShape;   // 256 x 256 tiles
 
 // Variant (a): tiles_b tile rows starting at p.tb0; p.nk = ceil(K / box_words).
 cudaError_t launch_popc(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
@@ -30,5 +31,7 @@ cudaError_t launch_popc(const CUtensorMap &tmA, const CUtensorMap &tmB, const Ld
 extern const int kMmaMaxSamples;
 cudaError_t launch_mma(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
                        int tiles_b, int r2_mode, cudaStream_t st);
+cudaError_t launch_mma_wide(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
+                            int tiles_b, int r2_mode, cudaStream_t st);
 
 }  // namespace qld

@@ -1,0 +1,136 @@
+// tcgen05.cuh -- building blocks of the tensor-core counts kernels:
+// UMMA shared-memory descriptors, tcgen05 wrappers, the bit -> byte unpack
+// and the static tile list of a launch.
+#pragma once
+
+#include "qld_device.cuh"
+
+namespace qld {
+namespace tc {
+
+// Instruction descriptor, kind::i8: D = s32 (bits 4-5 = 2), A and B unsigned
+// 8-bit (bits 7-9, 10-12 = 0), both K-major (bits 15, 16 = 0),
+// N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t idesc_i8(int M, int N) {
+    return (2u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+constexpr int COUNT_SHIFT = 14;   // log2(0x80 * 0x80): accumulators hold 2^14 * count
+
+// Shared-memory matrix descriptor for a K-major operand in the 128-byte
+// swizzled canonical layout: rows of 128 bytes, 8-row atoms 1024 bytes apart
+// (stride byte offset), fixed-constant bit 46, swizzle mode 2 (128 B).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1u << 16;                       // leading byte offset (unused, 16 B)
+    d |= (uint64_t)(1024u >> 4) << 32;             // stride byte offset
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)2u << 61;
+    return d;
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_ld_32x32b_x32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+          "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+          "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+          "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+__device__ __forceinline__ uint32_t imul(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("mul.lo.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+
+// chunk = ((w_j << s) & 0x80808080)_j with the shift as a multiply by 2^s.
+__device__ __forceinline__ uint4 unpack_chunk(const uint4 &w, uint32_t pow2) {
+    const uint32_t M = 0x80808080u;
+    return make_uint4(imul(w.x, pow2) & M, imul(w.y, pow2) & M, imul(w.z, pow2) & M,
+                      imul(w.w, pow2) & M);
+}
+
+// One unpack task: half of one packed row (4 of its 8 output chunks).
+struct UnpackTask {
+    uint32_t src;        // smem offset of the row in a packed stage (before stage base)
+    uint32_t xr;         // 64-byte swizzle phase of the packed row
+    uint32_t dst;        // smem offset of the row in an unpacked stage
+    uint32_t is_a;
+    uint32_t chunk_off[4];
+    uint32_t pow2[4];
+};
+
+// Tile list of one launch: B tile rows tb in [tb0, tb0 + tiles_b), and in
+// each the A tiles ta in [ta_lo(tb), TA) -- all of them for two regions,
+// those reaching the diagonal (a >= b somewhere) for a single region.
+// Tiles are numbered B-tile-row first.
+template <int BM, int BN>
+struct TileList {
+    int TA, tb0, tiles_b, symmetric;
+    __device__ __forceinline__ int ta_lo(int tb) const {
+        return symmetric ? (tb * BN) / BM : 0;
+    }
+    __device__ __forceinline__ int count() const {
+        int n = 0;
+        for (int t = 0; t < tiles_b; ++t) {
+            const int c = TA - ta_lo(tb0 + t);
+            n += c > 0 ? c : 0;
+        }
+        return n;
+    }
+    __device__ __forceinline__ void decode(int idx, int &ta, int &tb) const {
+        for (int t = 0; t < tiles_b; ++t) {
+            const int lo = ta_lo(tb0 + t);
+            const int c = TA - lo > 0 ? TA - lo : 0;
+            if (idx < c) {
+                ta = lo + idx;
+                tb = tb0 + t;
+                return;
+            }
+            idx -= c;
+        }
+        ta = tb = -1;
+    }
+};
+
+
+}  // namespace tc
+}  // namespace qld

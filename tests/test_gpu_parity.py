@@ -15,11 +15,17 @@ from qld_b200 import api, synth
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = [api.KERNEL_POPC, api.KERNEL_MMA]
+KERNELS = ["popc", "mma128", "mma256"]
+
+
+def set_kernel(ctx, name):
+    ctx.set_option(api.OPT_KERNEL, api.KERNEL_POPC if name == "popc" else api.KERNEL_MMA)
+    ctx.set_option(api.OPT_MMA_TILE, {"popc": 0, "mma128": 128, "mma256": 256}[name])
+    assert ctx.stats(reset=True) is not None
 
 
 def _check_task(ctx, A, B, S, symmetric, kernel):
-    ctx.set_option(api.OPT_KERNEL, kernel)
+    set_kernel(ctx, kernel)
     bcA = oracle.bitcounts(A)
     Bx = A if symmetric else B
     bcB = oracle.bitcounts(Bx)
@@ -72,7 +78,7 @@ def test_random_shapes(gpu_ctx, kernel, m, n, N, sym):
 @pytest.mark.parametrize("name", golden_names())
 def test_golden(gpu_ctx, kernel, name):
     g = load_golden(name)
-    gpu_ctx.set_option(api.OPT_KERNEL, kernel)
+    set_kernel(gpu_ctx, kernel)
     sym = g["symmetric"]
     mask = lower_mask(*g["counts"].shape) if sym else np.ones(g["counts"].shape, bool)
     gpu_ctx.set_option(api.OPT_R2_MODE, api.R2_REFERENCE)
@@ -92,7 +98,7 @@ def test_golden(gpu_ctx, kernel, name):
 @pytest.mark.parametrize("kernel", KERNELS)
 def test_device_resident_call(gpu_ctx, kernel):
     """qld_cuda_ld_device on torch buffers with padded pitches."""
-    gpu_ctx.set_option(api.OPT_KERNEL, kernel)
+    set_kernel(gpu_ctx, kernel)
     m, n, N = 700, 300, 3000
     t, _ = synth.all_pairs_workload(m=m + n, n=N, seed=4)
     K = t.shape[1]
@@ -124,7 +130,7 @@ def test_device_resident_call(gpu_ctx, kernel):
 @pytest.mark.parametrize("kernel", KERNELS)
 def test_streamed_bands(gpu_ctx, kernel):
     """Host-buffer call with several output bands (band rows < n)."""
-    gpu_ctx.set_option(api.OPT_KERNEL, kernel)
+    set_kernel(gpu_ctx, kernel)
     gpu_ctx.set_option(api.OPT_BAND_ROWS, 256)
     try:
         T1 = synth.all_pairs_workload(m=1100, n=1500, seed=9)[0].numpy().view(np.uint64)
@@ -138,6 +144,7 @@ def test_streamed_bands(gpu_ctx, kernel):
 
 
 def test_pinned_buffers(gpu_ctx):
+    set_kernel(gpu_ctx, "mma128")
     m, N = 900, 5000
     t, _ = synth.all_pairs_workload(m=m, n=N, seed=21)
     A = gpu_ctx.pinned_empty(t.shape, np.uint64)
@@ -159,3 +166,27 @@ def test_invalid_arguments_return_codes(gpu_ctx):
     with pytest.raises(api.QldError) as e:
         gpu_ctx.set_option(api.OPT_KERNEL, 99)
     assert e.value.code == api.ERR_INVALID
+    with pytest.raises(api.QldError) as e:
+        gpu_ctx.set_option(api.OPT_MMA_TILE, 64)
+    assert e.value.code == api.ERR_INVALID
+
+
+def test_tensor_core_limit_routes_to_popc(gpu_ctx):
+    """K * 64 above 131071 samples: AUTO takes the popcount kernel (exact),
+    an explicit tensor-core request is refused with UNSUPPORTED."""
+    N = 131_200
+    t, _ = synth.all_pairs_workload(m=40, n=N, seed=31)
+    A = t.numpy().view(np.uint64)
+    bc = oracle.bitcounts(A)
+    gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
+    gpu_ctx.set_option(api.OPT_MMA_TILE, 0)
+    gpu_ctx.stats(reset=True)
+    r2, cnt = gpu_ctx.ld(A, bc, S=N, counts=True)
+    assert gpu_ctx.stats().last_kernel == api.KERNEL_POPC
+    mask = lower_mask(40, 40)
+    assert np.array_equal(cnt[mask], oracle.counts(A)[mask])
+    gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_MMA)
+    with pytest.raises(api.QldError) as e:
+        gpu_ctx.ld(A, bc, S=N)
+    assert e.value.code == api.ERR_UNSUPPORTED
+    gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
