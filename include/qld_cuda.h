@@ -54,6 +54,7 @@ extern "C" {
 #define QLD_ERR_TIMEOUT     -5  /* a kernel's bounded wait gave up               */
 #define QLD_ERR_BUSY        -6  /* admission refused (serving)                   */
 #define QLD_ERR_UNSUPPORTED -7  /* shape/option not supported by this kernel     */
+#define QLD_ERR_TOO_LARGE   -8  /* task does not fit qld_cuda_ld_noalloc's scratch */
 
 /* r^2 evaluation modes */
 #define QLD_R2_EXACT      0
@@ -135,6 +136,30 @@ typedef struct qld_stats {
 } qld_stats;
 
 int qld_cuda_get_stats(qld_ctx *ctx, qld_stats *out, int reset);
+
+/*
+ * One LD task from host buffers that allocates nothing.  For callers that
+ * cannot call cudaMalloc: a host program whose device memory is reserved
+ * up front by another component (a pool or framework that owns the GPU's
+ * memory), or a plug-in loaded into one.  Same arguments and result as
+ * qld_cuda_ld() with r^2 in QLD_R2_EXACT mode and no counts output, on the
+ * current device and the given stream (a cudaStream_t; NULL = the legacy
+ * default stream); synchronous.  No context, stream, event or buffer is
+ * created: all device memory it uses is one static scratch array of
+ * QLD_NOALLOC_SCRATCH_BYTES that stays resident on every GPU where this code
+ * is loaded until the process exits.  The first call on a device sets up the
+ * array's device address; make that first call before any stream capture.
+ * Limit: 256 + bit counts + the packed tables (rows x K rounded up to an
+ * even word count x 8 bytes, A and, for two regions, B) plus at least one
+ * r^2 band (min(n, 256) rows x m x 4 bytes) must fit in the scratch; larger
+ * tasks return QLD_ERR_TOO_LARGE.  Calls share the scratch, so calls that
+ * overlap on the GPU (two streams or two threads) race: serialize them.
+ * No counterpart in the reference.
+ */
+#define QLD_NOALLOC_SCRATCH_BYTES (16u << 20)
+int qld_cuda_ld_noalloc(const uint64_t *A, const uint32_t *bcA, int m,
+                        const uint64_t *B, const uint32_t *bcB, int n,
+                        int K, int S, int symmetric, float *r2_out, void *stream);
 
 /* Measured peak of the popcount pipe on this device, in bit-ops/s (one POPC
  * of an ANDed 32-bit word = 32 bit-ops): the compute roofline of the
