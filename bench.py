@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mma-tile", type=int, default=0, choices=[0, 128, 256],
+                    help="tensor-core tile rows (0: per shape)")
     ap.add_argument("--snps", type=int, default=0,
                     help="use only the first N SNPs of the workload (profiling captures)")
     return ap.parse_args()
@@ -248,6 +250,7 @@ def ours_arm(args, rank, world, local_rank):
     ctx = api.Context(local_rank)
     kern = {"auto": api.KERNEL_AUTO, "popc": api.KERNEL_POPC, "mma": api.KERNEL_MMA}[args.kernel]
     ctx.set_option(api.OPT_KERNEL, kern)
+    ctx.set_option(api.OPT_MMA_TILE, args.mma_tile)
     ctx.set_option(api.OPT_PROFILE, 1)
     # A dedicated stream: torch's default stream is the legacy NULL stream,
     # which the C ABI reads as "the context's own stream".
