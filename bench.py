@@ -46,7 +46,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single_region", choices=["single_region", "all_pairs"])
+    ap.add_argument("--workload", default="single_region",
+                    choices=["single_region", "all_pairs", "batched"])
+    ap.add_argument("--jobs", type=int, default=4096, help="batched workload: number of tasks")
     ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -369,6 +371,101 @@ def ours_arm(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def make_batched_jobs(njobs, dev, seed=0):
+    """Batched workload: njobs independent tasks; SNPs per side log-uniform in
+    [64, 8192], samples log-uniform in [1000, 50000], per-SNP frequencies
+    Beta(0.5, 0.5), iid genotypes; even tasks single region (triangle), odd
+    tasks two regions (rectangle)."""
+    import numpy as np
+    import torch
+
+    from qld_b200 import synth
+    rng = np.random.default_rng(seed)
+    Ms = synth.log_uniform_ints(njobs, 64, 8192, rng)
+    Ns = synth.log_uniform_ints(njobs, 64, 8192, rng)
+    Ss = synth.log_uniform_ints(njobs, 1000, 50000, rng)
+    jobs, pairs, bitops = [], 0, 0
+    for j in range(njobs):
+        sym = j % 2 == 0
+        m = int(Ms[j])
+        n = m if sym else int(Ns[j])
+        S = int(Ss[j])
+        rows = m if sym else m + n
+        f = torch.from_numpy(rng.beta(0.5, 0.5, rows).astype(np.float32))
+        T = synth.iid_table(rows, S, f, seed * 100003 + j, device=dev, chunk=2048)
+        K = T.shape[1]
+        lda = K + (K & 1)
+        Tp = torch.zeros(rows, lda, dtype=torch.int64, device=dev)
+        Tp[:, :K] = T
+        del T
+        bc = synth.popcount_rows(Tp).to(torch.int32)
+        A, bcA = Tp[:m], bc[:m]
+        B, bcB = (A, bcA) if sym else (Tp[m:], bc[m:])
+        r2 = torch.empty(n, m, dtype=torch.float32, device=dev)
+        jobs.append(dict(A=A, bcA=bcA, m=m, lda=lda, B=B, bcB=bcB, n=n, ldb=lda, K=K, S=S,
+                         symmetric=sym, r2=r2, ldr=m))
+        p = m * (m - 1) // 2 if sym else m * n
+        pairs += p
+        bitops += p * 64 * K
+    return jobs, pairs, bitops
+
+
+def batched_arm(args, rank, world, local_rank):
+    import numpy as np  # noqa: F401
+    import torch
+
+    from qld_b200 import api
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    jobs, pairs, bitops = make_batched_jobs(args.jobs, dev, seed=rank)
+    ctx = api.Context(local_rank)
+    ctx.set_option(api.OPT_PROFILE, 1)
+    st = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(st)
+
+    def batched():
+        ctx.ld_batch(jobs, stream=st)
+
+    def plain():
+        for j in jobs:
+            ctx.ld_device(j["A"], j["bcA"], j["m"], j["lda"], j["B"], j["bcB"], j["n"],
+                          j["ldb"], j["K"], j["S"], j["symmetric"], j["r2"], j["ldr"], stream=st)
+
+    res = {}
+    for name, fn in (("batched", batched), ("plain", plain)):
+        for _ in range(args.warmup):
+            fn()
+        ctx.sync(stream=st)
+        ctx.stats(reset=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            fn()
+        e1.record(st)
+        ctx.sync(stream=st)
+        torch.cuda.synchronize()
+        res[name] = (e0.elapsed_time(e1) / args.steps, ctx.stats(reset=True))
+    ms_b, st_b = res["batched"]
+    ms_p, st_p = res["plain"]
+    line = {"metric": METRIC + ", batched tasks", "value": pairs / (ms_b * 1e-3),
+            "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_b, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64 popcount / f32 r2", "data": "synthetic",
+            "config": {"workload": f"batched_{args.jobs}_tasks", "snps_per_side": "logU(64,8192)",
+                       "samples": "logU(1000,50000)", "freq": "Beta(0.5,0.5)",
+                       "half": "single region (triangle) / two regions (rectangle)",
+                       "pairs_per_step": pairs, "bitops_per_step": bitops},
+            "bitops_per_s": bitops / (ms_b * 1e-3),
+            "gpu_launches": st_b.kernel_launches // max(1, args.steps),
+            "plain": {"value": pairs / (ms_p * 1e-3), "unit": "pairs/s", "ms_per_step": ms_p,
+                      "launches_per_step": st_p.kernel_launches // max(1, args.steps)},
+            "speedup_vs_plain": ms_p / ms_b}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -385,7 +482,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        ours_arm(args, rank, world, local_rank)
+        if args.workload == "batched":
+            batched_arm(args, rank, world, local_rank)
+        else:
+            ours_arm(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

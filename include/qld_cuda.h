@@ -120,6 +120,19 @@ typedef struct qld_ld_args {
 int qld_cuda_ld_device(qld_ctx *ctx, const qld_ld_args *args, void *stream);
 int qld_cuda_sync(qld_ctx *ctx, void *stream);
 
+/*
+ * Many independent tasks (region pairs of any SNP and sample counts, single
+ * or two-region) in ONE persistent launch: every output tile of every task is
+ * a work item taken from a device work queue by the SMs as they free up.
+ * Same per-task contract as qld_cuda_ld_device(); asynchronous on `stream`,
+ * collect with qld_cuda_sync().  The tasks of one call must not overlap in
+ * their outputs.  A task needs K * 64 <= 131,071 samples (the tensor-core
+ * accumulators' exact range), else QLD_ERR_UNSUPPORTED.  qLD runs such task
+ * lists one task at a time (-inputList: src/correlator/src/input_list.c:205-323,
+ * correlate_function.c:59-83); this is their batched replacement.
+ */
+int qld_cuda_ld_batch(qld_ctx *ctx, const qld_ld_args *jobs, int njobs, void *stream);
+
 /* Pinned host memory for tables and results (the -cuda reader allocates its
  * tables here so the host<->device copies run asynchronously). */
 int qld_cuda_host_alloc(qld_ctx *ctx, size_t bytes, void **ptr);

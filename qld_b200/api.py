@@ -31,7 +31,8 @@ OPT_KERNEL, OPT_R2_MODE, OPT_PROFILE, OPT_BAND_ROWS, OPT_MMA_TILE = 1, 2, 3, 4, 
 
 EXPORTED = (
     "qld_cuda_init", "qld_cuda_release", "qld_cuda_last_error", "qld_cuda_set_option",
-    "qld_cuda_ld", "qld_cuda_ld_device", "qld_cuda_sync", "qld_cuda_host_alloc",
+    "qld_cuda_ld", "qld_cuda_ld_device", "qld_cuda_ld_batch", "qld_cuda_sync",
+    "qld_cuda_host_alloc",
     "qld_cuda_host_free", "qld_cuda_get_stats", "qld_cuda_measure_popc_peak",
 )
 
@@ -84,6 +85,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.qld_cuda_set_option.argtypes = [vp, i, ll]
     lib.qld_cuda_ld.argtypes = [vp, vp, vp, i, vp, vp, i, i, i, i, vp, vp]
     lib.qld_cuda_ld_device.argtypes = [vp, ct.POINTER(_LdArgs), vp]
+    lib.qld_cuda_ld_batch.argtypes = [vp, ct.POINTER(_LdArgs), i, vp]
     lib.qld_cuda_sync.argtypes = [vp, vp]
     lib.qld_cuda_host_alloc.argtypes = [vp, ct.c_size_t, ct.POINTER(vp)]
     lib.qld_cuda_host_free.argtypes = [vp, vp]
@@ -201,6 +203,19 @@ class Context:
         a = _LdArgs(_p(A), _p(bcA), int(m), int(lda), _p(B), _p(bcB), int(n), int(ldb), int(K),
                     int(S), int(bool(symmetric)), _p(r2), int(ldr), _p(counts), int(ldc))
         self._check(self.lib.qld_cuda_ld_device(self.h, ct.byref(a), _stream(stream)))
+
+    def ld_batch(self, jobs, stream=None):
+        """Enqueue many tasks in one launch.  `jobs`: sequence of dicts with
+        the ld_device keyword names (A, bcA, m, lda, B, bcB, n, ldb, K, S,
+        symmetric, r2, ldr, counts=None, ldc=0)."""
+        arr = (_LdArgs * len(jobs))()
+        for i, j in enumerate(jobs):
+            arr[i] = _LdArgs(_p(j["A"]), _p(j["bcA"]), int(j["m"]), int(j["lda"]),
+                             _p(j.get("B")), _p(j.get("bcB")), int(j.get("n", j["m"])),
+                             int(j.get("ldb", j["lda"])), int(j["K"]), int(j["S"]),
+                             int(bool(j["symmetric"])), _p(j["r2"]), int(j["ldr"]),
+                             _p(j.get("counts")), int(j.get("ldc", 0)))
+        self._check(self.lib.qld_cuda_ld_batch(self.h, arr, len(jobs), _stream(stream)))
 
     def sync(self, stream=None):
         self._check(self.lib.qld_cuda_sync(self.h, _stream(stream)))

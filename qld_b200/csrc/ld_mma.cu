@@ -34,6 +34,7 @@
 // is unchanged: one shift and one AND per 4 bytes.  The shift is written as
 // a multiply by a per-thread power of two held in a register, so it runs on
 // the IMAD pipe and leaves the ALU pipe to the ANDs.
+#include "epilogue.cuh"
 #include "qld_kernels.h"
 #include "tcgen05.cuh"
 
@@ -69,7 +70,7 @@ constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
 constexpr int OFF_PA = OFF_UB + UST * UB_BYTES;
 constexpr int OFF_PB = OFF_PA + PST * PA_BYTES;
 constexpr int OFF_ROWS = OFF_PB + PST * PB_BYTES;            // per-B-row epilogue factors
-constexpr int ROWS_BYTES = BN * (8 + 4 + 4);
+constexpr int ROWS_BYTES = BN * epi::COL_BYTES;
 constexpr int OFF_BAR = OFF_ROWS + ROWS_BYTES;
 constexpr int NBARS = 2 * PST + 2 * UST + 2 + 2 + 1;
 constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
@@ -92,9 +93,7 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
     uint64_t *accempty = accfull + 2;
     uint64_t *mma_done = accempty + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + OFF_TMEM);
-    double *rowd = reinterpret_cast<double *>(smem + OFF_ROWS);
-    uint32_t *rowc = reinterpret_cast<uint32_t *>(smem + OFF_ROWS + BN * 8);
-    float *rowv = reinterpret_cast<float *>(smem + OFF_ROWS + BN * 12);
+    const epi::Cols cols(smem + OFF_ROWS, BN);
 
     if (grid_failed(p.status)) return;
     const TileList<BM, BN> tl{(p.m + BM - 1) / BM, p.tb0, tiles_b, p.symmetric};
@@ -285,15 +284,7 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
             for (int k = 0; k < 2; ++k) {
                 const int bl = et + k * EPI_THREADS;
                 const int b = tb * BN + bl;
-                const uint32_t c = b < p.n ? p.bcB[b] : 0u;
-                rowc[bl] = c;
-                if (MODE == R2_EXACT) {
-                    rowd[bl] = row_exact(c, p.S).inv_var;
-                } else {
-                    const RowRef r = row_ref(c, p.S);
-                    rowv[bl] = r.v;
-                    rowd[bl] = r.one_minus;
-                }
+                epi::store_col<MODE>(cols, bl, b < p.n ? p.bcB[b] : 0u, p.S);
             }
             named_bar_sync(1, EPI_THREADS);
             // On a failed wait the warp skips the tile but stays in the loop,
@@ -311,41 +302,16 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
                 tc_fence_after();
                 const int a = ta * BM + q * 32 + lane;
                 const bool a_ok = a < p.m;
-                const uint32_t ca = a_ok ? p.bcA[a] : 0u;
-                RowExact ra_e;
-                RowRef ra_r;
-                if (MODE == R2_EXACT) ra_e = row_exact(ca, p.S);
-                else ra_r = row_ref(ca, p.S);
+                const epi::ARow ra = epi::make_arow<MODE>(a_ok ? p.bcA[a] : 0u, p.S);
                 const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * BN);
 #pragma unroll 1
                 for (int col0 = 0; col0 < BN; col0 += 32) {
                     uint32_t v[32];
                     __syncwarp();
                     tc_ld_32x32b_x32(tbase + (uint32_t)col0, v);
-#pragma unroll
-                    for (int t = 0; t < 32; ++t) {
-                        const int bl = col0 + t;
-                        const int b = tb * BN + bl;
-                        if (b < p.n && a_ok && (!p.symmetric || a >= b)) {
-                            const uint32_t cnt = v[t] >> COUNT_SHIFT;
-                            float r2;
-                            if (MODE == R2_EXACT) {
-                                RowExact rb;
-                                rb.c = rowc[bl];
-                                rb.inv_var = rowd[bl];
-                                r2 = r2_exact(cnt, ra_e, rb, p.S);
-                            } else {
-                                RowRef rb;
-                                rb.c = rowc[bl];
-                                rb.v = rowv[bl];
-                                rb.one_minus = rowd[bl];
-                                r2 = r2_reference(cnt, ra_r, rb, p.S);
-                            }
-                            const long long o = (long long)(b - p.out_row0);
-                            p.r2[o * p.ldr + a] = r2;
-                            if (p.counts) p.counts[o * p.ldc + a] = cnt;
-                        }
-                    }
+                    epi::chunk<MODE, COUNT_SHIFT>(v, ra, cols, col0, tb * BN + col0, a, a_ok,
+                                                  p.n, p.symmetric, p.r2, p.ldr, p.counts, p.ldc,
+                                                  p.out_row0, p.S);
                 }
                 tc_fence_before();
                 __syncwarp();

@@ -20,6 +20,7 @@
 //                current tile (warp w reads TMEM lane quarter w % 4; the four
 //                warps of a quarter split the 2 accumulators x 2 column
 //                halves), then release the accumulators.
+#include "epilogue.cuh"
 #include "qld_kernels.h"
 #include "tcgen05.cuh"
 
@@ -52,7 +53,7 @@ constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
 constexpr int OFF_PA = OFF_UB + UST * UB_BYTES;
 constexpr int OFF_PB = OFF_PA + PST * PA_BYTES;
 constexpr int OFF_ROWS = OFF_PB + PST * PB_BYTES;
-constexpr int ROWS_BYTES = BN * (8 + 4 + 4);
+constexpr int ROWS_BYTES = BN * epi::COL_BYTES;
 constexpr int OFF_BAR = OFF_ROWS + ROWS_BYTES;
 constexpr int NBARS = 2 * PST + 2 * UST + 2 + 1;
 constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
@@ -98,9 +99,7 @@ k_ld_mma_wide(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     uint64_t *accempty = accfull + 1;
     uint64_t *mma_done = accempty + 1;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + OFF_TMEM);
-    double *rowd = reinterpret_cast<double *>(smem + OFF_ROWS);
-    uint32_t *rowc = reinterpret_cast<uint32_t *>(smem + OFF_ROWS + BN * 8);
-    float *rowv = reinterpret_cast<float *>(smem + OFF_ROWS + BN * 12);
+    const epi::Cols cols(smem + OFF_ROWS, BN);
 
     if (grid_failed(p.status)) return;
     const TileList<BM, BN> tl{(p.m + BM - 1) / BM, p.tb0, tiles_b, p.symmetric};
@@ -282,15 +281,7 @@ k_ld_mma_wide(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             // B-row factors of this tile (256 of them, threads 0..255)
             if (wt < BN) {
                 const int b = tb * BN + wt;
-                const uint32_t c = b < p.n ? p.bcB[b] : 0u;
-                rowc[wt] = c;
-                if (MODE == R2_EXACT) {
-                    rowd[wt] = row_exact(c, p.S).inv_var;
-                } else {
-                    const RowRef r = row_ref(c, p.S);
-                    rowv[wt] = r.v;
-                    rowd[wt] = r.one_minus;
-                }
+                epi::store_col<MODE>(cols, wt, b < p.n ? p.bcB[b] : 0u, p.S);
             }
             named_bar_sync(1, WORKERS);
             bool ready = ok && !failed && mbar_wait(smem_u32(accfull), it & 1, p.timeout_cycles,
@@ -305,11 +296,7 @@ k_ld_mma_wide(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
                 tc_fence_after();
                 const int a = ta * BM + acc_i * HM + q * 32 + lane;
                 const bool a_ok = a < p.m;
-                const uint32_t ca = a_ok ? p.bcA[a] : 0u;
-                RowExact ra_e;
-                RowRef ra_r;
-                if (MODE == R2_EXACT) ra_e = row_exact(ca, p.S);
-                else ra_r = row_ref(ca, p.S);
+                const epi::ARow ra = epi::make_arow<MODE>(a_ok ? p.bcA[a] : 0u, p.S);
                 const uint32_t tbase =
                     tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc_i * BN + colh * 128);
 #pragma unroll 1
@@ -317,30 +304,10 @@ k_ld_mma_wide(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
                     uint32_t v[32];
                     __syncwarp();
                     tc_ld_32x32b_x32(tbase + (uint32_t)c0, v);
-#pragma unroll
-                    for (int t = 0; t < 32; ++t) {
-                        const int bl = colh * 128 + c0 + t;
-                        const int b = tb * BN + bl;
-                        if (b < p.n && a_ok && (!p.symmetric || a >= b)) {
-                            const uint32_t cnt = v[t] >> COUNT_SHIFT;
-                            float r2;
-                            if (MODE == R2_EXACT) {
-                                RowExact rb;
-                                rb.c = rowc[bl];
-                                rb.inv_var = rowd[bl];
-                                r2 = r2_exact(cnt, ra_e, rb, p.S);
-                            } else {
-                                RowRef rb;
-                                rb.c = rowc[bl];
-                                rb.v = rowv[bl];
-                                rb.one_minus = rowd[bl];
-                                r2 = r2_reference(cnt, ra_r, rb, p.S);
-                            }
-                            const long long o = (long long)(b - p.out_row0);
-                            p.r2[o * p.ldr + a] = r2;
-                            if (p.counts) p.counts[o * p.ldc + a] = cnt;
-                        }
-                    }
+                    epi::chunk<MODE, COUNT_SHIFT>(v, ra, cols, colh * 128 + c0,
+                                                  tb * BN + colh * 128 + c0, a, a_ok, p.n,
+                                                  p.symmetric, p.r2, p.ldr, p.counts, p.ldc,
+                                                  p.out_row0, p.S);
                 }
                 tc_fence_before();
                 __syncwarp();

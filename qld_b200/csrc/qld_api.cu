@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <utility>
 #include <vector>
@@ -44,6 +45,8 @@ struct qld_ctx {
     int mma_tile = 0;                 // 0: per shape, else 128 or 256
     long long timeout_cycles = 4000000000LL;  // ~2 s at boost clock
     DevBuf dA, dB, dbcA, dbcB, dOut[2], dCnt[2];
+    DevBuf dJobs, dQueue;             // batched launches: job table, ticket counter
+    std::vector<BatchJob> hJobs;
     cudaEvent_t ev_band[2] = {nullptr, nullptr};
     cudaEvent_t ev_copy[2] = {nullptr, nullptr};
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
@@ -148,6 +151,23 @@ const KernelShape &shape_of(qld_ctx *c, int variant, const Task &t, int b0, int 
     return variant == QLD_KERNEL_MMA ? mma_shape(c, t, b0, b1) : kPopcShape;
 }
 
+// With QLD_OPT_PROFILE: an event pair around the next launch on `st`
+// (*end receives the closing event, recorded by the caller after the launch).
+int prof_begin(qld_ctx *c, cudaStream_t st, cudaEvent_t *end) {
+    *end = nullptr;
+    if (!c->profile) return QLD_OK;
+    if (c->prof_used == c->prof.size()) {
+        cudaEvent_t a, b;
+        CUDA_TRY(c, cudaEventCreate(&a));
+        CUDA_TRY(c, cudaEventCreate(&b));
+        c->prof.emplace_back(a, b);
+    }
+    *end = c->prof[c->prof_used].second;
+    CUDA_TRY(c, cudaEventRecord(c->prof[c->prof_used].first, st));
+    ++c->prof_used;
+    return QLD_OK;
+}
+
 // Launch the counts kernel over B rows [b0, b1) (b0 a multiple of 256),
 // writing r2/counts rows relative to out_row0.
 int launch_counts(qld_ctx *c, const Task &t, int b0, int b1, float *r2, long long ldr,
@@ -175,26 +195,15 @@ int launch_counts(qld_ctx *c, const Task &t, int b0, int b1, float *r2, long lon
     for (int done = 0; done < tiles_b; done += 65535) {
         const int nb = tiles_b - done < 65535 ? tiles_b - done : 65535;
         p.tb0 = tb0 + done;
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
-        if (c->profile) {
-            if (c->prof_used == c->prof.size()) {
-                cudaEvent_t a, b;
-                CUDA_TRY(c, cudaEventCreate(&a));
-                CUDA_TRY(c, cudaEventCreate(&b));
-                c->prof.emplace_back(a, b);
-            }
-            e0 = c->prof[c->prof_used].first;
-            e1 = c->prof[c->prof_used].second;
-            ++c->prof_used;
-            CUDA_TRY(c, cudaEventRecord(e0, st));
-        }
+        cudaEvent_t e1 = nullptr;
+        if (int rc = prof_begin(c, st, &e1)) return rc;
         cudaError_t e =
             variant != QLD_KERNEL_MMA ? launch_popc(tmA, tmB, p, nb, c->r2_mode, st)
             : &ks == &kMmaWideShape   ? launch_mma_wide(tmA, tmB, p, nb, c->r2_mode, st)
                                       : launch_mma(tmA, tmB, p, nb, c->r2_mode, st);
         if (e != cudaSuccess)
             return set_err(c, QLD_ERR_CUDA, "counts kernel launch failed: %s", cudaGetErrorString(e));
-        if (c->profile) CUDA_TRY(c, cudaEventRecord(e1, st));
+        if (e1) CUDA_TRY(c, cudaEventRecord(e1, st));
         c->stats.counts_launches++;
         c->stats.kernel_launches++;
     }
@@ -288,7 +297,7 @@ int qld_cuda_release(qld_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->copy) cudaStreamSynchronize(c->copy);
     DevBuf *bufs[] = {&c->dA, &c->dB, &c->dbcA, &c->dbcB, &c->dOut[0], &c->dOut[1],
-                      &c->dCnt[0], &c->dCnt[1]};
+                      &c->dCnt[0], &c->dCnt[1], &c->dJobs, &c->dQueue};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto &e : c->prof) {
@@ -459,6 +468,81 @@ int qld_cuda_ld_device(qld_ctx *c, const qld_ld_args *a, void *stream) {
     CUDA_TRY(c, cudaSetDevice(c->device));
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     return launch_counts(c, t, 0, t.n, a->r2, a->ldr, a->counts, a->ldc, 0, st);
+}
+
+int qld_cuda_ld_batch(qld_ctx *c, const qld_ld_args *jobs, int njobs, void *stream) {
+    if (!c || (njobs > 0 && !jobs) || njobs < 0) return QLD_ERR_INVALID;
+    if (njobs == 0) return QLD_OK;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const KernelShape &ks = kBatchShape;
+    std::vector<long long> tiles(njobs), cost(njobs);
+    std::vector<int> order(njobs);
+    for (int j = 0; j < njobs; ++j) {
+        qld_ld_args a = jobs[j];
+        if (a.symmetric) { a.B = a.A; a.bcB = a.bcA; a.n = a.m; a.ldb = a.lda; }
+        if (a.m < 0 || a.n < 0 || a.K < 1 || a.S < 1 || a.lda < a.K || a.ldb < a.K ||
+            (a.lda & 1) || (a.ldb & 1) || a.ldr < a.m || (a.counts && a.ldc < a.m) || !a.A ||
+            !a.B || !a.bcA || !a.bcB || !a.r2 || !aligned16(a.A) || !aligned16(a.B))
+            return set_err(c, QLD_ERR_INVALID, "batch job %d: bad sizes, strides or pointers", j);
+        if ((long long)a.K * 64 > kMmaMaxSamples)
+            return set_err(c, QLD_ERR_UNSUPPORTED,
+                           "batch job %d: K*64 > %d samples (use qld_cuda_ld_device)", j,
+                           kMmaMaxSamples);
+        Task t{a.A, a.bcA, a.m, a.lda, a.B, a.bcB, a.n, a.ldb, a.K, a.S, a.symmetric};
+        tiles[j] = (a.m == 0 || a.n == 0) ? 0 : tile_count(t, ks.bm, ks.bn, 0, a.n);
+        cost[j] = tiles[j] * (long long)a.K;
+        order[j] = j;
+    }
+    // Most expensive tasks first, so the queue ends on small items.
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return cost[x] > cost[y]; });
+    c->hJobs.resize(njobs);
+    long long items = 0;
+    for (int i = 0; i < njobs; ++i) {
+        const int j = order[i];
+        qld_ld_args a = jobs[j];
+        if (a.symmetric) { a.B = a.A; a.bcB = a.bcA; a.n = a.m; a.ldb = a.lda; }
+        BatchJob &J = c->hJobs[i];
+        memset(&J, 0, sizeof J);
+        J.bcA = a.bcA; J.bcB = a.bcB; J.r2 = a.r2; J.counts = a.counts;
+        J.ldr = a.ldr; J.ldc = a.ldc; J.item0 = items;
+        J.m = a.m; J.n = a.n; J.K = a.K; J.S = a.S; J.symmetric = a.symmetric;
+        if (tiles[j] > 0) {
+            int rc;
+            if ((rc = make_tmap(c, &J.tmA, a.A, a.m, a.K, a.lda, ks.box_words, ks.box_rows_a,
+                                ks.swizzle)) ||
+                (rc = make_tmap(c, &J.tmB, a.B, a.n, a.K, a.ldb, ks.box_words, ks.box_rows_b,
+                                ks.swizzle)))
+                return rc;
+        }
+        items += tiles[j];
+    }
+    if (items == 0) return QLD_OK;
+    int rc;
+    if ((rc = ensure(c, c->dJobs, sizeof(BatchJob) * (size_t)njobs)) ||
+        (rc = ensure(c, c->dQueue, sizeof(unsigned long long))))
+        return rc;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    CUDA_TRY(c, cudaMemcpyAsync(c->dJobs.p, c->hJobs.data(), sizeof(BatchJob) * (size_t)njobs,
+                                cudaMemcpyHostToDevice, st));
+    CUDA_TRY(c, cudaMemsetAsync(c->dQueue.p, 0, sizeof(unsigned long long), st));
+    BatchParams bp{};
+    bp.jobs = static_cast<const BatchJob *>(c->dJobs.p);
+    bp.njobs = njobs;
+    bp.nitems = items;
+    bp.queue = static_cast<unsigned long long *>(c->dQueue.p);
+    bp.status = c->d_status;
+    bp.timeout_cycles = c->timeout_cycles;
+    cudaEvent_t e1 = nullptr;
+    if ((rc = prof_begin(c, st, &e1))) return rc;
+    cudaError_t e = launch_batch(bp, c->r2_mode, 0, st);
+    if (e != cudaSuccess)
+        return set_err(c, QLD_ERR_CUDA, "batched launch failed: %s", cudaGetErrorString(e));
+    if (e1) CUDA_TRY(c, cudaEventRecord(e1, st));
+    c->stats.counts_launches++;
+    c->stats.kernel_launches++;
+    c->stats.last_kernel = QLD_KERNEL_MMA;
+    return QLD_OK;
 }
 
 int qld_cuda_sync(qld_ctx *c, void *stream) {

@@ -34,4 +34,30 @@ cudaError_t launch_mma(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdP
 cudaError_t launch_mma_wide(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
                             int tiles_b, int r2_mode, cudaStream_t st);
 
+// One task of a batched launch: its tensor maps (kBatchShape boxes), sizes,
+// output, and the number of work items (output tiles) of the tasks before it.
+struct BatchJob {
+    CUtensorMap tmA, tmB;
+    const uint32_t *bcA, *bcB;
+    float *r2;
+    uint32_t *counts;
+    long long ldr, ldc;
+    long long item0;
+    int m, n, K, S, symmetric;
+};
+
+struct BatchParams {
+    const BatchJob *jobs;
+    int njobs;
+    long long nitems;
+    unsigned long long *queue;   // work-queue ticket counter, zero at launch
+    unsigned *status;
+    long long timeout_cycles;
+};
+
+extern const KernelShape kBatchShape;
+
+// Persistent batched launch over all items of bp.jobs (max_ctas > 0 caps the grid).
+cudaError_t launch_batch(const BatchParams &bp, int r2_mode, int max_ctas, cudaStream_t st);
+
 }  // namespace qld
