@@ -121,6 +121,25 @@ int qld_cuda_ld_device(qld_ctx *ctx, const qld_ld_args *args, void *stream);
 int qld_cuda_sync(qld_ctx *ctx, void *stream);
 
 /*
+ * Windowed (band) LD over one region: r^2 only for SNP pairs (i, j) with
+ * 1 <= j - i <= band.  Output is the m x band array r2_band[i*band + d] =
+ * r^2(SNP i, SNP i+1+d) (entries with i+1+d >= m are unspecified); counts_band
+ * (optional) likewise.  The host-buffer form streams: the table goes to the
+ * device in row chunks, each block of QLD_OPT_BAND_ROWS rows is computed as
+ * soon as the rows it needs have arrived, and its band rows are copied back
+ * while the next block computes.  qLD has no band mode: its equivalent is a
+ * split_region-style -inputList of window pairs (utilities/split_region),
+ * one task each.
+ */
+int qld_cuda_ld_band(qld_ctx *ctx, const uint64_t *A, const uint32_t *bcA, int m, int K, int S,
+                     int band, float *r2_band, uint32_t *counts_band);
+/* Device-resident form: lda as in qld_ld_args, ldr/ldc >= band elements
+ * between consecutive rows of the band arrays; asynchronous on `stream`. */
+int qld_cuda_ld_band_device(qld_ctx *ctx, const uint64_t *A, const uint32_t *bcA, int m,
+                            long long lda, int K, int S, int band, float *r2_band,
+                            long long ldr, uint32_t *counts_band, long long ldc, void *stream);
+
+/*
  * Many independent tasks (region pairs of any SNP and sample counts, single
  * or two-region) in ONE persistent launch: every output tile of every task is
  * a work item taken from a device work queue by the SMs as they free up.

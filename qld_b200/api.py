@@ -31,7 +31,8 @@ OPT_KERNEL, OPT_R2_MODE, OPT_PROFILE, OPT_BAND_ROWS, OPT_MMA_TILE = 1, 2, 3, 4, 
 
 EXPORTED = (
     "qld_cuda_init", "qld_cuda_release", "qld_cuda_last_error", "qld_cuda_set_option",
-    "qld_cuda_ld", "qld_cuda_ld_device", "qld_cuda_ld_batch", "qld_cuda_sync",
+    "qld_cuda_ld", "qld_cuda_ld_device", "qld_cuda_ld_batch", "qld_cuda_ld_band",
+    "qld_cuda_ld_band_device", "qld_cuda_sync",
     "qld_cuda_host_alloc",
     "qld_cuda_host_free", "qld_cuda_get_stats", "qld_cuda_measure_popc_peak",
 )
@@ -86,6 +87,8 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.qld_cuda_ld.argtypes = [vp, vp, vp, i, vp, vp, i, i, i, i, vp, vp]
     lib.qld_cuda_ld_device.argtypes = [vp, ct.POINTER(_LdArgs), vp]
     lib.qld_cuda_ld_batch.argtypes = [vp, ct.POINTER(_LdArgs), i, vp]
+    lib.qld_cuda_ld_band.argtypes = [vp, vp, vp, i, i, i, i, vp, vp]
+    lib.qld_cuda_ld_band_device.argtypes = [vp, vp, vp, i, ll, i, i, i, vp, ll, vp, ll, vp]
     lib.qld_cuda_sync.argtypes = [vp, vp]
     lib.qld_cuda_host_alloc.argtypes = [vp, ct.c_size_t, ct.POINTER(vp)]
     lib.qld_cuda_host_free.argtypes = [vp, vp]
@@ -216,6 +219,28 @@ class Context:
                              int(bool(j["symmetric"])), _p(j["r2"]), int(j["ldr"]),
                              _p(j.get("counts")), int(j.get("ldc", 0)))
         self._check(self.lib.qld_cuda_ld_batch(self.h, arr, len(jobs), _stream(stream)))
+
+    def ld_band(self, A, bcA, *, S: int, band: int, r2_out=None, counts=False):
+        """Windowed LD from host arrays: r2 (m, band), r2[i, d] = r^2(i, i+1+d)."""
+        A = np.ascontiguousarray(A).view(np.uint64) if A.dtype != np.uint64 else np.ascontiguousarray(A)
+        bcA = np.ascontiguousarray(bcA, dtype=np.uint32)
+        m, K = A.shape
+        if r2_out is None:
+            r2_out = np.empty((m, band), np.float32)
+        cnt = None
+        if isinstance(counts, np.ndarray):
+            cnt = counts
+        elif counts:
+            cnt = np.empty((m, band), np.uint32)
+        self._check(self.lib.qld_cuda_ld_band(self.h, _ptr(A), _ptr(bcA), m, K, int(S), int(band),
+                                              _ptr(r2_out), _ptr(cnt)))
+        return (r2_out, cnt) if cnt is not None else r2_out
+
+    def ld_band_device(self, A, bcA, m, lda, K, S, band, r2, ldr, counts=None, ldc=0,
+                       stream=None):
+        self._check(self.lib.qld_cuda_ld_band_device(
+            self.h, _p(A), _p(bcA), int(m), int(lda), int(K), int(S), int(band), _p(r2),
+            int(ldr), _p(counts), int(ldc), _stream(stream)))
 
     def sync(self, stream=None):
         self._check(self.lib.qld_cuda_sync(self.h, _stream(stream)))

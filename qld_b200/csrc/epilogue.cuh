@@ -95,19 +95,19 @@ __device__ __forceinline__ float pair_r2(uint32_t cnt, const ARow &ra, const Col
 
 // One 32-column chunk: accumulators v[t] (holding count << shift) of A row a
 // against B rows b0 + t (local columns bl0 + t).  Output element (b, a) goes
-// to r2[(b - row0) * ldr + a] (and counts likewise).  Entries outside the
-// task (b >= n, a >= m) and, for a single region, above the diagonal
-// (a < b) are not written.
+// to r2[(b - row0) * ldr + a] (and counts likewise).  Only entries inside the
+// task (b < n, a < m) and the diagonal window dlo <= a - b <= dhi are
+// written (a single region: a >= b; a band: 1 <= a - b <= W).
 template <int MODE, int SHIFT>
 __device__ __forceinline__ void chunk(const uint32_t (&v)[32], const ARow &ra, const Cols &f,
-                                      int bl0, int b0, int a, bool a_ok, int n, int symmetric,
-                                      float *r2, long long ldr, uint32_t *counts, long long ldc,
-                                      int row0, int S) {
+                                      int bl0, int b0, int a, bool a_ok, int n, int dlo,
+                                      int dhi, float *r2, long long ldr, uint32_t *counts,
+                                      long long ldc, int row0, int S) {
     if (!a_ok) return;
     const double S_d = (double)S;
     float *o = r2 + (long long)(b0 - row0) * ldr + a;
     uint32_t *oc = counts ? counts + (long long)(b0 - row0) * ldc + a : nullptr;
-    const bool interior = (b0 + 31 < n) && (!symmetric || a >= b0 + 31);
+    const bool interior = (b0 + 31 < n) && (a - (b0 + 31) >= dlo) && (a - b0 <= dhi);
     if (interior) {
 #pragma unroll
         for (int t = 0; t < 32; ++t) {
@@ -119,7 +119,7 @@ __device__ __forceinline__ void chunk(const uint32_t (&v)[32], const ARow &ra, c
 #pragma unroll
         for (int t = 0; t < 32; ++t) {
             const int b = b0 + t;
-            if (b < n && (!symmetric || a >= b)) {
+            if (b < n && a - b >= dlo && a - b <= dhi) {
                 const uint32_t cnt = v[t] >> SHIFT;
                 o[(long long)t * ldr] = pair_r2<MODE>(cnt, ra, f, bl0 + t, S_d, S);
                 if (oc) oc[(long long)t * ldc] = cnt;

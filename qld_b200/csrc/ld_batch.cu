@@ -83,7 +83,7 @@ __device__ __forceinline__ Item decode_item(const BatchJob *jobs, int njobs, lon
         else hi = mid - 1;
     }
     const BatchJob &J = jobs[lo];
-    const TileList<BM, BN> tl{(J.m + BM - 1) / BM, 0, (J.n + BN - 1) / BN, J.symmetric};
+    const TileList<BM, BN> tl{(J.m + BM - 1) / BM, 0, (J.n + BN - 1) / BN, J.symmetric, 0};
     Item it;
     it.job = lo;
     tl.decode((int)(g - J.item0), it.ta, it.tb);
@@ -360,8 +360,8 @@ k_ld_batch(const BatchParams bp) {
                     __syncwarp();
                     tc_ld_32x32b_x32(tbase + (uint32_t)col0, v);
                     epi::chunk<MODE, COUNT_SHIFT>(v, ra, cols, col0, it.tb * BN + col0, a, a_ok,
-                                                  J.n, J.symmetric, J.r2, J.ldr, J.counts, J.ldc,
-                                                  0, J.S);
+                                                  J.n, diag_lo(J.symmetric, 0), diag_hi(0), J.r2,
+                                                  J.ldr, J.counts, J.ldc, 0, J.S);
                 }
                 tc_fence_before();
                 __syncwarp();

@@ -102,7 +102,8 @@ k_ld_mma_wide(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
     const epi::Cols cols(smem + OFF_ROWS, BN);
 
     if (grid_failed(p.status)) return;
-    const TileList<BM, BN> tl{(p.m + BM - 1) / BM, p.tb0, tiles_b, p.symmetric};
+    const TileList<BM, BN> tl{(p.m + BM - 1) / BM, p.tb0, tiles_b, p.symmetric, p.band};
+    const int dlo = diag_lo(p.symmetric, p.band), dhi = diag_hi(p.band);
     const int ntiles = tl.count();
     if ((int)blockIdx.x >= ntiles) return;
 
@@ -306,7 +307,7 @@ k_ld_mma_wide(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
                     tc_ld_32x32b_x32(tbase + (uint32_t)c0, v);
                     epi::chunk<MODE, COUNT_SHIFT>(v, ra, cols, colh * 128 + c0,
                                                   tb * BN + colh * 128 + c0, a, a_ok, p.n,
-                                                  p.symmetric, p.r2, p.ldr, p.counts, p.ldc,
+                                                  dlo, dhi, p.r2, p.ldr, p.counts, p.ldc,
                                                   p.out_row0, p.S);
                 }
                 tc_fence_before();
@@ -346,12 +347,8 @@ cudaError_t launch_mode(const CUtensorMap &tmA, const CUtensorMap &tmB, const Ld
             cudaSuccess)
             return e;
     }
-    const long long TA = (p.m + BM - 1) / BM;
-    long long ntiles = 0;
-    for (int t = 0; t < tiles_b; ++t) {
-        const long long lo = p.symmetric ? ((long long)(p.tb0 + t) * BN) / BM : 0;
-        ntiles += TA - lo > 0 ? TA - lo : 0;
-    }
+    const long long ntiles =
+        TileList<BM, BN>{(p.m + BM - 1) / BM, p.tb0, tiles_b, p.symmetric, p.band}.count();
     if (ntiles == 0) return cudaSuccess;
     const int grid = (int)(ntiles < g_sm_count ? ntiles : g_sm_count);
     kern<<<grid, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p, tiles_b);

@@ -47,8 +47,13 @@ k_ld_popc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
 
     const int ta = blockIdx.x;
     const int tb = p.tb0 + blockIdx.y;
-    // Single region: skip tiles with no entry a >= b.
-    if (p.symmetric && ta * BM + BM - 1 < tb * BN) return;
+    // Skip tiles with no entry in the diagonal window (single region: a >= b;
+    // band: 1 <= a - b <= band).
+    const int dlo = p.band > 0 ? 1 : (p.symmetric ? 0 : -2147483647 - 1);
+    const int dhi = p.band > 0 ? p.band : 2147483647;
+    if ((long long)ta * BM + BM - 1 - (long long)tb * BN < dlo ||
+        (long long)ta * BM - ((long long)tb * BN + BN - 1) > dhi)
+        return;
     if (grid_failed(p.status)) return;   // an earlier CTA already gave up
 
     const int tid = threadIdx.x;
@@ -150,7 +155,7 @@ k_ld_popc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 const int a = a0 + 16 * i;
-                if (a < p.m && (!p.symmetric || a >= b)) {
+                if (a < p.m && a - b >= dlo && a - b <= dhi) {
                     out[a] = r2_exact(acc[i][j], ra[i], rb[j], p.S);
                     if (cnt) cnt[a] = acc[i][j];
                 }
@@ -171,7 +176,7 @@ k_ld_popc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 const int a = a0 + 16 * i;
-                if (a < p.m && (!p.symmetric || a >= b)) {
+                if (a < p.m && a - b >= dlo && a - b <= dhi) {
                     out[a] = r2_reference(acc[i][j], ra[i], rb[j], p.S);
                     if (cnt) cnt[a] = acc[i][j];
                 }

@@ -18,6 +18,7 @@
 
 #include "qld_cuda.h"
 #include "qld_kernels.h"
+#include "tcgen05.cuh"
 
 using namespace qld;
 
@@ -35,6 +36,8 @@ struct qld_ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;   // kernels and host->device copies
     cudaStream_t copy = nullptr;     // device->host result copies
+    cudaStream_t h2d = nullptr;      // chunked host->device table copies (band calls)
+    std::vector<cudaEvent_t> h2d_ev;
     unsigned *d_status = nullptr;
     unsigned *h_status = nullptr;    // pinned mirror of d_status
     char err[512] = {0};
@@ -117,6 +120,7 @@ struct Task {
     const uint64_t *A; const uint32_t *bcA; int m; long long lda;
     const uint64_t *B; const uint32_t *bcB; int n; long long ldb;
     int K, S, symmetric;
+    int band;   // > 0: single region, entries 1 <= a - b <= band only
 };
 
 bool mma_exact_for(const Task &t) { return (long long)t.K * 64 <= kMmaMaxSamples; }
@@ -129,13 +133,12 @@ int choose_kernel(qld_ctx *c, const Task &t) {
 }
 
 long long tile_count(const Task &t, int bm, int bn, int b0, int b1) {
-    const long long TA = (t.m + bm - 1) / bm;
-    long long n = 0;
-    for (int tb = b0 / bn; tb * bn < b1; ++tb) {
-        const long long lo = t.symmetric ? ((long long)tb * bn) / bm : 0;
-        n += TA - lo > 0 ? TA - lo : 0;
-    }
-    return n;
+    const int tb0 = b0 / bn, tiles_b = (b1 - b0 + bn - 1) / bn;
+    if (bm == 256 && bn == 256)
+        return tc::TileList<256, 256>{(t.m + 255) / 256, tb0, tiles_b, t.symmetric, t.band}.count();
+    if (bm == 128 && bn == 256)
+        return tc::TileList<128, 256>{(t.m + 127) / 128, tb0, tiles_b, t.symmetric, t.band}.count();
+    return tc::TileList<128, 128>{(t.m + 127) / 128, tb0, tiles_b, t.symmetric, t.band}.count();
 }
 
 // The 256 x 256 tile unpacks 2/3 of the bytes per multiply-accumulate but
@@ -187,9 +190,17 @@ int launch_counts(qld_ctx *c, const Task &t, int b0, int b1, float *r2, long lon
     LdParams p{};
     p.m = t.m; p.n = t.n; p.K = t.K; p.S = t.S;
     p.symmetric = t.symmetric;
+    p.band = t.band;
     p.nk = (t.K + ks.box_words - 1) / ks.box_words;
     p.bcA = t.bcA; p.bcB = t.bcB;
     p.r2 = r2; p.ldr = ldr; p.counts = cnt; p.ldc = ldc; p.out_row0 = out_row0;
+    if (t.band > 0) {
+        // Band array: entry (b, a) at r2[(b - out_row0) * ldr + (a - b - 1)], i.e. the
+        // kernels' (b - out_row0) * ldr' + a with ldr' = ldr - 1 and a shifted base.
+        p.r2 = r2 - out_row0 - 1;
+        p.ldr = ldr - 1;
+        if (cnt) { p.counts = cnt - out_row0 - 1; p.ldc = ldc - 1; }
+    }
     p.status = c->d_status;
     p.timeout_cycles = c->timeout_cycles;
     for (int done = 0; done < tiles_b; done += 65535) {
@@ -260,7 +271,8 @@ int qld_cuda_init(int device, qld_ctx **ctx_out) {
     do {
         if (cudaSetDevice(device) != cudaSuccess) { rc = QLD_ERR_CUDA; break; }
         if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking) != cudaSuccess) {
             rc = QLD_ERR_CUDA; break;
         }
         for (int i = 0; i < 2; ++i)
@@ -296,6 +308,8 @@ int qld_cuda_release(qld_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->copy) cudaStreamSynchronize(c->copy);
+    if (c->h2d) cudaStreamSynchronize(c->h2d);
+    for (cudaEvent_t e : c->h2d_ev) cudaEventDestroy(e);
     DevBuf *bufs[] = {&c->dA, &c->dB, &c->dbcA, &c->dbcB, &c->dOut[0], &c->dOut[1],
                       &c->dCnt[0], &c->dCnt[1], &c->dJobs, &c->dQueue};
     for (DevBuf *b : bufs)
@@ -312,6 +326,7 @@ int qld_cuda_release(qld_ctx *c) {
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->copy) cudaStreamDestroy(c->copy);
+    if (c->h2d) cudaStreamDestroy(c->h2d);
     delete c;
     return QLD_OK;
 }
@@ -408,7 +423,7 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
         dbcB = static_cast<const uint32_t *>(c->dbcB.p);
     }
     Task t{static_cast<const uint64_t *>(c->dA.p), static_cast<const uint32_t *>(c->dbcA.p), m, Kp,
-           dB, dbcB, n, Kp, K, S, symmetric};
+           dB, dbcB, n, Kp, K, S, symmetric, 0};
 
     const int band = c->band_rows;  // multiple of 256: whole tile rows of every variant
     const int nbands = (n + band - 1) / band;
@@ -456,7 +471,7 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
 
 int qld_cuda_ld_device(qld_ctx *c, const qld_ld_args *a, void *stream) {
     if (!c || !a) return QLD_ERR_INVALID;
-    Task t{a->A, a->bcA, a->m, a->lda, a->B, a->bcB, a->n, a->ldb, a->K, a->S, a->symmetric};
+    Task t{a->A, a->bcA, a->m, a->lda, a->B, a->bcB, a->n, a->ldb, a->K, a->S, a->symmetric, 0};
     if (t.symmetric) { t.B = t.A; t.bcB = t.bcA; t.n = t.m; t.ldb = t.lda; }
     if (t.m < 0 || t.n < 0 || t.K < 1 || t.S < 1 || t.lda < t.K || t.ldb < t.K || (t.lda & 1) ||
         (t.ldb & 1) || a->ldr < t.m || (a->counts && a->ldc < t.m))
@@ -468,6 +483,85 @@ int qld_cuda_ld_device(qld_ctx *c, const qld_ld_args *a, void *stream) {
     CUDA_TRY(c, cudaSetDevice(c->device));
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     return launch_counts(c, t, 0, t.n, a->r2, a->ldr, a->counts, a->ldc, 0, st);
+}
+
+int qld_cuda_ld_band_device(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m,
+                            long long lda, int K, int S, int band, float *r2_band, long long ldr,
+                            uint32_t *counts_band, long long ldc, void *stream) {
+    if (!c) return QLD_ERR_INVALID;
+    if (m < 0 || K < 1 || S < 1 || band < 1 || lda < K || (lda & 1) || ldr < band ||
+        (counts_band && ldc < band))
+        return set_err(c, QLD_ERR_INVALID, "bad band sizes m=%d K=%d band=%d lda=%lld ldr=%lld", m,
+                       K, band, lda, ldr);
+    if (m == 0) return QLD_OK;
+    if (!A || !bcA || !r2_band || !aligned16(A))
+        return set_err(c, QLD_ERR_INVALID, "NULL or misaligned device pointer");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    Task t{A, bcA, m, lda, A, bcA, m, lda, K, S, 1, band};
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    return launch_counts(c, t, 0, m, r2_band, ldr, counts_band, ldc, 0, st);
+}
+
+int qld_cuda_ld_band(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, int K, int S,
+                     int band, float *r2_band, uint32_t *counts_band) {
+    if (!c) return QLD_ERR_INVALID;
+    if (m < 0 || K < 1 || S < 1 || band < 1)
+        return set_err(c, QLD_ERR_INVALID, "bad band sizes m=%d K=%d S=%d band=%d", m, K, S, band);
+    if (m == 0) return QLD_OK;
+    if (!A || !bcA || !r2_band)
+        return set_err(c, QLD_ERR_INVALID, "NULL table, bit-count or output pointer");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const long long Kp = K + (K & 1);
+    int rc;
+    if ((rc = ensure(c, c->dA, (size_t)m * Kp * 8)) || (rc = ensure(c, c->dbcA, (size_t)m * 4)))
+        return rc;
+    uint64_t *dA = static_cast<uint64_t *>(c->dA.p);
+    const int rows_blk = c->band_rows;                       // multiple of 256
+    const int nblk = (m + rows_blk - 1) / rows_blk;
+    for (int s = 0; s < 2 && s < nblk; ++s) {
+        if ((rc = ensure(c, c->dOut[s], (size_t)rows_blk * band * 4))) return rc;
+        if (counts_band && (rc = ensure(c, c->dCnt[s], (size_t)rows_blk * band * 4))) return rc;
+    }
+    // Host->device in row chunks on the h2d stream, an event after each.
+    while ((int)c->h2d_ev.size() < nblk) {
+        cudaEvent_t e;
+        CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->h2d_ev.push_back(e);
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(c->dbcA.p, bcA, (size_t)m * 4, cudaMemcpyHostToDevice, c->h2d));
+    for (int i = 0; i < nblk; ++i) {
+        const int r0 = i * rows_blk, r1 = r0 + rows_blk < m ? r0 + rows_blk : m;
+        CUDA_TRY(c, cudaMemcpy2DAsync(dA + (size_t)r0 * Kp, Kp * 8, A + (size_t)r0 * K,
+                                      (size_t)K * 8, (size_t)K * 8, r1 - r0,
+                                      cudaMemcpyHostToDevice, c->h2d));
+        CUDA_TRY(c, cudaEventRecord(c->h2d_ev[i], c->h2d));
+    }
+    Task t{dA, static_cast<const uint32_t *>(c->dbcA.p), m, Kp, dA,
+           static_cast<const uint32_t *>(c->dbcA.p), m, Kp, K, S, 1, band};
+    for (int bi = 0; bi < nblk; ++bi) {
+        const int s = bi & 1;
+        const int b0 = bi * rows_blk, b1 = b0 + rows_blk < m ? b0 + rows_blk : m;
+        // Rows a kernel on B rows [b0, b1) can touch: up to b1 + band plus a tile.
+        const long long need = (long long)b1 + band + 512;
+        const int last_chunk = (int)(((need < m ? need : m) - 1) / rows_blk);
+        CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->h2d_ev[last_chunk], 0));
+        if (bi >= 2) CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_copy[s], 0));
+        float *r2s = static_cast<float *>(c->dOut[s].p);
+        uint32_t *cs = counts_band ? static_cast<uint32_t *>(c->dCnt[s].p) : nullptr;
+        if ((rc = launch_counts(c, t, b0, b1, r2s, band, cs, band, b0, c->stream))) return rc;
+        CUDA_TRY(c, cudaEventRecord(c->ev_band[s], c->stream));
+        CUDA_TRY(c, cudaStreamWaitEvent(c->copy, c->ev_band[s], 0));
+        CUDA_TRY(c, cudaMemcpyAsync(r2_band + (size_t)b0 * band, r2s, (size_t)(b1 - b0) * band * 4,
+                                    cudaMemcpyDeviceToHost, c->copy));
+        if (cs)
+            CUDA_TRY(c, cudaMemcpyAsync(counts_band + (size_t)b0 * band, cs,
+                                        (size_t)(b1 - b0) * band * 4, cudaMemcpyDeviceToHost,
+                                        c->copy));
+        CUDA_TRY(c, cudaEventRecord(c->ev_copy[s], c->copy));
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(c->copy));
+    CUDA_TRY(c, cudaStreamSynchronize(c->h2d));
+    return finish(c, c->stream);
 }
 
 int qld_cuda_ld_batch(qld_ctx *c, const qld_ld_args *jobs, int njobs, void *stream) {
@@ -488,7 +582,7 @@ int qld_cuda_ld_batch(qld_ctx *c, const qld_ld_args *jobs, int njobs, void *stre
             return set_err(c, QLD_ERR_UNSUPPORTED,
                            "batch job %d: K*64 > %d samples (use qld_cuda_ld_device)", j,
                            kMmaMaxSamples);
-        Task t{a.A, a.bcA, a.m, a.lda, a.B, a.bcB, a.n, a.ldb, a.K, a.S, a.symmetric};
+        Task t{a.A, a.bcA, a.m, a.lda, a.B, a.bcB, a.n, a.ldb, a.K, a.S, a.symmetric, 0};
         tiles[j] = (a.m == 0 || a.n == 0) ? 0 : tile_count(t, ks.bm, ks.bn, 0, a.n);
         cost[j] = tiles[j] * (long long)a.K;
         order[j] = j;

@@ -26,6 +26,7 @@ enum R2Mode : int { R2_EXACT = 0, R2_REFERENCE = 1 };
 struct LdParams {
     int m, n, K, S;
     int symmetric;            // only entries with a >= b are produced
+    int band;                 // > 0: only entries with 1 <= a - b <= band (single region)
     int tb0;                  // first B tile of this launch
     int nk;                   // K chunks (of the kernel's chunk width)
     const uint32_t *bcA, *bcB;

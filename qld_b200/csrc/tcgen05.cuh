@@ -99,37 +99,57 @@ struct UnpackTask {
 };
 
 // Tile list of one launch: B tile rows tb in [tb0, tb0 + tiles_b), and in
-// each the A tiles ta in [ta_lo(tb), TA) -- all of them for two regions,
-// those reaching the diagonal (a >= b somewhere) for a single region.
-// Tiles are numbered B-tile-row first.
+// each the A tiles ta in [ta_lo(tb), ta_hi(tb)) -- all of them for two
+// regions, those reaching the diagonal (a >= b somewhere) for a single
+// region, those meeting 1 <= a - b <= band for a band.  Tiles are numbered
+// B-tile-row first.  Used on the host to size grids, on the device to decode.
 template <int BM, int BN>
 struct TileList {
-    int TA, tb0, tiles_b, symmetric;
-    __device__ __forceinline__ int ta_lo(int tb) const {
+    int TA, tb0, tiles_b, symmetric, band;
+    __host__ __device__ __forceinline__ int ta_lo(int tb) const {
+        if (band > 0) {
+            const long long v = (long long)tb * BN + 2 - BM;
+            return v <= 0 ? 0 : (int)((v + BM - 1) / BM);
+        }
         return symmetric ? (tb * BN) / BM : 0;
     }
-    __device__ __forceinline__ int count() const {
+    __host__ __device__ __forceinline__ int ta_hi(int tb) const {
+        if (band > 0) {
+            const long long h = ((long long)band + (long long)tb * BN + BN - 1) / BM + 1;
+            return h < TA ? (int)h : TA;
+        }
+        return TA;
+    }
+    __host__ __device__ __forceinline__ int count() const {
         int n = 0;
         for (int t = 0; t < tiles_b; ++t) {
-            const int c = TA - ta_lo(tb0 + t);
+            const int c = ta_hi(tb0 + t) - ta_lo(tb0 + t);
             n += c > 0 ? c : 0;
         }
         return n;
     }
-    __device__ __forceinline__ void decode(int idx, int &ta, int &tb) const {
+    __host__ __device__ __forceinline__ void decode(int idx, int &ta, int &tb) const {
         for (int t = 0; t < tiles_b; ++t) {
             const int lo = ta_lo(tb0 + t);
-            const int c = TA - lo > 0 ? TA - lo : 0;
-            if (idx < c) {
+            const int c = ta_hi(tb0 + t) - lo;
+            if (c > 0 && idx < c) {
                 ta = lo + idx;
                 tb = tb0 + t;
                 return;
             }
-            idx -= c;
+            idx -= c > 0 ? c : 0;
         }
         ta = tb = -1;
     }
 };
+
+// Diagonal window of the entries a launch produces: dlo <= a - b <= dhi.
+__host__ __device__ __forceinline__ int diag_lo(int symmetric, int band) {
+    return band > 0 ? 1 : (symmetric ? 0 : -2147483647 - 1);
+}
+__host__ __device__ __forceinline__ int diag_hi(int band) {
+    return band > 0 ? band : 2147483647;
+}
 
 
 }  // namespace tc
