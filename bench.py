@@ -47,7 +47,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="single_region",
-                    choices=["single_region", "all_pairs", "batched", "windowed"])
+                    choices=["single_region", "all_pairs", "batched", "windowed", "served"])
+    ap.add_argument("--queries", type=int, default=10000, help="served workload: query count")
+    ap.add_argument("--load", type=float, default=0.8,
+                    help="served workload: offered load as a fraction of measured capacity")
     ap.add_argument("--band", type=int, default=5000, help="windowed workload: band width")
     ap.add_argument("--jobs", type=int, default=4096, help="batched workload: number of tasks")
     ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma"])
@@ -557,6 +560,106 @@ def windowed_arm(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def served_arm(args, rank, world, local_rank):
+    """Served workload: 22 resident chromosomes (50,000-250,000 SNPs x 20,000
+    haplotypes, copying model), a Poisson stream of region-vs-region queries
+    (each side 100-20,000 SNPs, uniform placement), admitted by output memory.
+    The arrival rate is `load` x the capacity measured by a saturated burst."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    from qld_b200 import api, synth
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(5 + rank)
+    H = 20_000
+    srv = api.Server(local_rank, pool_bytes=48 << 30, max_inflight=3)
+    sizes = []
+    for c in range(22):
+        m = int(rng.integers(50_000, 250_001))
+        f = synth.beta_freqs(m, 0.1, 1.0, 100 + c, device=dev, clip_min=1.0 / H)
+        T = synth.copying_table(m, H, 50, 50, 500, 0.01, f, 100 + c, device=dev)
+        bc = synth.popcount_rows(T).to(torch.int32)
+        srv.add_table(T, bc, H)
+        sizes.append(m)
+        del T, bc
+    torch.cuda.synchronize()
+
+    def draw(n):
+        qs = []
+        for _ in range(n):
+            c = int(rng.integers(0, 22))
+            la, lb = (int(x) for x in rng.integers(100, 20_001, 2))
+            a0 = int(rng.integers(0, sizes[c] - la + 1))
+            b0 = int(rng.integers(0, sizes[c] - lb + 1))
+            qs.append((c, a0, a0 + la, b0, b0 + lb))
+        return qs
+
+    def run(qs, rate):
+        """Submit qs (Poisson arrivals at `rate` per second, all at once if
+        rate is None); return results and the wall time to the last one."""
+        results = {}
+        lock = threading.Lock()
+        done_evt = threading.Event()
+
+        def collector():
+            while len(results) < len(qs):
+                for r in srv.poll(wait_ms=50):
+                    with lock:
+                        results[r.id] = r
+                    if r.status == api.OK:
+                        srv.release(r.id)
+            done_evt.set()
+
+        th = threading.Thread(target=collector, daemon=True)
+        t0 = time.perf_counter()
+        th.start()
+        gaps = rng.exponential(1.0 / rate, len(qs)) if rate else np.zeros(len(qs))
+        t_next = t0
+        for q, g in zip(qs, gaps):
+            t_next += g
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            srv.submit(q[0], q[1], q[2], q[3], q[4], threshold=0.2)
+        done_evt.wait(timeout=3600)
+        return results, time.perf_counter() - t0
+
+    warm = draw(max(8, args.warmup * 8))
+    run(warm, None)
+    calib = draw(min(400, max(50, args.queries // 10)))
+    res_c, t_c = run(calib, None)
+    pairs_c = sum(r.pairs for r in res_c.values())
+    capacity_qps = len(calib) / t_c
+    qs = draw(args.queries)
+    res, t = run(qs, args.load * capacity_qps)
+    lat = np.array([r.latency_ms for r in res.values()])
+    pairs = sum(r.pairs for r in res.values())
+    K = (H + 63) // 64
+    line = {"metric": METRIC + ", served queries", "value": pairs / t, "unit": "pairs/s",
+            "n_gpus": world, "steps": 1, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64 popcount / f32 r2", "data": "synthetic",
+            "config": {"workload": f"served_{args.queries}_queries", "chromosomes": 22,
+                       "snps_per_chromosome": "U(50000,250000)", "haplotypes": H,
+                       "query_side_snps": "U(100,20000)", "arrivals": "Poisson",
+                       "offered_load": args.load, "pool_gb": 48, "max_inflight_batches": 3,
+                       "delivered": "per query: count of r2 >= 0.2 (< 100), sum, max; "
+                                    "r2 blocks stay on the device until released"},
+            "bitops_per_s": pairs * 64 * K / t,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                           "p99": float(np.percentile(lat, 99)),
+                           "mean": float(lat.mean()), "max": float(lat.max())},
+            "arrival_qps": args.load * capacity_qps, "completed": len(res),
+            "failed": sum(1 for r in res.values() if r.status != api.OK),
+            "saturated_burst": {"queries": len(calib), "pairs_per_s": pairs_c / t_c}}
+    srv.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -577,6 +680,8 @@ def main():
             batched_arm(args, rank, world, local_rank)
         elif args.workload == "windowed":
             windowed_arm(args, rank, world, local_rank)
+        elif args.workload == "served":
+            served_arm(args, rank, world, local_rank)
         else:
             ours_arm(args, rank, world, local_rank)
     finally:

@@ -152,6 +152,60 @@ int qld_cuda_ld_band_device(qld_ctx *ctx, const uint64_t *A, const uint32_t *bcA
  */
 int qld_cuda_ld_batch(qld_ctx *ctx, const qld_ld_args *jobs, int njobs, void *stream);
 
+/*
+ * Serving: a request loop over chromosome tables resident in HBM.
+ *
+ * qld_srv_create starts a server on `device` with a device output pool of
+ * `pool_bytes`; up to `max_inflight` batches run at once on their own
+ * streams.  qld_srv_add_table copies a packed table (rows of K words, bit
+ * counts, S samples) into HBM once.  qld_srv_submit enqueues a query -- SNP
+ * rows [a0, a1) against rows [b0, b1) of one table (a single region when
+ * the two ranges are equal, else all (a, b) pairs) -- and returns at once.
+ * A worker thread admits pending queries in arrival order while their r^2
+ * outputs ((b1-b0) x (a1-a0) floats) fit in the free pool, packs the
+ * admitted ones into one persistent batched launch (qld_cuda_ld_batch's
+ * kernel) and launches it while earlier batches still run: requests that
+ * arrive while others are on the GPU join the next batch as slots and
+ * memory free up (continuous batching).  Per query the server computes on
+ * the device the pairs with threshold <= r^2 < 100 (the rows qLD's writer
+ * would print at -r2limit threshold, correlate_IO.c:408), the sum of those
+ * r^2 below 100 and their maximum.  If host_r2 is set the full r^2 block is
+ * copied there and the device memory freed; otherwise it stays on the device
+ * until qld_srv_release (qld_srv_fetch copies it).  qld_srv_poll returns
+ * finished queries with their submit-to-ready latency.  No counterpart in
+ * the reference (qLD-compute is a batch tool).
+ */
+typedef struct qld_server qld_server;
+
+typedef struct qld_query {
+    int table;
+    int a0, a1;           /* side A: output columns (the reference's table A) */
+    int b0, b1;           /* side B: output rows (table B) */
+    float threshold;      /* summary threshold on r^2 */
+    float *host_r2;       /* optional (b1-b0) x (a1-a0) host buffer */
+} qld_query;
+
+typedef struct qld_query_result {
+    long long id;
+    int status;           /* QLD_OK, or the error that ended the query */
+    double latency_ms;    /* submit -> summary (and host_r2) ready */
+    long long pairs;      /* r^2 values the query defines */
+    long long n_above;    /* pairs with threshold <= r^2 < 100 */
+    double sum_r2;        /* sum of r^2 < 100 (NaN excluded) */
+    float max_r2;         /* largest r^2 < 100 (0 if none) */
+} qld_query_result;
+
+int qld_srv_create(int device, size_t pool_bytes, int max_inflight, qld_server **srv);
+/* A and bc may be host or device pointers (K words per row, no padding). */
+int qld_srv_add_table(qld_server *srv, const uint64_t *A, const uint32_t *bc, int m, int K,
+                      int S, int *table_id);
+int qld_srv_submit(qld_server *srv, const qld_query *q, long long *id);
+int qld_srv_poll(qld_server *srv, qld_query_result *out, int max, int *count, int wait_ms);
+int qld_srv_fetch(qld_server *srv, long long id, float *host_r2);
+int qld_srv_release(qld_server *srv, long long id);
+int qld_srv_destroy(qld_server *srv);
+const char *qld_srv_last_error(const qld_server *srv);
+
 /* Pinned host memory for tables and results (the -cuda reader allocates its
  * tables here so the host<->device copies run asynchronously). */
 int qld_cuda_host_alloc(qld_ctx *ctx, size_t bytes, void **ptr);

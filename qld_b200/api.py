@@ -35,6 +35,8 @@ EXPORTED = (
     "qld_cuda_ld_band_device", "qld_cuda_sync",
     "qld_cuda_host_alloc",
     "qld_cuda_host_free", "qld_cuda_get_stats", "qld_cuda_measure_popc_peak",
+    "qld_srv_create", "qld_srv_add_table", "qld_srv_submit", "qld_srv_poll", "qld_srv_fetch",
+    "qld_srv_release", "qld_srv_destroy", "qld_srv_last_error",
 )
 
 
@@ -67,6 +69,17 @@ class Stats:
     last_kernel: int
 
 
+class _Query(ct.Structure):
+    _fields_ = [("table", ct.c_int), ("a0", ct.c_int), ("a1", ct.c_int), ("b0", ct.c_int),
+                ("b1", ct.c_int), ("threshold", ct.c_float), ("host_r2", ct.c_void_p)]
+
+
+class _QueryResult(ct.Structure):
+    _fields_ = [("id", ct.c_longlong), ("status", ct.c_int), ("latency_ms", ct.c_double),
+                ("pairs", ct.c_longlong), ("n_above", ct.c_longlong), ("sum_r2", ct.c_double),
+                ("max_r2", ct.c_float)]
+
+
 _lib = None
 
 
@@ -94,6 +107,15 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.qld_cuda_host_free.argtypes = [vp, vp]
     lib.qld_cuda_get_stats.argtypes = [vp, ct.POINTER(_Stats), i]
     lib.qld_cuda_measure_popc_peak.argtypes = [vp, ct.POINTER(ct.c_double)]
+    lib.qld_srv_create.argtypes = [i, ct.c_size_t, i, ct.POINTER(vp)]
+    lib.qld_srv_add_table.argtypes = [vp, vp, vp, i, i, i, ct.POINTER(i)]
+    lib.qld_srv_submit.argtypes = [vp, ct.POINTER(_Query), ct.POINTER(ll)]
+    lib.qld_srv_poll.argtypes = [vp, ct.POINTER(_QueryResult), i, ct.POINTER(i), i]
+    lib.qld_srv_fetch.argtypes = [vp, ll, vp]
+    lib.qld_srv_release.argtypes = [vp, ll]
+    lib.qld_srv_destroy.argtypes = [vp]
+    lib.qld_srv_last_error.argtypes = [vp]
+    lib.qld_srv_last_error.restype = ct.c_char_p
     _lib = lib
     return lib
 
@@ -260,3 +282,80 @@ def _stream(s):
     if isinstance(s, int):
         return s
     return s.cuda_stream  # torch.cuda.Stream
+
+
+@dataclass
+class QueryResult:
+    id: int
+    status: int
+    latency_ms: float
+    pairs: int
+    n_above: int
+    sum_r2: float
+    max_r2: float
+
+
+class Server:
+    """The serving loop (qld_srv_*): resident tables, queries admitted by
+    output memory and batched continuously on the device."""
+
+    def __init__(self, device: int = 0, pool_bytes: int = 8 << 30, max_inflight: int = 3):
+        self.lib = load_library()
+        h = ct.c_void_p()
+        rc = self.lib.qld_srv_create(int(device), int(pool_bytes), int(max_inflight), ct.byref(h))
+        if rc != OK:
+            raise QldError(rc, "qld_srv_create failed")
+        self.h = h
+
+    def _check(self, rc):
+        if rc != OK:
+            raise QldError(rc, self.lib.qld_srv_last_error(self.h).decode(errors="replace"))
+
+    def add_table(self, A, bc, S) -> int:
+        """A: (m, K) uint64 numpy array or contiguous int64 torch tensor (host
+        or device); bc: its row bit counts."""
+        if isinstance(A, np.ndarray):
+            A = np.ascontiguousarray(A).view(np.uint64)
+            bc = np.ascontiguousarray(bc, dtype=np.uint32)
+        tid = ct.c_int()
+        self._check(self.lib.qld_srv_add_table(self.h, _ptr(A), _ptr(bc), A.shape[0], A.shape[1],
+                                               int(S), ct.byref(tid)))
+        return tid.value
+
+    def submit(self, table, a0, a1, b0, b1, threshold=0.2, host_r2=None) -> int:
+        q = _Query(int(table), int(a0), int(a1), int(b0), int(b1), float(threshold),
+                   _ptr(host_r2))
+        qid = ct.c_longlong()
+        self._check(self.lib.qld_srv_submit(self.h, ct.byref(q), ct.byref(qid)))
+        return qid.value
+
+    def poll(self, max_results=256, wait_ms=100):
+        arr = (_QueryResult * max_results)()
+        n = ct.c_int()
+        self._check(self.lib.qld_srv_poll(self.h, arr, max_results, ct.byref(n), int(wait_ms)))
+        return [QueryResult(r.id, r.status, r.latency_ms, r.pairs, r.n_above, r.sum_r2, r.max_r2)
+                for r in arr[:n.value]]
+
+    def fetch(self, qid, out: np.ndarray):
+        self._check(self.lib.qld_srv_fetch(self.h, int(qid), _ptr(out)))
+        return out
+
+    def release(self, qid):
+        self._check(self.lib.qld_srv_release(self.h, int(qid)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.qld_srv_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
