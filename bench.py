@@ -156,6 +156,21 @@ class ClockSampler:
                 "window": "timed region" if inside else "whole run (no sample inside the region)"}
 
 
+def measured_traffic(variant, workload):
+    """DRAM bytes per launch of the counts kernel from the ncu capture
+    summarised under profiles/ (None when no capture covers this case)."""
+    if variant != 2 or workload != "single_region_29817x16622_lower_triangle":
+        return None
+    path = os.path.join(ROOT, "profiles", "k_ld_mma_wide_traffic_16384.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch_full:"):
+                return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 # ------------------------------------------------------------ reference CPU --
 
 def cpu_reference_rate(T_np, S, seconds_target=12.0, threads=None):
@@ -329,7 +344,7 @@ def ours_arm(args, rank, world, local_rank):
                 "unit": "Tbit-op/s", "frac": achieved / (popc_peak / 1e12),
                 "peak_source": "measured: qld_cuda_measure_popc_peak (register-only AND+POPC)"}
     alg_bytes = m * K * 8 * 2 + pairs * 4
-    roof["traffic"] = None
+    roof["traffic"] = measured_traffic(variant, cfg["workload"])
     roof["algorithmic_bytes_per_launch"] = alg_bytes
     roof["kernel_ms"] = kern_ms
     roof["hbm_frac_of_measured"] = (alg_bytes / (kern_ms * 1e-3) / 1e9) / 6538.9
