@@ -1,0 +1,81 @@
+/*
+ * qld_host.h -- C host layer of the -cuda mode: MDF dataset loading into
+ * pinned memory and the text report, both multithreaded (libqld_host.so).
+ *
+ * Formats are qLD's own:
+ *  - an MDF dataset is a directory with <id>_header.vcf.gz (VCF meta line,
+ *    #CHROM ... FORMAT <samples> line, then "<id> snipsPerFile snipSize
+ *    totalSnips posMin posMax": readHeaderFile, src/correlator/src/
+ *    correlate_IO.c:79-259) and parts <id>_<i0>_<i1>_<pos0>_<pos1>.mdf whose
+ *    rows are CHROM POS ID BC w0 w1 ... with decimal 64-bit words
+ *    (writeMDF_x64 / readTable_x64, correlate_IOx64.c:27-122,351-461);
+ *  - the report is writeResultsHeader()/writeResults() (correlate_IO.c:378-429)
+ *    with fprint_f()'s 9-digit truncation (fast_print.c:35-103).
+ * Status codes are qld_cuda.h's.
+ */
+#ifndef QLD_HOST_H
+#define QLD_HOST_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "qld_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct qld_mdf_header {
+    char id[256];          /* alignment id: the header file name up to its first '_' */
+    int snips_per_file;
+    int snip_size;         /* S of the r^2 epilogue */
+    int total_snips;
+    int pos_min, pos_max;
+    int samples;           /* sample names on the #CHROM line */
+} qld_mdf_header;
+
+/* One region read from a dataset: rows in file order, K words each. */
+typedef struct qld_table {
+    uint64_t *words;       /* rows x K: pinned (qld_cuda_host_alloc) when loaded with a
+                              context, else 64-byte aligned pageable memory */
+    uint32_t *bc;          /* the rows' BC field */
+    uint32_t *pos;         /* POS */
+    char **ids;            /* ID strings */
+    char *id_pool;
+    int rows, K;
+    int pinned;            /* words came from qld_cuda_host_alloc */
+} qld_table;
+
+/* Replaces readHeaderFile() (correlate_IO.c:79-259) for an MDF directory. */
+int qld_mdf_read_header(const char *dir, qld_mdf_header *h);
+
+/*
+ * Rows with pos_min <= POS <= pos_max of every part of the dataset, in file
+ * order, K words per row (K = ceil(valid samples / 64)); words past K on a
+ * line must be zero (qLD-parse-2MDF's diploid default writes such padding).
+ * Parts are parsed by `threads` threads and assembled in pinned memory from
+ * `ctx` (ctx NULL: pageable memory, no GPU needed).  Replaces findFiles() + readTable_x64() (correlate_IO.c:294-376,
+ * correlate_IOx64.c:351-461) for MDF input; returns QLD_ERR_INVALID with a
+ * message (qld_host_last_error) for malformed files instead of exiting.
+ */
+int qld_mdf_load(qld_ctx *ctx, const char *dir, int pos_min, int pos_max, int K, int threads,
+                 qld_table *out);
+void qld_table_free(qld_ctx *ctx, qld_table *t);   /* ctx: the one it was loaded with */
+
+/*
+ * The report of one task: header line, then for B row i (outer) and A row j
+ * (inner, j > i for a single region) every r2[i*m + j] with
+ * r2limit <= r^2 < 100 as "POS2\tPOS1\tID2\tID1\tfreq[2]\tfreq[1]\tLD".
+ * Rows are formatted by `threads` threads and written in order.
+ */
+int qld_report_write(FILE *fp, const qld_table *A, const qld_table *B, const float *r2,
+                     int snip_size, float r2limit, int single_region, int threads);
+
+const char *qld_host_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QLD_HOST_H */

@@ -1,10 +1,13 @@
-"""Build libqld_cuda.so in-tree with nvcc for sm_100a (cross-compiles without a GPU).
+"""Build the native libraries in-tree (cross-compiles without a GPU).
 
     python -m qld_b200.build [--verbose]
 
 Every .cu file under csrc/ is compiled for ``-gencode arch=compute_100a,
 code=sm_100a`` and linked into ``qld_b200/libqld_cuda.so`` (static CUDA
 runtime, so the library carries its own runtime independent of torch's).
+The C host layer (host/mdf_loader.c, host/report.c) becomes
+``qld_b200/libqld_host.so`` and host/qld_ld_main.c the ``qld_b200/qld-ld``
+command, both linked against libqld_cuda.so through an $ORIGIN rpath.
 """
 from __future__ import annotations
 
@@ -18,6 +21,10 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libqld_cuda.so")
+HOST = os.path.join(PKG, "host")
+HOST_LIB = os.path.join(PKG, "libqld_host.so")
+CLI = os.path.join(PKG, "qld-ld")
+HOST_FLAGS = ["-O3", "-std=gnu11", "-Wall", "-Wextra", "-Wno-unused-parameter", "-fPIC"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -60,6 +67,37 @@ def build(verbose: bool = False, force: bool = False) -> str:
     return LIB
 
 
+def cc() -> str:
+    for cand in (shutil.which("gcc"), "/usr/bin/gcc", shutil.which("cc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise FileNotFoundError("gcc not found")
+
+
+def build_host(force: bool = False) -> str:
+    """libqld_host.so and qld-ld (needs libqld_cuda.so first)."""
+    lib_srcs = [os.path.join(HOST, f) for f in ("mdf_loader.c", "report.c")]
+    main = os.path.join(HOST, "qld_ld_main.c")
+    deps = (lib_srcs + [main, LIB] + glob.glob(os.path.join(ROOT, "include", "*.h"))
+            + glob.glob(os.path.join(HOST, "*.h")))
+    if (not force and os.path.exists(HOST_LIB) and os.path.exists(CLI)
+            and all(os.path.getmtime(d) <= min(os.path.getmtime(HOST_LIB), os.path.getmtime(CLI))
+                    for d in deps)):
+        return CLI
+    inc = ["-I", os.path.join(ROOT, "include")]
+    link = ["-L", PKG, "-lqld_cuda", "-Wl,-rpath,$ORIGIN", "-lz", "-lpthread"]
+    subprocess.run([cc(), *HOST_FLAGS, *inc, "-shared", "-o", HOST_LIB + ".tmp", *lib_srcs, *link],
+                   check=True)
+    os.replace(HOST_LIB + ".tmp", HOST_LIB)
+    subprocess.run([cc(), *HOST_FLAGS, *inc, "-o", CLI + ".tmp", main, "-L", PKG, "-lqld_host",
+                    *link], check=True)
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
+
+
 if __name__ == "__main__":
     build(verbose="--verbose" in sys.argv, force=True)
+    build_host(force=True)
     print(LIB)
+    print(HOST_LIB)
+    print(CLI)

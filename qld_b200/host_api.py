@@ -1,0 +1,162 @@
+"""ctypes binding of libqld_host.so (include/qld_host.h): MDF loading and
+qLD's text report from Python.
+
+    hdr = host_api.read_header(path)
+    tab = host_api.load_mdf(path, pos_min, pos_max, K, threads=8, ctx=None)
+    host_api.write_report(out_path, tab_a, tab_b, r2, snip_size, r2limit,
+                          single_region, threads=8)
+
+``load_mdf`` returns a ``Table`` (numpy copies of words, BC, POS and IDs) and
+releases the C-side buffers; with a ``api.Context`` the C side assembles in
+pinned memory, with ``ctx=None`` in pageable memory (no GPU needed).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import api
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libqld_host.so")
+CLI_PATH = os.path.join(_PKG, "qld-ld")
+
+
+class _Header(ct.Structure):
+    _fields_ = [("id", ct.c_char * 256), ("snips_per_file", ct.c_int), ("snip_size", ct.c_int),
+                ("total_snips", ct.c_int), ("pos_min", ct.c_int), ("pos_max", ct.c_int),
+                ("samples", ct.c_int)]
+
+
+class _Table(ct.Structure):
+    _fields_ = [("words", ct.POINTER(ct.c_uint64)), ("bc", ct.POINTER(ct.c_uint32)),
+                ("pos", ct.POINTER(ct.c_uint32)), ("ids", ct.POINTER(ct.c_char_p)),
+                ("id_pool", ct.c_char_p), ("rows", ct.c_int), ("K", ct.c_int),
+                ("pinned", ct.c_int)]
+
+
+@dataclass
+class Header:
+    id: str
+    snips_per_file: int
+    snip_size: int
+    total_snips: int
+    pos_min: int
+    pos_max: int
+    samples: int
+
+
+@dataclass
+class Table:
+    words: np.ndarray      # (rows, K) uint64
+    bc: np.ndarray         # (rows,) uint32
+    pos: np.ndarray        # (rows,) uint32
+    ids: list
+
+    @property
+    def rows(self) -> int:
+        return self.words.shape[0]
+
+
+_lib = None
+
+
+def lib() -> ct.CDLL:
+    global _lib
+    if _lib is None:
+        api.load_library()   # libqld_cuda.so first: libqld_host.so resolves against it
+        if not os.path.exists(LIB_PATH):
+            raise api.QldError(api.ERR_INVALID, f"{LIB_PATH} not built (python -m qld_b200.build)")
+        L = ct.CDLL(LIB_PATH)
+        L.qld_mdf_read_header.argtypes = [ct.c_char_p, ct.POINTER(_Header)]
+        L.qld_mdf_read_header.restype = ct.c_int
+        L.qld_mdf_load.argtypes = [ct.c_void_p, ct.c_char_p, ct.c_int, ct.c_int, ct.c_int, ct.c_int,
+                                   ct.POINTER(_Table)]
+        L.qld_mdf_load.restype = ct.c_int
+        L.qld_table_free.argtypes = [ct.c_void_p, ct.POINTER(_Table)]
+        L.qld_table_free.restype = None
+        L.qld_report_write.argtypes = [ct.c_void_p, ct.POINTER(_Table), ct.POINTER(_Table),
+                                       ct.c_void_p, ct.c_int, ct.c_float, ct.c_int, ct.c_int]
+        L.qld_report_write.restype = ct.c_int
+        L.qld_host_last_error.argtypes = []
+        L.qld_host_last_error.restype = ct.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != api.OK:
+        msg = lib().qld_host_last_error()
+        raise api.QldError(rc, msg.decode() if msg else "")
+
+
+def read_header(path: str) -> Header:
+    h = _Header()
+    _check(lib().qld_mdf_read_header(os.fsencode(path), ct.byref(h)))
+    return Header(h.id.decode(), h.snips_per_file, h.snip_size, h.total_snips, h.pos_min,
+                  h.pos_max, h.samples)
+
+
+def load_mdf(path: str, pos_min: int, pos_max: int, K: int, threads: int = 1,
+             ctx: "api.Context | None" = None) -> Table:
+    t = _Table()
+    handle = ctx.h if ctx is not None else None
+    _check(lib().qld_mdf_load(handle, os.fsencode(path), int(pos_min), int(pos_max), int(K),
+                              int(threads), ct.byref(t)))
+    try:
+        n = t.rows
+        words = np.ctypeslib.as_array(t.words, (max(n, 1), K))[:n].copy() if n else \
+            np.zeros((0, K), np.uint64)
+        bc = np.ctypeslib.as_array(t.bc, (n,)).copy() if n else np.zeros(0, np.uint32)
+        pos = np.ctypeslib.as_array(t.pos, (n,)).copy() if n else np.zeros(0, np.uint32)
+        ids = [t.ids[i].decode() for i in range(n)]
+    finally:
+        lib().qld_table_free(handle, ct.byref(t))
+    return Table(words, bc, pos, ids)
+
+
+def _as_c_table(tab: Table, keep: list) -> _Table:
+    t = _Table()
+    n = len(tab.pos)
+    bc = np.ascontiguousarray(tab.bc, np.uint32)
+    pos = np.ascontiguousarray(tab.pos, np.uint32)
+    ids = (ct.c_char_p * max(n, 1))()
+    ids[:n] = [s.encode() for s in tab.ids]
+    keep += [bc, pos, ids]
+    t.words = None
+    t.bc = bc.ctypes.data_as(ct.POINTER(ct.c_uint32))
+    t.pos = pos.ctypes.data_as(ct.POINTER(ct.c_uint32))
+    t.ids = ct.cast(ids, ct.POINTER(ct.c_char_p))
+    t.rows = n
+    t.K = 0
+    return t
+
+
+def write_report(path: str, A: Table, B: Table, r2: np.ndarray, snip_size: int,
+                 r2limit: float, single_region: bool, threads: int = 1) -> None:
+    """qLD's report of one task; r2 is (B rows, A rows) float32."""
+    r2 = np.ascontiguousarray(r2, np.float32)
+    if r2.shape != (len(B.pos), len(A.pos)):
+        raise ValueError(f"r2 is {r2.shape}, expected {(len(B.pos), len(A.pos))}")
+    libc = ct.CDLL(None)
+    libc.fopen.argtypes = [ct.c_char_p, ct.c_char_p]
+    libc.fopen.restype = ct.c_void_p
+    libc.fclose.argtypes = [ct.c_void_p]
+    libc.fclose.restype = ct.c_int
+    keep: list = []
+    ta = _as_c_table(A, keep)
+    tb = ta if B is A else _as_c_table(B, keep)
+    fp = libc.fopen(os.fsencode(path), b"wb")
+    if not fp:
+        raise OSError(f"cannot open {path}")
+    try:
+        rc = lib().qld_report_write(fp, ct.byref(ta), ct.byref(tb), r2.ctypes.data,
+                                    int(snip_size), float(r2limit), int(bool(single_region)),
+                                    int(threads))
+    finally:
+        if libc.fclose(fp) != 0:
+            raise OSError(f"cannot close {path}")
+    _check(rc)

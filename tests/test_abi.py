@@ -1,5 +1,6 @@
-"""CPU tests of the C ABI: the library loads and exports every function
-include/qld_cuda.h declares; init without a GPU fails with a status code."""
+"""CPU tests of the C ABI: each library loads and exports every function its
+header declares (include/qld_cuda.h -> libqld_cuda.so, include/qld_host.h ->
+libqld_host.so); init without a GPU fails with a status code."""
 import ctypes as ct
 import os
 import re
@@ -12,9 +13,12 @@ HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.j
            if f.endswith(".h")]
 
 
-def declared_functions():
+LIBS = {"qld_cuda.h": "libqld_cuda.so", "qld_host.h": "libqld_host.so"}
+
+
+def declared_functions(headers=None):
     names = []
-    for h in HEADERS:
+    for h in headers or HEADERS:
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names += re.findall(r"^\s*(?:const\s+)?\w+[\s*]+(qld_\w+)\s*\(", text, flags=re.M)
@@ -27,14 +31,24 @@ def test_header_declares_functions():
     assert len(names) >= 10
 
 
-def test_library_exports_every_declared_symbol():
+def test_every_header_has_its_library():
+    assert sorted(os.path.basename(h) for h in HEADERS) == sorted(LIBS)
+
+
+@pytest.mark.parametrize("header", sorted(LIBS))
+def test_library_exports_every_declared_symbol(header):
     from qld_b200 import api, build
     build.build()
-    lib = ct.CDLL(api.LIB_PATH)
-    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    build.build_host()
+    api.load_library()                  # libqld_host.so resolves against libqld_cuda.so
+    lib = ct.CDLL(os.path.join(ROOT, "qld_b200", LIBS[header]))
+    names = declared_functions([os.path.join(ROOT, "include", header)])
+    assert names
+    missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, f"not exported: {missing}"
-    for n in api.EXPORTED:
-        assert hasattr(lib, n)
+    if header == "qld_cuda.h":
+        for n in api.EXPORTED:
+            assert hasattr(lib, n)
 
 
 def test_init_without_gpu_returns_status():

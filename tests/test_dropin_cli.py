@@ -93,8 +93,9 @@ def test_two_inputs_report_identical(dataset):
 
 def test_split_file_inputs_report_identical(dataset):
     """Two inputs over the same window: qLD sets posWset2 = 0 with a
-    different table B (load_balancer.c:262-268); the fallback gemm() computes
-    A x B and the writer prints the triangle -- so does correlate_cuda()."""
+    different table B (load_balancer.c:262-268), which readTable_x64() then
+    reads only up to each part's column-name line (correlate_IOx64.c:444):
+    correlate() gets an empty table B and both reports are the header alone."""
     tmp, d1, _, d3 = dataset
     ref, cuda = _reports(tmp, "split", ["-input", d1, "-input2", d3, "-ploidy", "haploid",
                                         "-mdf", "-posWmin1", "1000", "-posWmax1", "6990",
