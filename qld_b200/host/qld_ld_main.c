@@ -9,8 +9,10 @@
  * -posWmin2/-posWmax2, -r2limit, -threads; plus -device, -r2mode
  * reference|exact (default reference: the report is byte-identical to
  * qLD-compute's) and -timing (per-task phase times as JSON on stderr).
- * -competing, -sorted, -rTable, -gpu and -seed are accepted and change
- * nothing (scheduling switches); -sampleList is not supported.
+ * -competing, -sorted, -rTable and -gpu are accepted and change nothing
+ * (scheduling switches); -sampleList is not supported; -seed is rejected as
+ * qLD-compute rejects it (its parser falls through to the invalid-parameter
+ * error, correlate_our_kernel.c:387-392,434-436).
  * Window resolution is preprocess_data()'s (load_balancer.c:122-345), the
  * single-region / two-table choice and the "input2 equals input" rule are
  * correlate_function()'s (correlate_function.c:94-104,239-295), and
@@ -304,7 +306,6 @@ int main(int argc, char **argv)
         else if (!strcmp(a, "-r2limit")) r2limit = (float)atof(v);
         else if (!strcmp(a, "-threads")) threads = atoi(v);
         else if (!strcmp(a, "-device")) device = atoi(v);
-        else if (!strcmp(a, "-seed")) { /* qLD's srand() seed: nothing here is random */ }
         else if (!strcmp(a, "-ploidy")) {
             if (!strcmp(v, "haploid")) ploidy = 1;
             else if (!strcmp(v, "phased_diploid") || !strcmp(v, "unphased_diploid")) ploidy = 2;

@@ -158,5 +158,7 @@ def test_cli_argument_errors(dataset, tmp_path):
     assert r.returncode == 1
     r = _cli("-input", path, "-ploidy", "haploid", "-mdf", "-bogus", "1")
     assert r.returncode == 1 and "not a valid" in r.stderr
+    r = _cli("-input", path, "-ploidy", "haploid", "-mdf", "-seed", "3")
+    assert r.returncode == 1 and "not a valid" in r.stderr
     r = _cli("-help")
     assert r.returncode == 0 and "usage" in r.stdout
