@@ -121,6 +121,30 @@ int qld_cuda_ld_device(qld_ctx *ctx, const qld_ld_args *args, void *stream);
 int qld_cuda_sync(qld_ctx *ctx, void *stream);
 
 /*
+ * The report's pairs only, filtered on the GPU.  Computes the task as
+ * qld_cuda_ld() does, one block of QLD_OPT_BAND_ROWS B rows at a time, and
+ * keeps the pairs qLD's writeResults() prints (src/correlator/src/
+ * correlate_IO.c:403-409): r2limit <= r^2 < 100, and with `triangle` only
+ * j > i (qLD's posWset2 == 0; implied by `symmetric`).  Each block crosses
+ * PCIe as a bit mask (m/8 bytes per row) plus the passing values, and is
+ * handed to `fn` on the calling thread while the GPU computes the next
+ * block.  The block's arrays are valid during the call only.  `fn` returns 0
+ * to go on; any other value stops the task and is returned.
+ */
+typedef struct qld_hits_block {
+    int row0, rows;            /* B rows [row0, row0 + rows) */
+    int m;                     /* columns: A rows */
+    int words;                 /* mask words per row: ceil(m / 32) */
+    const uint32_t *mask;      /* rows x words: bit (j & 31) of word j >> 5 set <=> (row, j) kept */
+    const long long *row_off;  /* rows + 1 offsets into val, row_off[0] == 0 */
+    const float *val;          /* the kept r^2 of each row, in column order */
+} qld_hits_block;
+typedef int (*qld_hits_fn)(void *user, const qld_hits_block *block);
+int qld_cuda_ld_hits(qld_ctx *ctx, const uint64_t *A, const uint32_t *bcA, int m,
+                     const uint64_t *B, const uint32_t *bcB, int n, int K, int S, int symmetric,
+                     int triangle, float r2limit, qld_hits_fn fn, void *user);
+
+/*
  * Windowed (band) LD over one region: r^2 only for SNP pairs (i, j) with
  * 1 <= j - i <= band.  Output is the m x band array r2_band[i*band + d] =
  * r^2(SNP i, SNP i+1+d) (entries with i+1+d >= m are unspecified); counts_band
@@ -219,6 +243,8 @@ typedef struct qld_stats {
     long long kernel_launches;
     double counts_kernel_ms;
     int last_kernel;           /* QLD_KERNEL_* used by the last call */
+    long long hits_rows;       /* qld_cuda_ld_hits: B rows delivered */
+    long long hits_pairs;      /* qld_cuda_ld_hits: kept pairs delivered */
 } qld_stats;
 
 int qld_cuda_get_stats(qld_ctx *ctx, qld_stats *out, int reset);

@@ -72,6 +72,18 @@ void qld_table_free(qld_ctx *ctx, qld_table *t);   /* ctx: the one it was loaded
 int qld_report_write(FILE *fp, const qld_table *A, const qld_table *B, const float *r2,
                      int snip_size, float r2limit, int single_region, int threads);
 
+/*
+ * The same report, streamed from qld_cuda_ld_hits blocks: open writes the
+ * header line and formats the tables' per-row text once; each call of
+ * qld_report_hits appends the rows of one block (blocks in B-row order, as
+ * qld_cuda_ld_hits delivers them; it can be called from its callback).
+ */
+typedef struct qld_report qld_report;
+int qld_report_open(qld_report **rep, FILE *fp, const qld_table *A, const qld_table *B,
+                    int snip_size, int threads);
+int qld_report_hits(qld_report *rep, const qld_hits_block *block);
+int qld_report_close(qld_report *rep);
+
 const char *qld_host_last_error(void);
 
 #ifdef __cplusplus

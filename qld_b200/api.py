@@ -31,7 +31,8 @@ OPT_KERNEL, OPT_R2_MODE, OPT_PROFILE, OPT_BAND_ROWS, OPT_MMA_TILE = 1, 2, 3, 4, 
 
 EXPORTED = (
     "qld_cuda_init", "qld_cuda_release", "qld_cuda_last_error", "qld_cuda_set_option",
-    "qld_cuda_ld", "qld_cuda_ld_device", "qld_cuda_ld_batch", "qld_cuda_ld_band",
+    "qld_cuda_ld", "qld_cuda_ld_device", "qld_cuda_ld_hits", "qld_cuda_ld_batch",
+    "qld_cuda_ld_band",
     "qld_cuda_ld_band_device", "qld_cuda_sync",
     "qld_cuda_host_alloc",
     "qld_cuda_host_free", "qld_cuda_get_stats", "qld_cuda_measure_popc_peak",
@@ -58,7 +59,8 @@ class _LdArgs(ct.Structure):
 
 class _Stats(ct.Structure):
     _fields_ = [("counts_launches", ct.c_longlong), ("kernel_launches", ct.c_longlong),
-                ("counts_kernel_ms", ct.c_double), ("last_kernel", ct.c_int)]
+                ("counts_kernel_ms", ct.c_double), ("last_kernel", ct.c_int),
+                ("hits_rows", ct.c_longlong), ("hits_pairs", ct.c_longlong)]
 
 
 @dataclass
@@ -67,6 +69,18 @@ class Stats:
     kernel_launches: int
     counts_kernel_ms: float
     last_kernel: int
+    hits_rows: int = 0
+    hits_pairs: int = 0
+
+
+class HitsBlock(ct.Structure):
+    """qld_hits_block: one block of B rows of qld_cuda_ld_hits."""
+    _fields_ = [("row0", ct.c_int), ("rows", ct.c_int), ("m", ct.c_int), ("words", ct.c_int),
+                ("mask", ct.POINTER(ct.c_uint32)), ("row_off", ct.POINTER(ct.c_longlong)),
+                ("val", ct.POINTER(ct.c_float))]
+
+
+HITS_FN = ct.CFUNCTYPE(ct.c_int, ct.c_void_p, ct.POINTER(HitsBlock))
 
 
 class _Query(ct.Structure):
@@ -100,6 +114,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.qld_cuda_ld.argtypes = [vp, vp, vp, i, vp, vp, i, i, i, i, vp, vp]
     lib.qld_cuda_ld_device.argtypes = [vp, ct.POINTER(_LdArgs), vp]
     lib.qld_cuda_ld_batch.argtypes = [vp, ct.POINTER(_LdArgs), i, vp]
+    lib.qld_cuda_ld_hits.argtypes = [vp, vp, vp, i, vp, vp, i, i, i, i, i, ct.c_float, HITS_FN, vp]
     lib.qld_cuda_ld_band.argtypes = [vp, vp, vp, i, i, i, i, vp, vp]
     lib.qld_cuda_ld_band_device.argtypes = [vp, vp, vp, i, ll, i, i, i, vp, ll, vp, ll, vp]
     lib.qld_cuda_sync.argtypes = [vp, vp]
@@ -171,7 +186,8 @@ class Context:
     def stats(self, reset: bool = False) -> Stats:
         s = _Stats()
         self._check(self.lib.qld_cuda_get_stats(self.h, ct.byref(s), int(reset)))
-        return Stats(s.counts_launches, s.kernel_launches, s.counts_kernel_ms, s.last_kernel)
+        return Stats(s.counts_launches, s.kernel_launches, s.counts_kernel_ms, s.last_kernel,
+                     s.hits_rows, s.hits_pairs)
 
     def measure_popc_peak(self) -> float:
         """Measured popcount-pipe peak in bit-ops/s."""
@@ -220,6 +236,65 @@ class Context:
         self._check(self.lib.qld_cuda_ld(self.h, _ptr(A), _ptr(bcA), m, _ptr(B), _ptr(bcB), n,
                                          K, int(S), int(bool(symmetric)), _ptr(r2_out), _ptr(cnt)))
         return (r2_out, cnt) if cnt is not None else r2_out
+
+    def ld_hits(self, A, bcA, B=None, bcB=None, *, S: int, r2limit: float,
+                symmetric: bool | None = None, triangle: bool | None = None,
+                on_block=None):
+        """The report's pairs of one task, filtered on the GPU.
+
+        Without `on_block`: returns (mask (n, ceil(m/32)) uint32, row_off (n+1,)
+        int64, val (total,) float32) for the whole task.  With `on_block`, it
+        is called with each HitsBlock (valid during the call) and may return a
+        nonzero int to stop.  triangle defaults to symmetric."""
+        if symmetric is None:
+            symmetric = B is None
+        if triangle is None:
+            triangle = symmetric
+        A = np.ascontiguousarray(A).view(np.uint64)
+        bcA = np.ascontiguousarray(bcA, dtype=np.uint32)
+        m, K = A.shape
+        if symmetric:
+            B, bcB, n = A, bcA, m
+        else:
+            B = np.ascontiguousarray(B).view(np.uint64)
+            bcB = np.ascontiguousarray(bcB, dtype=np.uint32)
+            n = B.shape[0]
+        W = (m + 31) // 32
+        masks, offs, vals = [], [np.zeros(1, np.int64)], []
+        err: list = []
+
+        def cb(_user, bp):
+            try:
+                b = bp.contents
+                if on_block is not None:
+                    return int(on_block(b) or 0)
+                mk = np.ctypeslib.as_array(b.mask, (b.rows * b.words,)).reshape(b.rows, b.words)
+                of = np.ctypeslib.as_array(b.row_off, (b.rows + 1,))
+                tot = int(of[b.rows])
+                masks.append(mk.copy())
+                offs.append(of[1:] + offs[-1][-1])
+                vals.append(np.ctypeslib.as_array(b.val, (tot,)).copy() if tot else
+                            np.zeros(0, np.float32))
+                return 0
+            except Exception as e:   # surface Python errors after the call
+                err.append(e)
+                return -100
+
+        fn = HITS_FN(cb)
+        rc = self.lib.qld_cuda_ld_hits(self.h, _ptr(A), _ptr(bcA), m, _ptr(B), _ptr(bcB), n, K,
+                                       int(S), int(bool(symmetric)), int(bool(triangle)),
+                                       float(r2limit), fn, None)
+        if err:
+            raise err[0]
+        if on_block is not None and rc > 0:
+            return rc
+        self._check(rc)
+        if on_block is not None:
+            return 0
+        mask = np.concatenate(masks) if masks else np.zeros((0, W), np.uint32)
+        row_off = np.concatenate(offs)
+        val = np.concatenate(vals) if vals else np.zeros(0, np.float32)
+        return mask, row_off, val
 
     # ------------------------------------------------------------ device --
     def ld_device(self, A, bcA, m, lda, B, bcB, n, ldb, K, S, symmetric, r2, ldr,

@@ -29,6 +29,11 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+struct HostBuf {   // pinned
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
 }  // namespace
 
 struct qld_ctx {
@@ -52,6 +57,10 @@ struct qld_ctx {
     std::vector<BatchJob> hJobs;
     cudaEvent_t ev_band[2] = {nullptr, nullptr};
     cudaEvent_t ev_copy[2] = {nullptr, nullptr};
+    // qld_cuda_ld_hits: per slot the device mask / counts / offsets / values
+    // and their pinned host mirrors
+    DevBuf dMask[2], dHcnt[2], dHoff[2], dHval[2];
+    HostBuf hMask[2], hOff[2], hVal[2], hStat;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
     size_t prof_used = 0;
     qld_stats stats{};
@@ -92,6 +101,21 @@ int ensure(qld_ctx *c, DevBuf &b, size_t bytes) {
             return set_err(c, QLD_ERR_NOMEM, "cudaMalloc(%zu) failed", bytes);
         }
         want = bytes;
+    }
+    b.bytes = want;
+    return QLD_OK;
+}
+
+int ensure_host(qld_ctx *c, HostBuf &b, size_t bytes) {
+    if (bytes <= b.bytes) return QLD_OK;
+    if (b.p) cudaFreeHost(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    const size_t want = bytes + bytes / 4;
+    if (cudaMallocHost(&b.p, want) != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        return set_err(c, QLD_ERR_NOMEM, "cudaMallocHost(%zu) failed", want);
     }
     b.bytes = want;
     return QLD_OK;
@@ -245,6 +269,34 @@ int finish(qld_ctx *c, cudaStream_t st) {
 
 bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// Copy host tables into the context's device buffers (rows padded to an even
+// word count, 16-byte aligned for TMA) on c->stream; *t describes them.
+int stage_tables(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const uint64_t *B,
+                 const uint32_t *bcB, int n, int K, int S, int symmetric, Task *t) {
+    const long long Kp = K + (K & 1);
+    int rc;
+    if ((rc = ensure(c, c->dA, (size_t)m * Kp * 8)) || (rc = ensure(c, c->dbcA, (size_t)m * 4)))
+        return rc;
+    CUDA_TRY(c, cudaMemcpy2DAsync(c->dA.p, Kp * 8, A, (size_t)K * 8, (size_t)K * 8, m,
+                                  cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->dbcA.p, bcA, (size_t)m * 4, cudaMemcpyHostToDevice, c->stream));
+    const uint64_t *dB = static_cast<const uint64_t *>(c->dA.p);
+    const uint32_t *dbcB = static_cast<const uint32_t *>(c->dbcA.p);
+    if (!symmetric) {
+        if ((rc = ensure(c, c->dB, (size_t)n * Kp * 8)) || (rc = ensure(c, c->dbcB, (size_t)n * 4)))
+            return rc;
+        CUDA_TRY(c, cudaMemcpy2DAsync(c->dB.p, Kp * 8, B, (size_t)K * 8, (size_t)K * 8, n,
+                                      cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(c->dbcB.p, bcB, (size_t)n * 4, cudaMemcpyHostToDevice,
+                                    c->stream));
+        dB = static_cast<const uint64_t *>(c->dB.p);
+        dbcB = static_cast<const uint32_t *>(c->dbcB.p);
+    }
+    *t = Task{static_cast<const uint64_t *>(c->dA.p), static_cast<const uint32_t *>(c->dbcA.p), m,
+              Kp, dB, dbcB, n, Kp, K, S, symmetric, 0};
+    return QLD_OK;
+}
+
 }  // namespace
 
 // ================================================================== C ABI ==
@@ -310,10 +362,16 @@ int qld_cuda_release(qld_ctx *c) {
     if (c->copy) cudaStreamSynchronize(c->copy);
     if (c->h2d) cudaStreamSynchronize(c->h2d);
     for (cudaEvent_t e : c->h2d_ev) cudaEventDestroy(e);
-    DevBuf *bufs[] = {&c->dA, &c->dB, &c->dbcA, &c->dbcB, &c->dOut[0], &c->dOut[1],
-                      &c->dCnt[0], &c->dCnt[1], &c->dJobs, &c->dQueue};
+    DevBuf *bufs[] = {&c->dA,       &c->dB,       &c->dbcA,     &c->dbcB,     &c->dOut[0],
+                      &c->dOut[1],  &c->dCnt[0],  &c->dCnt[1],  &c->dJobs,    &c->dQueue,
+                      &c->dMask[0], &c->dMask[1], &c->dHcnt[0], &c->dHcnt[1], &c->dHoff[0],
+                      &c->dHoff[1], &c->dHval[0], &c->dHval[1]};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
+    HostBuf *hbufs[] = {&c->hMask[0], &c->hMask[1], &c->hOff[0], &c->hOff[1],
+                        &c->hVal[0],  &c->hVal[1],  &c->hStat};
+    for (HostBuf *b : hbufs)
+        if (b->p) cudaFreeHost(b->p);
     for (auto &e : c->prof) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
@@ -403,27 +461,9 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
     if (!A || !bcA || !B || !bcB || !r2_out)
         return set_err(c, QLD_ERR_INVALID, "NULL table, bit-count or output pointer");
     CUDA_TRY(c, cudaSetDevice(c->device));
-    const long long Kp = K + (K & 1);
+    Task t;
     int rc;
-    if ((rc = ensure(c, c->dA, (size_t)m * Kp * 8)) || (rc = ensure(c, c->dbcA, (size_t)m * 4)))
-        return rc;
-    CUDA_TRY(c, cudaMemcpy2DAsync(c->dA.p, Kp * 8, A, (size_t)K * 8, (size_t)K * 8, m,
-                                  cudaMemcpyHostToDevice, c->stream));
-    CUDA_TRY(c, cudaMemcpyAsync(c->dbcA.p, bcA, (size_t)m * 4, cudaMemcpyHostToDevice, c->stream));
-    const uint64_t *dB = static_cast<const uint64_t *>(c->dA.p);
-    const uint32_t *dbcB = static_cast<const uint32_t *>(c->dbcA.p);
-    if (!symmetric) {
-        if ((rc = ensure(c, c->dB, (size_t)n * Kp * 8)) || (rc = ensure(c, c->dbcB, (size_t)n * 4)))
-            return rc;
-        CUDA_TRY(c, cudaMemcpy2DAsync(c->dB.p, Kp * 8, B, (size_t)K * 8, (size_t)K * 8, n,
-                                      cudaMemcpyHostToDevice, c->stream));
-        CUDA_TRY(c, cudaMemcpyAsync(c->dbcB.p, bcB, (size_t)n * 4, cudaMemcpyHostToDevice,
-                                    c->stream));
-        dB = static_cast<const uint64_t *>(c->dB.p);
-        dbcB = static_cast<const uint32_t *>(c->dbcB.p);
-    }
-    Task t{static_cast<const uint64_t *>(c->dA.p), static_cast<const uint32_t *>(c->dbcA.p), m, Kp,
-           dB, dbcB, n, Kp, K, S, symmetric, 0};
+    if ((rc = stage_tables(c, A, bcA, m, B, bcB, n, K, S, symmetric, &t))) return rc;
 
     const int band = c->band_rows;  // multiple of 256: whole tile rows of every variant
     const int nbands = (n + band - 1) / band;
@@ -467,6 +507,108 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
     }
     CUDA_TRY(c, cudaStreamSynchronize(c->copy));
     return finish(c, c->stream);
+}
+
+int qld_cuda_ld_hits(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m,
+                     const uint64_t *B, const uint32_t *bcB, int n, int K, int S, int symmetric,
+                     int triangle, float r2limit, qld_hits_fn fn, void *user) {
+    if (!c) return QLD_ERR_INVALID;
+    if (symmetric) { B = A; bcB = bcA; n = m; triangle = 1; }
+    if (m < 0 || n < 0 || K < 1 || S < 1)
+        return set_err(c, QLD_ERR_INVALID, "bad sizes m=%d n=%d K=%d S=%d", m, n, K, S);
+    if (!fn) return set_err(c, QLD_ERR_INVALID, "NULL block callback");
+    if (m == 0 || n == 0) return QLD_OK;
+    if (!A || !bcA || !B || !bcB)
+        return set_err(c, QLD_ERR_INVALID, "NULL table or bit-count pointer");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    Task t;
+    int rc;
+    if ((rc = stage_tables(c, A, bcA, m, B, bcB, n, K, S, symmetric, &t))) return rc;
+
+    const int rows_blk = n < c->band_rows ? n : c->band_rows;
+    const int nblk = (n + c->band_rows - 1) / c->band_rows;
+    const long long ldr = ((long long)m + 127) / 128 * 128;   // float4 groups of 128 columns
+    const int W = (m + 31) / 32;
+    for (int s = 0; s < 2 && s < nblk; ++s) {
+        if ((rc = ensure(c, c->dOut[s], (size_t)rows_blk * ldr * 4)) ||
+            (rc = ensure(c, c->dMask[s], (size_t)rows_blk * W * 4)) ||
+            (rc = ensure(c, c->dHcnt[s], (size_t)rows_blk * 8)) ||
+            (rc = ensure(c, c->dHoff[s], (size_t)(rows_blk + 1) * 8)) ||
+            (rc = ensure(c, c->dHval[s], (size_t)rows_blk * m * 4)) ||
+            (rc = ensure_host(c, c->hMask[s], (size_t)rows_blk * W * 4)) ||
+            (rc = ensure_host(c, c->hOff[s], (size_t)(rows_blk + 1) * 8)))
+            return rc;
+    }
+    if ((rc = ensure_host(c, c->hStat, 2 * sizeof(unsigned)))) return rc;
+    unsigned *hstat = static_cast<unsigned *>(c->hStat.p);
+
+    // Block bi: counts + r^2 into dOut[s], the filter, then (copy stream)
+    // the offsets, the mask and the status word to the host.
+    auto issue = [&](int bi) -> int {
+        const int s = bi & 1;
+        const int b0 = bi * c->band_rows, b1 = b0 + c->band_rows < n ? b0 + c->band_rows : n;
+        float *r2s = static_cast<float *>(c->dOut[s].p);
+        int rc2;
+        if ((rc2 = launch_counts(c, t, b0, b1, r2s, ldr, nullptr, 0, b0, c->stream))) return rc2;
+        cudaError_t e = launch_hits(r2s, ldr, b1 - b0, m, b0, triangle, r2limit,
+                                    static_cast<uint32_t *>(c->dMask[s].p),
+                                    W, static_cast<long long *>(c->dHcnt[s].p),
+                                    static_cast<long long *>(c->dHoff[s].p),
+                                    static_cast<float *>(c->dHval[s].p), c->stream);
+        if (e != cudaSuccess)
+            return set_err(c, QLD_ERR_CUDA, "filter launch failed: %s", cudaGetErrorString(e));
+        c->stats.kernel_launches += 3;
+        CUDA_TRY(c, cudaEventRecord(c->ev_band[s], c->stream));
+        CUDA_TRY(c, cudaStreamWaitEvent(c->copy, c->ev_band[s], 0));
+        CUDA_TRY(c, cudaMemcpyAsync(c->hOff[s].p, c->dHoff[s].p, (size_t)(b1 - b0 + 1) * 8,
+                                    cudaMemcpyDeviceToHost, c->copy));
+        CUDA_TRY(c, cudaMemcpyAsync(c->hMask[s].p, c->dMask[s].p, (size_t)(b1 - b0) * W * 4,
+                                    cudaMemcpyDeviceToHost, c->copy));
+        CUDA_TRY(c, cudaMemcpyAsync(hstat + s, c->d_status, sizeof(unsigned),
+                                    cudaMemcpyDeviceToHost, c->copy));
+        CUDA_TRY(c, cudaEventRecord(c->ev_copy[s], c->copy));
+        return QLD_OK;
+    };
+    // Wait for block bi's offsets and mask, fetch its values, call fn.
+    auto consume = [&](int bi) -> int {
+        const int s = bi & 1;
+        const int b0 = bi * c->band_rows, b1 = b0 + c->band_rows < n ? b0 + c->band_rows : n;
+        CUDA_TRY(c, cudaEventSynchronize(c->ev_copy[s]));
+        if (hstat[s]) return QLD_ERR_TIMEOUT;
+        const long long *off = static_cast<const long long *>(c->hOff[s].p);
+        const long long total = off[b1 - b0];
+        int rc2;
+        if ((rc2 = ensure_host(c, c->hVal[s], (size_t)(total > 0 ? total : 1) * 4))) return rc2;
+        if (total > 0) {
+            CUDA_TRY(c, cudaMemcpyAsync(c->hVal[s].p, c->dHval[s].p, (size_t)total * 4,
+                                        cudaMemcpyDeviceToHost, c->copy));
+            CUDA_TRY(c, cudaStreamSynchronize(c->copy));
+        }
+        qld_hits_block blk;
+        blk.row0 = b0;
+        blk.rows = b1 - b0;
+        blk.m = m;
+        blk.words = W;
+        blk.mask = static_cast<const uint32_t *>(c->hMask[s].p);
+        blk.row_off = off;
+        blk.val = static_cast<const float *>(c->hVal[s].p);
+        c->stats.hits_rows += blk.rows;
+        c->stats.hits_pairs += total;
+        return fn(user, &blk);
+    };
+    rc = issue(0);
+    for (int bi = 1; rc == QLD_OK && bi <= nblk; ++bi) {
+        if (bi < nblk && (rc = issue(bi))) break;
+        rc = consume(bi - 1);
+    }
+    // Drain whatever is still queued, then report a kernel that gave up.
+    cudaStreamSynchronize(c->stream);
+    cudaStreamSynchronize(c->copy);
+    const int frc = finish(c, c->stream);
+    if (rc == QLD_ERR_TIMEOUT || (rc == QLD_OK && frc != QLD_OK))
+        return frc != QLD_OK ? frc
+                             : set_err(c, QLD_ERR_TIMEOUT, "a counts kernel gave up a bounded wait");
+    return rc;
 }
 
 int qld_cuda_ld_device(qld_ctx *c, const qld_ld_args *a, void *stream) {

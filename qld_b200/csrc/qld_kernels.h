@@ -60,4 +60,12 @@ extern const KernelShape kBatchShape;
 // Persistent batched launch over all items of bp.jobs (max_ctas > 0 caps the grid).
 cudaError_t launch_batch(const BatchParams &bp, int r2_mode, int max_ctas, cudaStream_t st);
 
+// Report filter over `rows` r^2 rows (ldr >= m rounded up to 128 floats,
+// 16-byte aligned rows): mask (rows x W words, W = ceil(m / 32)), per-row
+// counts, offsets (rows + 1) and the kept values (hits.cu).  Row r is B row
+// row0 + r; with `triangle` only columns j > row0 + r are kept.
+cudaError_t launch_hits(const float *r2, long long ldr, int rows, int m, int row0, int triangle,
+                        float r2limit, uint32_t *mask, int W, long long *cnt, long long *off,
+                        float *val, cudaStream_t st);
+
 }  // namespace qld

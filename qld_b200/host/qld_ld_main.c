@@ -8,7 +8,10 @@
  * -input2, -inputList, -output, -ploidy, -mdf, -posWmin1/-posWmax1/
  * -posWmin2/-posWmax2, -r2limit, -threads; plus -device, -r2mode
  * reference|exact (default reference: the report is byte-identical to
- * qLD-compute's) and -timing (per-task phase times as JSON on stderr).
+ * qLD-compute's), -filter gpu|host (default gpu: qld_cuda_ld_hits keeps the
+ * report's pairs on the device and only they cross PCIe; host: the dense r^2
+ * array comes back and report.c filters it) and -timing (per-task phase
+ * times as JSON on stderr).
  * -competing, -sorted, -rTable and -gpu are accepted and change nothing
  * (scheduling switches); -sampleList is not supported; -seed is rejected as
  * qLD-compute rejects it (its parser falls through to the invalid-parameter
@@ -59,8 +62,8 @@ static void usage(FILE *f)
     fputs("usage: qld-ld -input DIR [-input2 DIR] -output FILE -ploidy haploid|phased_diploid|"
           "unphased_diploid -mdf\n"
           "              [-posWmin1 P -posWmax1 P -posWmin2 P -posWmax2 P] [-inputList CSV]\n"
-          "              [-r2limit R] [-threads T] [-device D] [-r2mode reference|exact]"
-          " [-timing]\n",
+          "              [-r2limit R] [-threads T] [-device D] [-r2mode reference|exact]\n"
+          "              [-filter gpu|host] [-timing]\n",
           f);
 }
 
@@ -263,11 +266,94 @@ static int read_list(const char *path, const task *base, task **tasks, int *ntas
     return ts ? 0 : -1;
 }
 
+/* Report callback of qld_cuda_ld_hits: append the block's rows. */
+typedef struct hits_arg {
+    qld_report *rep;
+    int host_failed;
+    double rep_s;
+} hits_arg;
+
+static int on_block(void *user, const qld_hits_block *blk)
+{
+    hits_arg *h = user;
+    const double t0 = now_s();
+    const int rc = qld_report_hits(h->rep, blk);
+    h->rep_s += now_s() - t0;
+    if (rc != QLD_OK)
+        h->host_failed = 1;
+    return rc;
+}
+
+/* The task with the report filter on the GPU: only the kept pairs cross
+ * PCIe, and each block is formatted while the GPU computes the next. */
+static int run_filtered(qld_ctx *ctx, const loaded *l, const char *out, float r2limit,
+                        int threads, double *ld_s, double *rep_s)
+{
+    const qld_table *A = &l->A, *B = l->single ? &l->A : &l->B;
+    FILE *fp = fopen(out, "wb");
+    if (!fp) {
+        fprintf(stderr, "ERROR: cannot write %s\n", out);
+        return 1;
+    }
+    const double t0 = now_s();
+    hits_arg h = {NULL, 0, 0.0};
+    int rc = qld_report_open(&h.rep, fp, A, B, l->S, threads);
+    if (rc == QLD_OK && A->rows && B->rows)
+        rc = qld_cuda_ld_hits(ctx, A->words, A->bc, A->rows, B->words, B->bc, B->rows, l->K, l->S,
+                              l->single, l->tri, r2limit, on_block, &h);
+    if (rc != QLD_OK)
+        fprintf(stderr, "ERROR: %s: %s\n", out,
+                (h.host_failed || !h.rep) ? qld_host_last_error() : qld_cuda_last_error(ctx));
+    qld_report_close(h.rep);
+    if (fclose(fp) != 0)
+        rc = QLD_ERR_INVALID;
+    *ld_s = now_s() - t0;
+    *rep_s = h.rep_s;
+    return rc != QLD_OK;
+}
+
+/* The task with a dense r^2 array copied back and filtered on the host. */
+static int run_dense(qld_ctx *ctx, const loaded *l, const char *out, float r2limit, int threads,
+                     double *ld_s, double *rep_s)
+{
+    const qld_table *A = &l->A, *B = l->single ? &l->A : &l->B;
+    const double t0 = now_s();
+    float *r2 = NULL;
+    const size_t cells = (size_t)A->rows * (size_t)B->rows;
+    int rc = cells ? qld_cuda_host_alloc(ctx, cells * sizeof(float), (void **)&r2) : QLD_OK;
+    if (rc == QLD_OK && cells)
+        rc = qld_cuda_ld(ctx, A->words, A->bc, A->rows, B->words, B->bc, B->rows, l->K, l->S,
+                         l->single, r2, NULL);
+    *ld_s = now_s() - t0;
+    int bad = 0;
+    FILE *fp = NULL;
+    if (rc != QLD_OK) {
+        fprintf(stderr, "ERROR: %s: %s\n", out, qld_cuda_last_error(ctx));
+        bad = 1;
+    } else if (!(fp = fopen(out, "wb"))) {
+        fprintf(stderr, "ERROR: cannot write %s\n", out);
+        bad = 1;
+    } else {
+        const double t1 = now_s();
+        if (qld_report_write(fp, A, B, r2, l->S, r2limit, l->tri, threads) != QLD_OK) {
+            fprintf(stderr, "ERROR: %s: %s\n", out, qld_host_last_error());
+            bad = 1;
+        }
+        if (fclose(fp) != 0)
+            bad = 1;
+        *rep_s = now_s() - t1;
+    }
+    if (r2)
+        qld_cuda_host_free(ctx, r2);
+    return bad;
+}
+
 int main(int argc, char **argv)
 {
     task base;
     memset(&base, 0, sizeof base);
     int ploidy = 0, threads = 1, device = 0, mode = QLD_R2_REFERENCE, timing = 0, mdf = 0;
+    int gpu_filter = 1;
     int have_in = 0, have_out = 0;
     float r2limit = 0.2f;   /* qLD-compute's default */
     const char *list = NULL;
@@ -311,6 +397,13 @@ int main(int argc, char **argv)
             else if (!strcmp(v, "phased_diploid") || !strcmp(v, "unphased_diploid")) ploidy = 2;
             else {
                 fprintf(stderr, "Please insert supported ploidy (see --help for more info)\n");
+                return 1;
+            }
+        } else if (!strcmp(a, "-filter")) {
+            if (!strcmp(v, "gpu")) gpu_filter = 1;
+            else if (!strcmp(v, "host")) gpu_filter = 0;
+            else {
+                fprintf(stderr, "ERROR: -filter is gpu or host\n");
                 return 1;
             }
         } else if (!strcmp(a, "-r2mode")) {
@@ -376,44 +469,21 @@ int main(int argc, char **argv)
         load_arg na = {ctx, t + 1 < ntasks ? &tasks[t + 1] : NULL, ploidy, threads, &next};
         if (t + 1 < ntasks && pthread_create(&pre, NULL, load_task, &na) == 0)
             prefetching = 1;
-        const double t0 = now_s();
-        double gpu_s = 0, rep_s = 0;
         if (cur.rc != QLD_OK) {
             fprintf(stderr, "ERROR: %s: %s\n", tasks[t].out, cur.err);
             status = 1;
         } else {
-            const qld_table *A = &cur.A, *B = cur.single ? &cur.A : &cur.B;
-            float *r2 = NULL;
-            const size_t cells = (size_t)A->rows * (size_t)B->rows;
-            rc = cells ? qld_cuda_host_alloc(ctx, cells * sizeof(float), (void **)&r2) : QLD_OK;
-            if (rc == QLD_OK && cells)
-                rc = qld_cuda_ld(ctx, A->words, A->bc, A->rows, B->words, B->bc, B->rows, cur.K,
-                                 cur.S, cur.single, r2, NULL);
-            gpu_s = now_s() - t0;
-            FILE *fp = NULL;
-            if (rc != QLD_OK) {
-                fprintf(stderr, "ERROR: %s: %s\n", tasks[t].out, qld_cuda_last_error(ctx));
+            double ld_s = 0, rep_s = 0;
+            const qld_table *B = cur.single ? &cur.A : &cur.B;
+            if ((gpu_filter ? run_filtered : run_dense)(ctx, &cur, tasks[t].out, r2limit, threads,
+                                                       &ld_s, &rep_s))
                 status = 1;
-            } else if (!(fp = fopen(tasks[t].out, "wb"))) {
-                fprintf(stderr, "ERROR: cannot write %s\n", tasks[t].out);
-                status = 1;
-            } else {
-                const double t1 = now_s();
-                if (qld_report_write(fp, A, B, r2, cur.S, r2limit, cur.tri, threads) != QLD_OK) {
-                    fprintf(stderr, "ERROR: %s: %s\n", tasks[t].out, qld_host_last_error());
-                    status = 1;
-                }
-                if (fclose(fp) != 0)
-                    status = 1;
-                rep_s = now_s() - t1;
-            }
-            if (r2)
-                qld_cuda_host_free(ctx, r2);
             if (timing)
                 fprintf(stderr,
                         "{\"task\": \"%s\", \"rows_a\": %d, \"rows_b\": %d, \"load_s\": %.6f, "
-                        "\"ld_s\": %.6f, \"report_s\": %.6f}\n",
-                        tasks[t].out, A->rows, B->rows, cur.load_s, gpu_s, rep_s);
+                        "\"ld_s\": %.6f, \"report_s\": %.6f, \"filter\": \"%s\"}\n",
+                        tasks[t].out, cur.A.rows, B->rows, cur.load_s, ld_s, rep_s,
+                        gpu_filter ? "gpu" : "host");
         }
         qld_table_free(ctx, &cur.A);
         qld_table_free(ctx, &cur.B);

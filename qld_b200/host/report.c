@@ -8,7 +8,9 @@
  * POS2 \t POS1 \t ID2 \t ID1 \t freq[2] \t freq[1] \t LD.
  * The per-row pieces (positions, IDs, the two frequencies) are formatted once
  * per row; worker threads format blocks of B rows into private buffers and
- * the blocks are written in order.
+ * the blocks are written in order.  Rows come from a dense r^2 array
+ * (qld_report_write) or from qld_cuda_ld_hits blocks, whose mask bits and
+ * packed values are already filtered on the GPU (qld_report_hits).
  */
 #define _GNU_SOURCE
 #include <pthread.h>
@@ -114,17 +116,6 @@ typedef struct block {
     size_t len, cap;
 } block;
 
-typedef struct rep_job {
-    const float *r2;
-    int m, n, row0, single;   /* row0: B row of local row 0 */
-    float r2limit;
-    const rowtxt *ta, *tb;
-    block *blocks;
-    int nblocks, rows_per_block;
-    atomic_int next;
-    atomic_int failed;
-} rep_job;
-
 static int ensure(block *b, size_t extra)
 {
     if (b->len + extra <= b->cap)
@@ -140,6 +131,66 @@ static int ensure(block *b, size_t extra)
     return 0;
 }
 
+/* One report line: POS2 POS1 ID2 ID1 freq[2] freq[1] LD. */
+static int emit(block *b, const rowtxt *bt, const rowtxt *at, float v)
+{
+    if (ensure(b, (size_t)bt->pos_n + at->pos_n + bt->id_n + at->id_n + bt->freq_n +
+                      at->freq_n + 64))
+        return -1;
+    char *o = b->buf + b->len;
+    memcpy(o, bt->pos, bt->pos_n); o += bt->pos_n; *o++ = '\t';
+    memcpy(o, at->pos, at->pos_n); o += at->pos_n; *o++ = '\t';
+    memcpy(o, bt->id, bt->id_n); o += bt->id_n; *o++ = '\t';
+    memcpy(o, at->id, at->id_n); o += at->id_n; *o++ = '\t';
+    memcpy(o, bt->freq, bt->freq_n); o += bt->freq_n; *o++ = '\t';
+    memcpy(o, at->freq, at->freq_n); o += at->freq_n; *o++ = '\t';
+    o += fmt_f(o, v, 9);
+    *o++ = '\n';
+    b->len = (size_t)(o - b->buf);
+    return 0;
+}
+
+/* Rows [row0, row0 + n) of B, from a dense r^2 block (r2 row i at
+ * r2 + i*m, kept if r2limit <= v < 100 and, with `single`, j > row0 + i) or
+ * from a qld_cuda_ld_hits block (mask bits and packed values). */
+typedef struct rep_job {
+    const float *r2;
+    float r2limit;
+    int single;
+    const qld_hits_block *hits;
+    int m, n, row0;
+    const rowtxt *ta, *tb;     /* tb indexed by B row */
+    block *blocks;
+    int nblocks, rows_per_block;
+    atomic_int next;
+    atomic_int failed;
+} rep_job;
+
+static int format_row(const rep_job *j, int i, block *b)
+{
+    const int gi = j->row0 + i;
+    const rowtxt *bt = &j->tb[gi];
+    if (j->hits) {
+        const qld_hits_block *h = j->hits;
+        const uint32_t *mw = h->mask + (size_t)i * h->words;
+        const float *v = h->val + h->row_off[i];
+        for (int w = 0; w < h->words; ++w)
+            for (uint32_t bits = mw[w]; bits; bits &= bits - 1) {
+                const int c = w * 32 + __builtin_ctz(bits);
+                if (emit(b, bt, &j->ta[c], *v++))
+                    return -1;
+            }
+        return 0;
+    }
+    const float *row = j->r2 + (size_t)i * j->m;
+    for (int c = j->single ? gi + 1 : 0; c < j->m; ++c) {
+        const float v = row[c];
+        if (v >= j->r2limit && v < 100 && emit(b, bt, &j->ta[c], v))
+            return -1;
+    }
+    return 0;
+}
+
 static void *rep_worker(void *arg)
 {
     rep_job *j = arg;
@@ -150,33 +201,122 @@ static void *rep_worker(void *arg)
         block *b = &j->blocks[bi];
         const int i0 = bi * j->rows_per_block;
         const int i1 = i0 + j->rows_per_block < j->n ? i0 + j->rows_per_block : j->n;
-        for (int i = i0; i < i1; ++i) {
-            const rowtxt *bt = &j->tb[i];
-            const float *row = j->r2 + (size_t)i * j->m;
-            for (int c = j->single ? j->row0 + i + 1 : 0; c < j->m; ++c) {
-                const float v = row[c];
-                if (!(v >= j->r2limit && v < 100))
-                    continue;
-                const rowtxt *at = &j->ta[c];
-                if (ensure(b, (size_t)bt->pos_n + at->pos_n + bt->id_n + at->id_n + bt->freq_n +
-                                  at->freq_n + 64)) {
-                    atomic_store(&j->failed, 1);
-                    return NULL;
-                }
-                char *o = b->buf + b->len;
-                memcpy(o, bt->pos, bt->pos_n); o += bt->pos_n; *o++ = '\t';
-                memcpy(o, at->pos, at->pos_n); o += at->pos_n; *o++ = '\t';
-                memcpy(o, bt->id, bt->id_n); o += bt->id_n; *o++ = '\t';
-                memcpy(o, at->id, at->id_n); o += at->id_n; *o++ = '\t';
-                memcpy(o, bt->freq, bt->freq_n); o += bt->freq_n; *o++ = '\t';
-                memcpy(o, at->freq, at->freq_n); o += at->freq_n; *o++ = '\t';
-                o += fmt_f(o, v, 9);
-                *o++ = '\n';
-                b->len = (size_t)(o - b->buf);
+        for (int i = i0; i < i1; ++i)
+            if (format_row(j, i, b)) {
+                atomic_store(&j->failed, 1);
+                return NULL;
             }
-        }
     }
     return NULL;
+}
+
+struct qld_report {
+    FILE *fp;
+    const qld_table *A, *B;
+    rowtxt *ta, *tb;
+    char *pa, *pb;
+    int snip_size, threads, per_round, rows_per_block;
+    block *blocks;
+};
+
+int qld_report_open(qld_report **out, FILE *fp, const qld_table *A, const qld_table *B,
+                    int snip_size, int threads)
+{
+    if (!out)
+        return qld_host_fail(QLD_ERR_INVALID, "NULL report handle");
+    *out = NULL;
+    if (!fp || !A || !B || snip_size < 1)
+        return qld_host_fail(QLD_ERR_INVALID, "bad report arguments");
+    qld_report *r = calloc(1, sizeof *r);
+    if (!r)
+        return qld_host_fail(QLD_ERR_NOMEM, "out of memory");
+    r->fp = fp;
+    r->A = A;
+    r->B = B;
+    r->snip_size = snip_size;
+    r->threads = threads < 1 ? 1 : threads;
+    r->rows_per_block = 64;
+    r->per_round = r->threads * 4;   /* row blocks formatted before each write-out */
+    r->blocks = calloc((size_t)r->per_round, sizeof *r->blocks);
+    if (!r->blocks || row_texts(A, snip_size, &r->ta, &r->pa) ||
+        (B == A ? (r->tb = r->ta, 0) : row_texts(B, snip_size, &r->tb, &r->pb))) {
+        qld_report_close(r);
+        return qld_host_fail(QLD_ERR_NOMEM, "out of memory");
+    }
+    if (fputs("POS2\tPOS1\tID2\tID1\tfreq[2]\tfreq[1]\tLD\n", fp) == EOF) {
+        qld_report_close(r);
+        return qld_host_fail(QLD_ERR_INVALID, "write failed");
+    }
+    *out = r;
+    return QLD_OK;
+}
+
+/* Format rows [row0, row0 + n) with the report's threads and write them in
+ * order, per_round row blocks at a time. */
+static int run_rows(qld_report *r, rep_job *proto, int row0, int n)
+{
+    const int span = r->rows_per_block * r->per_round;
+    for (int i0 = 0; i0 < n; i0 += span) {
+        const int rows = n - i0 < span ? n - i0 : span;
+        rep_job j = *proto;
+        j.row0 = row0 + i0;
+        j.n = rows;
+        if (j.r2)
+            j.r2 = proto->r2 + (size_t)i0 * j.m;
+        qld_hits_block sub;
+        if (proto->hits) {   /* the same block seen from local row i0 */
+            sub = *proto->hits;
+            sub.mask += (size_t)i0 * sub.words;
+            sub.row_off += i0;
+            j.hits = &sub;
+        }
+        j.ta = r->ta;
+        j.tb = r->tb;
+        j.blocks = r->blocks;
+        j.rows_per_block = r->rows_per_block;
+        j.nblocks = (rows + r->rows_per_block - 1) / r->rows_per_block;
+        atomic_init(&j.next, 0);
+        atomic_init(&j.failed, 0);
+        for (int k = 0; k < j.nblocks; ++k)
+            r->blocks[k].len = 0;
+        qld_run_threads(rep_worker, &j, r->threads < j.nblocks ? r->threads : j.nblocks);
+        if (atomic_load(&j.failed))
+            return qld_host_fail(QLD_ERR_NOMEM, "out of memory");
+        for (int k = 0; k < j.nblocks; ++k)
+            if (r->blocks[k].len &&
+                fwrite(r->blocks[k].buf, 1, r->blocks[k].len, r->fp) != r->blocks[k].len)
+                return qld_host_fail(QLD_ERR_INVALID, "write failed");
+    }
+    return QLD_OK;
+}
+
+int qld_report_hits(qld_report *r, const qld_hits_block *blk)
+{
+    if (!r || !blk || blk->rows < 0 || blk->row0 < 0 || blk->row0 + blk->rows > r->B->rows ||
+        blk->m != r->A->rows || (blk->rows && (!blk->mask || !blk->row_off)))
+        return qld_host_fail(QLD_ERR_INVALID, "block does not match the report's tables");
+    rep_job proto;
+    memset(&proto, 0, sizeof proto);
+    proto.hits = blk;
+    proto.m = blk->m;
+    return run_rows(r, &proto, blk->row0, blk->rows);
+}
+
+int qld_report_close(qld_report *r)
+{
+    if (!r)
+        return QLD_OK;
+    for (int k = 0; r->blocks && k < r->per_round; ++k)
+        free(r->blocks[k].buf);
+    free(r->blocks);
+    if (r->tb != r->ta) {
+        free(r->tb);
+        free(r->pb);
+    }
+    free(r->ta);
+    free(r->pa);
+    free(r);
+    return QLD_OK;
 }
 
 int qld_report_write(FILE *fp, const qld_table *A, const qld_table *B, const float *r2,
@@ -184,62 +324,19 @@ int qld_report_write(FILE *fp, const qld_table *A, const qld_table *B, const flo
 {
     if (!fp || !A || !B || (!r2 && A->rows && B->rows) || snip_size < 1)
         return qld_host_fail(QLD_ERR_INVALID, "bad report arguments");
-    if (fputs("POS2\tPOS1\tID2\tID1\tfreq[2]\tfreq[1]\tLD\n", fp) == EOF)
-        return qld_host_fail(QLD_ERR_INVALID, "write failed");
-    if (!A->rows || !B->rows)
-        return QLD_OK;
-    rowtxt *ta = NULL, *tb = NULL;
-    char *pa = NULL, *pb = NULL;
-    if (row_texts(A, snip_size, &ta, &pa) ||
-        (B == A ? (tb = ta, pb = NULL, 0) : row_texts(B, snip_size, &tb, &pb))) {
-        free(ta);
-        free(pa);
-        return qld_host_fail(QLD_ERR_NOMEM, "out of memory");
+    qld_report *r;
+    int rc = qld_report_open(&r, fp, A, B, snip_size, threads);
+    if (rc != QLD_OK)
+        return rc;
+    if (A->rows && B->rows) {
+        rep_job proto;
+        memset(&proto, 0, sizeof proto);
+        proto.r2 = r2;
+        proto.r2limit = r2limit;
+        proto.single = single_region;
+        proto.m = A->rows;
+        rc = run_rows(r, &proto, 0, B->rows);
     }
-    if (threads < 1)
-        threads = 1;
-    const int rows_per_block = 64;
-    const int per_round = threads * 4;   /* blocks formatted before each write-out */
-    block *blocks = calloc((size_t)per_round, sizeof *blocks);
-    int rc = blocks ? QLD_OK : qld_host_fail(QLD_ERR_NOMEM, "out of memory");
-    for (int i0 = 0; rc == QLD_OK && i0 < B->rows; i0 += rows_per_block * per_round) {
-        const int rows = B->rows - i0 < rows_per_block * per_round ? B->rows - i0
-                                                                   : rows_per_block * per_round;
-        rep_job j;
-        j.r2 = r2 + (size_t)i0 * A->rows;
-        j.m = A->rows;
-        j.n = rows;
-        j.row0 = i0;
-        j.single = single_region;
-        j.r2limit = r2limit;
-        j.ta = ta;
-        j.tb = tb + i0;
-        j.blocks = blocks;
-        j.rows_per_block = rows_per_block;
-        j.nblocks = (rows + rows_per_block - 1) / rows_per_block;
-        atomic_init(&j.next, 0);
-        atomic_init(&j.failed, 0);
-        for (int k = 0; k < j.nblocks; ++k)
-            blocks[k].len = 0;
-        qld_run_threads(rep_worker, &j, threads < j.nblocks ? threads : j.nblocks);
-        if (atomic_load(&j.failed)) {
-            rc = qld_host_fail(QLD_ERR_NOMEM, "out of memory");
-            break;
-        }
-        for (int k = 0; k < j.nblocks; ++k)
-            if (blocks[k].len && fwrite(blocks[k].buf, 1, blocks[k].len, fp) != blocks[k].len) {
-                rc = qld_host_fail(QLD_ERR_INVALID, "write failed");
-                break;
-            }
-    }
-    for (int k = 0; blocks && k < per_round; ++k)
-        free(blocks[k].buf);
-    free(blocks);
-    if (tb != ta) {
-        free(tb);
-        free(pb);
-    }
-    free(ta);
-    free(pa);
+    qld_report_close(r);
     return rc;
 }

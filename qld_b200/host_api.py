@@ -5,6 +5,7 @@ qLD's text report from Python.
     tab = host_api.load_mdf(path, pos_min, pos_max, K, threads=8, ctx=None)
     host_api.write_report(out_path, tab_a, tab_b, r2, snip_size, r2limit,
                           single_region, threads=8)
+    host_api.write_report_hits(out_path, tab_a, tab_b, blocks, snip_size)
 
 ``load_mdf`` returns a ``Table`` (numpy copies of words, BC, POS and IDs) and
 releases the C-side buffers; with a ``api.Context`` the C side assembles in
@@ -81,6 +82,13 @@ def lib() -> ct.CDLL:
         L.qld_report_write.argtypes = [ct.c_void_p, ct.POINTER(_Table), ct.POINTER(_Table),
                                        ct.c_void_p, ct.c_int, ct.c_float, ct.c_int, ct.c_int]
         L.qld_report_write.restype = ct.c_int
+        L.qld_report_open.argtypes = [ct.POINTER(ct.c_void_p), ct.c_void_p, ct.POINTER(_Table),
+                                      ct.POINTER(_Table), ct.c_int, ct.c_int]
+        L.qld_report_open.restype = ct.c_int
+        L.qld_report_hits.argtypes = [ct.c_void_p, ct.POINTER(api.HitsBlock)]
+        L.qld_report_hits.restype = ct.c_int
+        L.qld_report_close.argtypes = [ct.c_void_p]
+        L.qld_report_close.restype = ct.c_int
         L.qld_host_last_error.argtypes = []
         L.qld_host_last_error.restype = ct.c_char_p
         _lib = L
@@ -135,17 +143,72 @@ def _as_c_table(tab: Table, keep: list) -> _Table:
     return t
 
 
+def _libc():
+    libc = ct.CDLL(None)
+    libc.fopen.argtypes = [ct.c_char_p, ct.c_char_p]
+    libc.fopen.restype = ct.c_void_p
+    libc.fclose.argtypes = [ct.c_void_p]
+    libc.fclose.restype = ct.c_int
+    return libc
+
+
+def hits_from_dense(r2: np.ndarray, r2limit: float, triangle: bool, row0: int = 0):
+    """(mask, row_off, val) of a dense (rows, m) r^2 block under qLD's report
+    rule -- the host-side statement of what qld_cuda_ld_hits delivers."""
+    r2 = np.asarray(r2, np.float32)
+    rows, m = r2.shape
+    keep = (r2 >= np.float32(r2limit)) & (r2 < 100)
+    if triangle:
+        keep &= np.arange(m)[None, :] > (row0 + np.arange(rows))[:, None]
+    W = (m + 31) // 32
+    bits = np.zeros((rows, W * 32), bool)
+    bits[:, :m] = keep
+    mask = (bits.reshape(rows, W, 32).astype(np.uint64) << np.arange(32, dtype=np.uint64)).sum(
+        axis=2).astype(np.uint32)
+    row_off = np.zeros(rows + 1, np.int64)
+    row_off[1:] = np.cumsum(keep.sum(axis=1))
+    return mask, row_off, r2[keep].astype(np.float32)
+
+
+def write_report_hits(path: str, A: Table, B: Table, blocks, snip_size: int,
+                      threads: int = 1) -> None:
+    """qLD's report from filtered blocks: `blocks` yields (row0, mask, row_off,
+    val) in B-row order (qld_report_open / qld_report_hits / qld_report_close)."""
+    libc = _libc()
+    keep: list = []
+    ta = _as_c_table(A, keep)
+    tb = ta if B is A else _as_c_table(B, keep)
+    fp = libc.fopen(os.fsencode(path), b"wb")
+    if not fp:
+        raise OSError(f"cannot open {path}")
+    rep = ct.c_void_p()
+    try:
+        _check(lib().qld_report_open(ct.byref(rep), fp, ct.byref(ta), ct.byref(tb),
+                                     int(snip_size), int(threads)))
+        try:
+            for row0, mask, row_off, val in blocks:
+                mask = np.ascontiguousarray(mask, np.uint32)
+                row_off = np.ascontiguousarray(row_off, np.int64)
+                val = np.ascontiguousarray(val, np.float32)
+                b = api.HitsBlock(int(row0), mask.shape[0], len(A.pos), mask.shape[1],
+                                  mask.ctypes.data_as(ct.POINTER(ct.c_uint32)),
+                                  row_off.ctypes.data_as(ct.POINTER(ct.c_longlong)),
+                                  val.ctypes.data_as(ct.POINTER(ct.c_float)))
+                _check(lib().qld_report_hits(rep, ct.byref(b)))
+        finally:
+            lib().qld_report_close(rep)
+    finally:
+        if libc.fclose(fp) != 0:
+            raise OSError(f"cannot close {path}")
+
+
 def write_report(path: str, A: Table, B: Table, r2: np.ndarray, snip_size: int,
                  r2limit: float, single_region: bool, threads: int = 1) -> None:
     """qLD's report of one task; r2 is (B rows, A rows) float32."""
     r2 = np.ascontiguousarray(r2, np.float32)
     if r2.shape != (len(B.pos), len(A.pos)):
         raise ValueError(f"r2 is {r2.shape}, expected {(len(B.pos), len(A.pos))}")
-    libc = ct.CDLL(None)
-    libc.fopen.argtypes = [ct.c_char_p, ct.c_char_p]
-    libc.fopen.restype = ct.c_void_p
-    libc.fclose.argtypes = [ct.c_void_p]
-    libc.fclose.restype = ct.c_int
+    libc = _libc()
     keep: list = []
     ta = _as_c_table(A, keep)
     tb = ta if B is A else _as_c_table(B, keep)

@@ -133,6 +133,22 @@ def test_input_list_identical(list_reports):
     assert ref == qld
 
 
+def test_host_filter_matches(dataset):
+    """-filter host (dense r^2 back, filtered by report.c) writes the same bytes."""
+    tmp, d1, d2, _, _ = dataset
+    for name, args in (("hf1", ["-input", d1, "-r2limit", "0.01"]),
+                       ("hf2", ["-input", d1, "-input2", d2, "-posWmin1", "1000",
+                                "-posWmax1", "9990", "-posWmin2", "100000",
+                                "-posWmax2", "104193", "-r2limit", "0.005"])):
+        outs = []
+        for flt in ("gpu", "host"):
+            d = os.path.join(tmp, f"{name}_{flt}")
+            _run([*args, "-ploidy", "haploid", "-mdf", "-filter", flt, "-threads", "3",
+                  "-output", os.path.join(d, "out.txt")], d, host_api.CLI_PATH)
+            outs.append(open(os.path.join(d, "out.txt"), "rb").read())
+        assert outs[0] == outs[1] and outs[0].count(b"\n") > 100
+
+
 def test_exact_mode_against_oracle(dataset, tmp_path):
     tmp, d1, _, _, T = dataset
     out = tmp_path / "exact.txt"

@@ -141,6 +141,42 @@ def test_report_rectangle_with_triangle_rule(tmp_path):
     assert out.read_bytes() == want
 
 
+@pytest.mark.parametrize("single,block_rows", [(True, 64), (True, 1000), (False, 77)])
+def test_report_from_hit_blocks_matches_dense(tmp_path, single, block_rows):
+    """The streamed writer fed with filtered blocks (mask + packed values, the
+    form qld_cuda_ld_hits delivers) writes the dense writer's bytes."""
+    rng = np.random.default_rng(4)
+    m, n = 700, (700 if single else 450)
+    r2 = (rng.random((n, m), dtype=np.float32) ** 4).astype(np.float32)
+    r2.flat[rng.integers(0, r2.size, 500)] = np.float32(np.nan)
+    r2.flat[rng.integers(0, r2.size, 500)] = np.float32(123.456)
+    S = 999
+    A = host_api.Table(np.zeros((m, 1), np.uint64), rng.integers(0, S, m).astype(np.uint32),
+                       np.arange(m, dtype=np.uint32) * 3 + 1, [f"a{i}" for i in range(m)])
+    B = A if single else host_api.Table(
+        np.zeros((n, 1), np.uint64), rng.integers(0, S, n).astype(np.uint32),
+        np.arange(n, dtype=np.uint32) * 5 + 2, [f"b{i}" for i in range(n)])
+    dense = tmp_path / "dense.txt"
+    host_api.write_report(str(dense), A, B, r2, S, 0.03, single, threads=2)
+
+    def blocks():
+        for r0 in range(0, n, block_rows):
+            mask, off, val = host_api.hits_from_dense(r2[r0:r0 + block_rows], 0.03, single, r0)
+            yield r0, mask, off, val
+
+    hits = tmp_path / "hits.txt"
+    host_api.write_report_hits(str(hits), A, B, blocks(), S, threads=3)
+    assert hits.read_bytes() == dense.read_bytes()
+
+
+def test_report_hits_rejects_foreign_block(tmp_path):
+    A = host_api.Table(np.zeros((40, 1), np.uint64), np.ones(40, np.uint32),
+                       np.arange(40, dtype=np.uint32), [f"a{i}" for i in range(40)])
+    mask, off, val = host_api.hits_from_dense(np.ones((10, 40), np.float32) * 0.5, 0.1, False)
+    with pytest.raises(api.QldError):          # rows 35..44 of a 40-row table B
+        host_api.write_report_hits(str(tmp_path / "x.txt"), A, A, [(35, mask, off, val)], 10)
+
+
 def _cli(*args, timeout=60):
     return subprocess.run([host_api.CLI_PATH, *args], capture_output=True, text=True,
                           timeout=timeout)
