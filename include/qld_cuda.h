@@ -145,6 +145,23 @@ int qld_cuda_ld_hits(qld_ctx *ctx, const uint64_t *A, const uint32_t *bcA, int m
                      int triangle, float r2limit, qld_hits_fn fn, void *user);
 
 /*
+ * COUNTSTATES: qLD-compute's -DCOUNTSTATES build replaces the r^2 task by
+ * countStates_mode() (src/correlator/src/correlate_IO.c:472-516).  For every
+ * pair a state value: st = 0, then per 64-bit word st = popcount(st | S),
+ * S = the joint states (A bit, B bit) present among the word's 64 bit pairs
+ * (bit 2*a + b); the zero tail bits of the last word count as state (0,0).
+ * states_out[i*m + j] (B-major, one byte) for B row i and A row j; with
+ * `symmetric` (B is A) only entries j >= i are defined.  Host-buffer and
+ * device forms as qld_cuda_ld / qld_cuda_ld_device (lds >= m bytes between
+ * B rows).
+ */
+int qld_cuda_count_states(qld_ctx *ctx, const uint64_t *A, int m, const uint64_t *B, int n,
+                          int K, int symmetric, uint8_t *states_out);
+int qld_cuda_count_states_device(qld_ctx *ctx, const uint64_t *A, int m, long long lda,
+                                 const uint64_t *B, int n, long long ldb, int K, int symmetric,
+                                 uint8_t *states, long long lds, void *stream);
+
+/*
  * Windowed (band) LD over one region: r^2 only for SNP pairs (i, j) with
  * 1 <= j - i <= band.  Output is the m x band array r2_band[i*band + d] =
  * r^2(SNP i, SNP i+1+d) (entries with i+1+d >= m are unspecified); counts_band

@@ -73,6 +73,15 @@ int qld_report_write(FILE *fp, const qld_table *A, const qld_table *B, const flo
                      int snip_size, float r2limit, int single_region, int threads);
 
 /*
+ * COUNTSTATES report: writeStateCount() (correlate_IO.c:430-470) -- header
+ * "POS2\tPOS1\tID2\tID1\tNo_STATES", then for B row i (outer) and A row j
+ * (j > i for a single region) "POS2\tPOS1\tID2\tID1\t<states>\t" per line,
+ * states[i*m + j] as qld_cuda_count_states() writes them.
+ */
+int qld_report_states(FILE *fp, const qld_table *A, const qld_table *B, const uint8_t *states,
+                      int single_region, int threads);
+
+/*
  * The same report, streamed from qld_cuda_ld_hits blocks: open writes the
  * header line and formats the tables' per-row text once; each call of
  * qld_report_hits appends the rows of one block (blocks in B-row order, as

@@ -66,6 +66,12 @@ def _lib(name: str) -> ct.CDLL:
                 _u32p, ct.POINTER(ct.c_char_p), _u32p, ct.c_int, ct.c_int,
                 _f32p, ct.c_float, ct.c_int]
             lib.qo_write_results.restype = ct.c_size_t
+            lib.qo_count_states.argtypes = [_u64p, ct.c_int, _u64p, ct.c_int, ct.c_int,
+                                            ct.c_void_p]
+            lib.qo_write_states.argtypes = [
+                ct.c_char_p, ct.c_size_t, _u32p, ct.POINTER(ct.c_char_p), ct.c_int,
+                _u32p, ct.POINTER(ct.c_char_p), ct.c_int, ct.c_void_p, ct.c_int]
+            lib.qo_write_states.restype = ct.c_size_t
         elif name == "ref":
             path = os.path.join(_HERE, "_ref", "libqldref.so")
             if not os.path.exists(path):
@@ -164,6 +170,30 @@ def write_results(posA, idA, bcA, posB, idB, bcB, S, results, r2limit, posWset2,
     need = lib.qo_write_results(None, 0, *args)
     buf = ct.create_string_buffer(need + 1)
     lib.qo_write_results(buf, need + 1, *args)
+    return buf.raw[:need]
+
+
+def count_states(A, B=None) -> np.ndarray:
+    """countStates_mode()'s state counts, (n, m) uint8 (B-major)."""
+    A = _c(A, np.uint64)
+    B = A if B is None else _c(B, np.uint64)
+    m, K = A.shape
+    n = B.shape[0]
+    out = np.empty((n, m), np.uint8)
+    _lib("oracle").qo_count_states(A, m, B, n, K, out.ctypes.data)
+    return out
+
+
+def write_states(posA, idA, posB, idB, states, posWset2) -> bytes:
+    """writeStateCount()'s report bytes."""
+    posA, posB = _c(posA, np.uint32), _c(posB, np.uint32)
+    states = _c(states, np.uint8)
+    m, n = len(posA), len(posB)
+    lib = _lib("oracle")
+    args = (posA, _ids(idA), m, posB, _ids(idB), n, states.ctypes.data, int(posWset2))
+    need = lib.qo_write_states(None, 0, *args)
+    buf = ct.create_string_buffer(need + 1)
+    lib.qo_write_states(buf, need + 1, *args)
     return buf.raw[:need]
 
 

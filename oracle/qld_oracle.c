@@ -21,6 +21,9 @@
  *                         cases (zero popcount -> 0, > 1.0001 -> 123.456).
  *   qo_write_results   <- writeResultsHeader()/writeResults() correlate_IO.c:378-429
  *   qo_fprint_f        <- fprint_f()/reverse()  fast_print.c:21-103
+ *   qo_count_states    <- countStates_mode()  correlate_IO.c:472-516 (the
+ *                         COUNTSTATES build), bit loop and all
+ *   qo_write_states    <- writeStateCount()   correlate_IO.c:430-470
  *
  * Build with -ffp-contract=off: every fused multiply-add below is written as
  * an explicit fmaf() so the rounding never depends on compiler flags.
@@ -260,6 +263,68 @@ QO_EXPORT size_t qo_write_results(char *buf, size_t cap, int with_header,
                 fmt_f(&s, v, 9);
                 sink_putc(&s, '\n');
             }
+        }
+    }
+    return s.len;
+}
+
+/* ----------------------------------------------------------- COUNTSTATES -- */
+
+/*
+ * countStates_mode (correlate_IO.c:472-516), pair (A row a, B row b): st
+ * starts at 0; for every word k, bit p = 0..63 ORs 1 << (bitA*2 + bitB) into
+ * st (stopping early once st == 15), and st is then replaced by its own
+ * popcount -- so the next word starts from that count read as a bit set.
+ * Written as the reference's loop; out[b*m + a] (B-major like r^2).
+ */
+QO_EXPORT void qo_count_states(const uint64_t *A, int m, const uint64_t *B, int n, int K,
+                               uint8_t *out)
+{
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int b = 0; b < n; b++) {
+        for (int a = 0; a < m; a++) {
+            uint8_t st = 0;
+            for (int k = 0; k < K; k++) {
+                const uint64_t wa = A[(size_t)a * K + k], wb = B[(size_t)b * K + k];
+                for (int p = 0; p < 64; p++) {
+                    if (st == 15)
+                        break;
+                    st |= (uint8_t)(1u << (((wa >> p) & 1u) * 2 + ((wb >> p) & 1u)));
+                }
+                st = (uint8_t)__builtin_popcount(st);
+            }
+            out[(size_t)b * m + a] = st;
+        }
+    }
+}
+
+/*
+ * writeStateCount (correlate_IO.c:430-470): header, then for B row i and A
+ * row j (j > i when posWset2 == 0) "POS2\tPOS1\tID2\tID1\t<states>\t\n".
+ * Returns the byte count; writes at most cap bytes.
+ */
+QO_EXPORT size_t qo_write_states(char *buf, size_t cap, const uint32_t *posA, char **idA, int m,
+                                 const uint32_t *posB, char **idB, int n, const uint8_t *st,
+                                 int posWset2)
+{
+    qo_sink s = {buf, 0, cap};
+    sink_puts(&s, "POS2\tPOS1\tID2\tID1\tNo_STATES\n");
+    char num[16];
+    for (int i = 0; i < n; i++) {
+        for (int j = posWset2 == 0 ? i + 1 : 0; j < m; j++) {
+            snprintf(num, sizeof num, "%u", posB[i]);
+            sink_puts(&s, num);
+            sink_putc(&s, '\t');
+            snprintf(num, sizeof num, "%u", posA[j]);
+            sink_puts(&s, num);
+            sink_putc(&s, '\t');
+            sink_puts(&s, idB[i]);
+            sink_putc(&s, '\t');
+            sink_puts(&s, idA[j]);
+            sink_putc(&s, '\t');
+            snprintf(num, sizeof num, "%u", (unsigned)st[(size_t)i * m + j]);
+            sink_puts(&s, num);
+            sink_puts(&s, "\t\n");
         }
     }
     return s.len;

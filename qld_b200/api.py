@@ -32,6 +32,7 @@ OPT_KERNEL, OPT_R2_MODE, OPT_PROFILE, OPT_BAND_ROWS, OPT_MMA_TILE = 1, 2, 3, 4, 
 EXPORTED = (
     "qld_cuda_init", "qld_cuda_release", "qld_cuda_last_error", "qld_cuda_set_option",
     "qld_cuda_ld", "qld_cuda_ld_device", "qld_cuda_ld_hits", "qld_cuda_ld_batch",
+    "qld_cuda_count_states", "qld_cuda_count_states_device",
     "qld_cuda_ld_band",
     "qld_cuda_ld_band_device", "qld_cuda_sync",
     "qld_cuda_host_alloc",
@@ -114,6 +115,8 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.qld_cuda_ld.argtypes = [vp, vp, vp, i, vp, vp, i, i, i, i, vp, vp]
     lib.qld_cuda_ld_device.argtypes = [vp, ct.POINTER(_LdArgs), vp]
     lib.qld_cuda_ld_batch.argtypes = [vp, ct.POINTER(_LdArgs), i, vp]
+    lib.qld_cuda_count_states.argtypes = [vp, vp, i, vp, i, i, i, vp]
+    lib.qld_cuda_count_states_device.argtypes = [vp, vp, i, ll, vp, i, ll, i, i, vp, ll, vp]
     lib.qld_cuda_ld_hits.argtypes = [vp, vp, vp, i, vp, vp, i, i, i, i, i, ct.c_float, HITS_FN, vp]
     lib.qld_cuda_ld_band.argtypes = [vp, vp, vp, i, i, i, i, vp, vp]
     lib.qld_cuda_ld_band_device.argtypes = [vp, vp, vp, i, ll, i, i, i, vp, ll, vp, ll, vp]
@@ -295,6 +298,30 @@ class Context:
         row_off = np.concatenate(offs)
         val = np.concatenate(vals) if vals else np.zeros(0, np.float32)
         return mask, row_off, val
+
+    def count_states(self, A, B=None, *, symmetric: bool | None = None, out=None):
+        """COUNTSTATES: (n, m) uint8 state values (qld_cuda_count_states)."""
+        if symmetric is None:
+            symmetric = B is None
+        A = np.ascontiguousarray(A).view(np.uint64)
+        m, K = A.shape
+        if symmetric:
+            B, n = A, m
+        else:
+            B = np.ascontiguousarray(B).view(np.uint64)
+            n = B.shape[0]
+            if B.shape[1] != K:
+                raise ValueError("A and B must have the same number of words per row")
+        if out is None:
+            out = np.empty((n, m), np.uint8)
+        self._check(self.lib.qld_cuda_count_states(self.h, _ptr(A), m, _ptr(B), n, K,
+                                                   int(bool(symmetric)), _ptr(out)))
+        return out
+
+    def count_states_device(self, A, m, lda, B, n, ldb, K, symmetric, out, lds, stream=None):
+        self._check(self.lib.qld_cuda_count_states_device(
+            self.h, _p(A), int(m), int(lda), _p(B), int(n), int(ldb), int(K),
+            int(bool(symmetric)), _p(out), int(lds), _stream(stream)))
 
     # ------------------------------------------------------------ device --
     def ld_device(self, A, bcA, m, lda, B, bcB, n, ldb, K, S, symmetric, r2, ldr,

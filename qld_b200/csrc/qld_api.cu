@@ -269,8 +269,41 @@ int finish(qld_ctx *c, cudaStream_t st) {
 
 bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// COUNTSTATES over B rows [b0, b1) (b0 a multiple of 128), one byte per pair
+// at out[(b - out_row0) * lds + a].
+int launch_states_range(qld_ctx *c, const Task &t, int b0, int b1, uint8_t *out, long long lds,
+                        int out_row0, cudaStream_t st) {
+    const KernelShape &ks = kStatesShape;
+    CUtensorMap tmA, tmB;
+    int rc;
+    if ((rc = make_tmap(c, &tmA, t.A, t.m, t.K, t.lda, ks.box_words, ks.box_rows_a, ks.swizzle)) ||
+        (rc = make_tmap(c, &tmB, t.B, t.n, t.K, t.ldb, ks.box_words, ks.box_rows_b, ks.swizzle)))
+        return rc;
+    const int tb0 = b0 / ks.bn;
+    const int tiles_b = (b1 - b0 + ks.bn - 1) / ks.bn;
+    StatesParams p{};
+    p.m = t.m; p.n = t.n; p.K = t.K; p.symmetric = t.symmetric;
+    p.out = out; p.lds = lds; p.out_row0 = out_row0;
+    p.status = c->d_status;
+    p.timeout_cycles = c->timeout_cycles;
+    for (int done = 0; done < tiles_b; done += 65535) {
+        const int nb = tiles_b - done < 65535 ? tiles_b - done : 65535;
+        p.tb0 = tb0 + done;
+        cudaEvent_t e1 = nullptr;
+        if ((rc = prof_begin(c, st, &e1))) return rc;
+        cudaError_t e = launch_states(tmA, tmB, p, nb, st);
+        if (e != cudaSuccess)
+            return set_err(c, QLD_ERR_CUDA, "states kernel launch failed: %s",
+                           cudaGetErrorString(e));
+        if (e1) CUDA_TRY(c, cudaEventRecord(e1, st));
+        c->stats.kernel_launches++;
+    }
+    return QLD_OK;
+}
+
 // Copy host tables into the context's device buffers (rows padded to an even
 // word count, 16-byte aligned for TMA) on c->stream; *t describes them.
+// NULL bit counts are not copied (COUNTSTATES does not use them).
 int stage_tables(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const uint64_t *B,
                  const uint32_t *bcB, int n, int K, int S, int symmetric, Task *t) {
     const long long Kp = K + (K & 1);
@@ -279,7 +312,9 @@ int stage_tables(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, cons
         return rc;
     CUDA_TRY(c, cudaMemcpy2DAsync(c->dA.p, Kp * 8, A, (size_t)K * 8, (size_t)K * 8, m,
                                   cudaMemcpyHostToDevice, c->stream));
-    CUDA_TRY(c, cudaMemcpyAsync(c->dbcA.p, bcA, (size_t)m * 4, cudaMemcpyHostToDevice, c->stream));
+    if (bcA)
+        CUDA_TRY(c, cudaMemcpyAsync(c->dbcA.p, bcA, (size_t)m * 4, cudaMemcpyHostToDevice,
+                                    c->stream));
     const uint64_t *dB = static_cast<const uint64_t *>(c->dA.p);
     const uint32_t *dbcB = static_cast<const uint32_t *>(c->dbcA.p);
     if (!symmetric) {
@@ -287,8 +322,9 @@ int stage_tables(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, cons
             return rc;
         CUDA_TRY(c, cudaMemcpy2DAsync(c->dB.p, Kp * 8, B, (size_t)K * 8, (size_t)K * 8, n,
                                       cudaMemcpyHostToDevice, c->stream));
-        CUDA_TRY(c, cudaMemcpyAsync(c->dbcB.p, bcB, (size_t)n * 4, cudaMemcpyHostToDevice,
-                                    c->stream));
+        if (bcB)
+            CUDA_TRY(c, cudaMemcpyAsync(c->dbcB.p, bcB, (size_t)n * 4, cudaMemcpyHostToDevice,
+                                        c->stream));
         dB = static_cast<const uint64_t *>(c->dB.p);
         dbcB = static_cast<const uint32_t *>(c->dbcB.p);
     }
@@ -609,6 +645,57 @@ int qld_cuda_ld_hits(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m,
         return frc != QLD_OK ? frc
                              : set_err(c, QLD_ERR_TIMEOUT, "a counts kernel gave up a bounded wait");
     return rc;
+}
+
+int qld_cuda_count_states(qld_ctx *c, const uint64_t *A, int m, const uint64_t *B, int n, int K,
+                          int symmetric, uint8_t *states_out) {
+    if (!c) return QLD_ERR_INVALID;
+    if (symmetric) { B = A; n = m; }
+    if (m < 0 || n < 0 || K < 1)
+        return set_err(c, QLD_ERR_INVALID, "bad sizes m=%d n=%d K=%d", m, n, K);
+    if (m == 0 || n == 0) return QLD_OK;
+    if (!A || !B || !states_out)
+        return set_err(c, QLD_ERR_INVALID, "NULL table or output pointer");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    Task t;
+    int rc;
+    if ((rc = stage_tables(c, A, nullptr, m, B, nullptr, n, K, 1, symmetric, &t))) return rc;
+    const int band = c->band_rows;
+    const int nbands = (n + band - 1) / band;
+    const size_t slot_rows = (size_t)(n < band ? n : band);
+    for (int s = 0; s < 2 && s < nbands; ++s)
+        if ((rc = ensure(c, c->dOut[s], slot_rows * m))) return rc;
+    for (int bi = 0; bi < nbands; ++bi) {
+        const int s = bi & 1;
+        const int b0 = bi * band, b1 = b0 + band < n ? b0 + band : n;
+        if (bi >= 2) CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_copy[s], 0));
+        uint8_t *os = static_cast<uint8_t *>(c->dOut[s].p);
+        if ((rc = launch_states_range(c, t, b0, b1, os, m, b0, c->stream))) return rc;
+        CUDA_TRY(c, cudaEventRecord(c->ev_band[s], c->stream));
+        CUDA_TRY(c, cudaStreamWaitEvent(c->copy, c->ev_band[s], 0));
+        CUDA_TRY(c, cudaMemcpyAsync(states_out + (size_t)b0 * m, os, (size_t)(b1 - b0) * m,
+                                    cudaMemcpyDeviceToHost, c->copy));
+        CUDA_TRY(c, cudaEventRecord(c->ev_copy[s], c->copy));
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(c->copy));
+    return finish(c, c->stream);
+}
+
+int qld_cuda_count_states_device(qld_ctx *c, const uint64_t *A, int m, long long lda,
+                                 const uint64_t *B, int n, long long ldb, int K, int symmetric,
+                                 uint8_t *states, long long lds, void *stream) {
+    if (!c) return QLD_ERR_INVALID;
+    if (symmetric) { B = A; n = m; ldb = lda; }
+    if (m < 0 || n < 0 || K < 1 || lda < K || ldb < K || (lda & 1) || (ldb & 1) || lds < m)
+        return set_err(c, QLD_ERR_INVALID, "bad sizes/strides m=%d n=%d K=%d lda=%lld ldb=%lld",
+                       m, n, K, lda, ldb);
+    if (m == 0 || n == 0) return QLD_OK;
+    if (!A || !B || !states || !aligned16(A) || !aligned16(B))
+        return set_err(c, QLD_ERR_INVALID, "NULL or misaligned device pointer");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    Task t{A, nullptr, m, lda, B, nullptr, n, ldb, K, 1, symmetric, 0};
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    return launch_states_range(c, t, 0, n, states, lds, 0, st);
 }
 
 int qld_cuda_ld_device(qld_ctx *c, const qld_ld_args *a, void *stream) {

@@ -60,6 +60,21 @@ extern const KernelShape kBatchShape;
 // Persistent batched launch over all items of bp.jobs (max_ctas > 0 caps the grid).
 cudaError_t launch_batch(const BatchParams &bp, int r2_mode, int max_ctas, cudaStream_t st);
 
+// COUNTSTATES (ld_states.cu): state value of every pair, one byte each at
+// out[(b - out_row0) * lds + a]; single region: only a >= b.
+struct StatesParams {
+    int m, n, K, symmetric;
+    int tb0;                  // first B tile of this launch
+    uint8_t *out;
+    long long lds;
+    int out_row0;
+    unsigned *status;
+    long long timeout_cycles;
+};
+extern const KernelShape kStatesShape;
+cudaError_t launch_states(const CUtensorMap &tmA, const CUtensorMap &tmB, const StatesParams &p,
+                          int tiles_b, cudaStream_t st);
+
 // Report filter over `rows` r^2 rows (ldr >= m rounded up to 128 floats,
 // 16-byte aligned rows): mask (rows x W words, W = ceil(m / 32)), per-row
 // counts, offsets (rows + 1) and the kept values (hits.cu).  Row r is B row

@@ -10,8 +10,9 @@
  * reference|exact (default reference: the report is byte-identical to
  * qLD-compute's), -filter gpu|host (default gpu: qld_cuda_ld_hits keeps the
  * report's pairs on the device and only they cross PCIe; host: the dense r^2
- * array comes back and report.c filters it) and -timing (per-task phase
- * times as JSON on stderr).
+ * array comes back and report.c filters it), -countstates (the COUNTSTATES
+ * report of qLD-compute's -DCOUNTSTATES build, correlate_IO.c:430-516,
+ * instead of r^2) and -timing (per-task phase times as JSON on stderr).
  * -competing, -sorted, -rTable and -gpu are accepted and change nothing
  * (scheduling switches); -sampleList is not supported; -seed is rejected as
  * qLD-compute rejects it (its parser falls through to the invalid-parameter
@@ -63,7 +64,7 @@ static void usage(FILE *f)
           "unphased_diploid -mdf\n"
           "              [-posWmin1 P -posWmax1 P -posWmin2 P -posWmax2 P] [-inputList CSV]\n"
           "              [-r2limit R] [-threads T] [-device D] [-r2mode reference|exact]\n"
-          "              [-filter gpu|host] [-timing]\n",
+          "              [-filter gpu|host] [-countstates] [-timing]\n",
           f);
 }
 
@@ -348,12 +349,49 @@ static int run_dense(qld_ctx *ctx, const loaded *l, const char *out, float r2lim
     return bad;
 }
 
+/* COUNTSTATES task (qLD's -DCOUNTSTATES build): every pair's state value on
+ * the GPU, then writeStateCount()'s report. */
+static int run_states(qld_ctx *ctx, const loaded *l, const char *out, int threads, double *ld_s,
+                      double *rep_s)
+{
+    const qld_table *A = &l->A, *B = l->single ? &l->A : &l->B;
+    const double t0 = now_s();
+    uint8_t *st = NULL;
+    const size_t cells = (size_t)A->rows * (size_t)B->rows;
+    int rc = cells ? qld_cuda_host_alloc(ctx, cells, (void **)&st) : QLD_OK;
+    if (rc == QLD_OK && cells)
+        rc = qld_cuda_count_states(ctx, A->words, A->rows, B->words, B->rows, l->K, l->single,
+                                   st);
+    *ld_s = now_s() - t0;
+    int bad = 0;
+    FILE *fp = NULL;
+    if (rc != QLD_OK) {
+        fprintf(stderr, "ERROR: %s: %s\n", out, qld_cuda_last_error(ctx));
+        bad = 1;
+    } else if (!(fp = fopen(out, "wb"))) {
+        fprintf(stderr, "ERROR: cannot write %s\n", out);
+        bad = 1;
+    } else {
+        const double t1 = now_s();
+        if (qld_report_states(fp, A, B, st, l->tri, threads) != QLD_OK) {
+            fprintf(stderr, "ERROR: %s: %s\n", out, qld_host_last_error());
+            bad = 1;
+        }
+        if (fclose(fp) != 0)
+            bad = 1;
+        *rep_s = now_s() - t1;
+    }
+    if (st)
+        qld_cuda_host_free(ctx, st);
+    return bad;
+}
+
 int main(int argc, char **argv)
 {
     task base;
     memset(&base, 0, sizeof base);
     int ploidy = 0, threads = 1, device = 0, mode = QLD_R2_REFERENCE, timing = 0, mdf = 0;
-    int gpu_filter = 1;
+    int gpu_filter = 1, count_states = 0;
     int have_in = 0, have_out = 0;
     float r2limit = 0.2f;   /* qLD-compute's default */
     const char *list = NULL;
@@ -366,6 +404,7 @@ int main(int argc, char **argv)
         }
         if (!strcmp(a, "-mdf")) { mdf = 1; continue; }
         if (!strcmp(a, "-timing")) { timing = 1; continue; }
+        if (!strcmp(a, "-countstates")) { count_states = 1; continue; }
         /* qLD-compute's scheduling switches: tasks run in list order on one
          * GPU here, so they change nothing in the reports */
         if (!strcmp(a, "-competing") || !strcmp(a, "-sorted") || !strcmp(a, "-rTable") ||
@@ -475,15 +514,17 @@ int main(int argc, char **argv)
         } else {
             double ld_s = 0, rep_s = 0;
             const qld_table *B = cur.single ? &cur.A : &cur.B;
-            if ((gpu_filter ? run_filtered : run_dense)(ctx, &cur, tasks[t].out, r2limit, threads,
-                                                       &ld_s, &rep_s))
+            if (count_states ? run_states(ctx, &cur, tasks[t].out, threads, &ld_s, &rep_s)
+                             : (gpu_filter ? run_filtered : run_dense)(ctx, &cur, tasks[t].out,
+                                                                      r2limit, threads, &ld_s,
+                                                                      &rep_s))
                 status = 1;
             if (timing)
                 fprintf(stderr,
                         "{\"task\": \"%s\", \"rows_a\": %d, \"rows_b\": %d, \"load_s\": %.6f, "
                         "\"ld_s\": %.6f, \"report_s\": %.6f, \"filter\": \"%s\"}\n",
                         tasks[t].out, cur.A.rows, B->rows, cur.load_s, ld_s, rep_s,
-                        gpu_filter ? "gpu" : "host");
+                        count_states ? "states" : gpu_filter ? "gpu" : "host");
         }
         qld_table_free(ctx, &cur.A);
         qld_table_free(ctx, &cur.B);

@@ -154,6 +154,7 @@ static int emit(block *b, const rowtxt *bt, const rowtxt *at, float v)
  * r2 + i*m, kept if r2limit <= v < 100 and, with `single`, j > row0 + i) or
  * from a qld_cuda_ld_hits block (mask bits and packed values). */
 typedef struct rep_job {
+    const uint8_t *states;     /* COUNTSTATES rows instead of r^2 */
     const float *r2;
     float r2limit;
     int single;
@@ -166,10 +167,41 @@ typedef struct rep_job {
     atomic_int failed;
 } rep_job;
 
+/* writeStateCount's line: POS2 POS1 ID2 ID1 <states> and a trailing tab. */
+static int emit_states(block *b, const rowtxt *bt, const rowtxt *at, unsigned st)
+{
+    if (ensure(b, (size_t)bt->pos_n + at->pos_n + bt->id_n + at->id_n + 16))
+        return -1;
+    char *o = b->buf + b->len;
+    memcpy(o, bt->pos, bt->pos_n); o += bt->pos_n; *o++ = '\t';
+    memcpy(o, at->pos, at->pos_n); o += at->pos_n; *o++ = '\t';
+    memcpy(o, bt->id, bt->id_n); o += bt->id_n; *o++ = '\t';
+    memcpy(o, at->id, at->id_n); o += at->id_n; *o++ = '\t';
+    char d[4];
+    int nd = 0;
+    do {
+        d[nd++] = (char)('0' + st % 10);
+        st /= 10;
+    } while (st);
+    while (nd)
+        *o++ = d[--nd];
+    *o++ = '\t';
+    *o++ = '\n';
+    b->len = (size_t)(o - b->buf);
+    return 0;
+}
+
 static int format_row(const rep_job *j, int i, block *b)
 {
     const int gi = j->row0 + i;
     const rowtxt *bt = &j->tb[gi];
+    if (j->states) {
+        const uint8_t *row = j->states + (size_t)i * j->m;
+        for (int c = j->single ? gi + 1 : 0; c < j->m; ++c)
+            if (emit_states(b, bt, &j->ta[c], row[c]))
+                return -1;
+        return 0;
+    }
     if (j->hits) {
         const qld_hits_block *h = j->hits;
         const uint32_t *mw = h->mask + (size_t)i * h->words;
@@ -263,6 +295,8 @@ static int run_rows(qld_report *r, rep_job *proto, int row0, int n)
         j.n = rows;
         if (j.r2)
             j.r2 = proto->r2 + (size_t)i0 * j.m;
+        if (j.states)
+            j.states = proto->states + (size_t)i0 * j.m;
         qld_hits_block sub;
         if (proto->hits) {   /* the same block seen from local row i0 */
             sub = *proto->hits;
@@ -333,6 +367,40 @@ int qld_report_write(FILE *fp, const qld_table *A, const qld_table *B, const flo
         memset(&proto, 0, sizeof proto);
         proto.r2 = r2;
         proto.r2limit = r2limit;
+        proto.single = single_region;
+        proto.m = A->rows;
+        rc = run_rows(r, &proto, 0, B->rows);
+    }
+    qld_report_close(r);
+    return rc;
+}
+
+int qld_report_states(FILE *fp, const qld_table *A, const qld_table *B, const uint8_t *states,
+                      int single_region, int threads)
+{
+    if (!fp || !A || !B || (!states && A->rows && B->rows))
+        return qld_host_fail(QLD_ERR_INVALID, "bad report arguments");
+    qld_report *r = calloc(1, sizeof *r);
+    if (!r)
+        return qld_host_fail(QLD_ERR_NOMEM, "out of memory");
+    r->fp = fp;
+    r->A = A;
+    r->B = B;
+    r->snip_size = 1;
+    r->threads = threads < 1 ? 1 : threads;
+    r->rows_per_block = 64;
+    r->per_round = r->threads * 4;
+    r->blocks = calloc((size_t)r->per_round, sizeof *r->blocks);
+    int rc = QLD_OK;
+    if (!r->blocks || row_texts(A, 1, &r->ta, &r->pa) ||
+        (B == A ? (r->tb = r->ta, 0) : row_texts(B, 1, &r->tb, &r->pb)))
+        rc = qld_host_fail(QLD_ERR_NOMEM, "out of memory");
+    else if (fputs("POS2\tPOS1\tID2\tID1\tNo_STATES\n", fp) == EOF)
+        rc = qld_host_fail(QLD_ERR_INVALID, "write failed");
+    else if (A->rows && B->rows) {
+        rep_job proto;
+        memset(&proto, 0, sizeof proto);
+        proto.states = states;
         proto.single = single_region;
         proto.m = A->rows;
         rc = run_rows(r, &proto, 0, B->rows);

@@ -89,6 +89,9 @@ def lib() -> ct.CDLL:
         L.qld_report_hits.restype = ct.c_int
         L.qld_report_close.argtypes = [ct.c_void_p]
         L.qld_report_close.restype = ct.c_int
+        L.qld_report_states.argtypes = [ct.c_void_p, ct.POINTER(_Table), ct.POINTER(_Table),
+                                        ct.c_void_p, ct.c_int, ct.c_int]
+        L.qld_report_states.restype = ct.c_int
         L.qld_host_last_error.argtypes = []
         L.qld_host_last_error.restype = ct.c_char_p
         _lib = L
@@ -219,6 +222,28 @@ def write_report(path: str, A: Table, B: Table, r2: np.ndarray, snip_size: int,
         rc = lib().qld_report_write(fp, ct.byref(ta), ct.byref(tb), r2.ctypes.data,
                                     int(snip_size), float(r2limit), int(bool(single_region)),
                                     int(threads))
+    finally:
+        if libc.fclose(fp) != 0:
+            raise OSError(f"cannot close {path}")
+    _check(rc)
+
+
+def write_states_report(path: str, A: Table, B: Table, states: np.ndarray,
+                        single_region: bool, threads: int = 1) -> None:
+    """qLD's COUNTSTATES report (writeStateCount); states is (B rows, A rows) uint8."""
+    states = np.ascontiguousarray(states, np.uint8)
+    if states.shape != (len(B.pos), len(A.pos)):
+        raise ValueError(f"states is {states.shape}, expected {(len(B.pos), len(A.pos))}")
+    libc = _libc()
+    keep: list = []
+    ta = _as_c_table(A, keep)
+    tb = ta if B is A else _as_c_table(B, keep)
+    fp = libc.fopen(os.fsencode(path), b"wb")
+    if not fp:
+        raise OSError(f"cannot open {path}")
+    try:
+        rc = lib().qld_report_states(fp, ct.byref(ta), ct.byref(tb), states.ctypes.data,
+                                     int(bool(single_region)), int(threads))
     finally:
         if libc.fclose(fp) != 0:
             raise OSError(f"cannot close {path}")

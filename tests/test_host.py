@@ -177,6 +177,22 @@ def test_report_hits_rejects_foreign_block(tmp_path):
         host_api.write_report_hits(str(tmp_path / "x.txt"), A, A, [(35, mask, off, val)], 10)
 
 
+@pytest.mark.parametrize("threads", [1, 4])
+def test_states_report_matches_golden(tmp_path, threads):
+    """The C states writer with the oracle's states against the reference's
+    COUNTSTATES reports (tests/golden/states)."""
+    from test_oracle import _states_cases, load_states_golden
+    for name in _states_cases():
+        g = load_states_golden(name)
+        st = oracle.count_states(g["A"], g["B"])
+        A = host_api.Table(g["A"], np.zeros(len(g["posA"]), np.uint32), g["posA"], g["idA"])
+        B = A if g["single"] else host_api.Table(g["B"], np.zeros(len(g["posB"]), np.uint32),
+                                                 g["posB"], g["idB"])
+        out = tmp_path / f"{name}.txt"
+        host_api.write_states_report(str(out), A, B, st, g["single"], threads=threads)
+        assert out.read_bytes() == g["report"], name
+
+
 def _cli(*args, timeout=60):
     return subprocess.run([host_api.CLI_PATH, *args], capture_output=True, text=True,
                           timeout=timeout)

@@ -1,10 +1,12 @@
 """CPU tests: the oracle against the reference's golden vectors (and against
 the reference library itself when it is built)."""
+import os
+
 import numpy as np
 import pytest
 
 import oracle
-from conftest import golden_names, load_golden, lower_mask
+from conftest import GOLDEN, golden_names, load_golden, lower_mask
 
 
 @pytest.mark.parametrize("name", golden_names())
@@ -87,3 +89,57 @@ def test_restatement_matches_reference_library_random():
         r_ref = oracle.ref_ld_score(bcA, bcB, C.astype(np.uint64), S)
         r_me = oracle.r2_reference(bcA, bcB, C, S, fma_contract=False)
         assert np.array_equal(r_ref.view(np.uint32), r_me.view(np.uint32))
+
+
+def _states_cases():
+    d = os.path.join(GOLDEN, "states")
+    return sorted(f[:-4] for f in os.listdir(d) if f.endswith(".npz")) if os.path.isdir(d) else []
+
+
+def load_states_golden(name):
+    """A COUNTSTATES golden case: the table, its A/B windows (rows by
+    position, as qLD's window rule keeps them) and the reference's report."""
+    z = np.load(os.path.join(GOLDEN, "states", f"{name}.npz"))
+    flags = [str(f) for f in z["flags"]]
+    t, pos = z["table"], z["positions"]
+    win = dict(zip(flags[::2], (int(v) for v in flags[1::2])))
+    single = "-posWmin2" not in win
+    lo1, hi1 = win.get("-posWmin1", int(pos[0])), win.get("-posWmax1", int(pos[-1]))
+    a = (pos >= lo1) & (pos <= hi1)
+    b = a if single else (pos >= win["-posWmin2"]) & (pos <= win["-posWmax2"])
+    ids = np.array([f"rs{i + 1}" for i in range(len(pos))])
+    with open(os.path.join(GOLDEN, "states", f"{name}.report.txt"), "rb") as f:
+        report = f.read()
+    return dict(z=z, flags=flags, single=single, A=t[a], posA=pos[a], idA=list(ids[a]),
+                B=t[b], posB=pos[b], idB=list(ids[b]), report=report)
+
+
+@pytest.mark.parametrize("name", _states_cases())
+def test_count_states_report_matches_golden(name):
+    g = load_states_golden(name)
+    st = oracle.count_states(g["A"], g["B"])
+    rep = oracle.write_states(g["posA"], g["idA"], g["posB"], g["idB"], st,
+                              0 if g["single"] else 1)
+    assert rep == g["report"]
+
+
+def test_count_states_small_python_restatement():
+    """The C loop against a literal Python transcription on a small case."""
+    rng = np.random.default_rng(5)
+    A = rng.integers(0, 2**63, (6, 2), dtype=np.uint64)
+    A[0] = 0
+    A[1, 1] = 0
+    B = rng.integers(0, 2**63, (4, 2), dtype=np.uint64) & np.uint64(0xF0F0F0F0F0F0F0F0)
+
+    def states(a, b):
+        s = 0
+        for k in range(len(a)):
+            for p in range(64):
+                if s == 15:
+                    break
+                s |= 1 << (((int(a[k]) >> p) & 1) * 2 + ((int(b[k]) >> p) & 1))
+            s = bin(s).count("1")
+        return s
+
+    want = np.array([[states(A[j], B[i]) for j in range(6)] for i in range(4)], np.uint8)
+    assert np.array_equal(oracle.count_states(A, B), want)
