@@ -162,6 +162,34 @@ int qld_cuda_count_states_device(qld_ctx *ctx, const uint64_t *A, int m, long lo
                                  uint8_t *states, long long lds, void *stream);
 
 /*
+ * VCF -> MDF packing on the GPU: the per-sample half of qLD-parse-2MDF
+ * (src/mdf_extension/src/process_data.c:152-328, snip_processing.c).  Each
+ * site is one VCF data line that passed its fixed-field checks: the bytes of
+ * its sample fields in `text` (separated by spaces/tabs), the index of GT in
+ * FORMAT and the REF/ALT state characters.  Per site: the valid samples'
+ * alleles (getGTfield/getGTdata: digits -> states, '.' -> 'N', unphased
+ * '/' groups shuffled with rand()), qLD's polymorphism test and the packed
+ * row -- K words MSB-first, bit 1 for a base other than the site's first
+ * base -- with its BC.  `rng` is called once per random draw, in qLD's order
+ * (libc rand() reproduces qLD's shuffles); it may be NULL when no genotype
+ * is unphased.  Outputs per site: words (nsites x K), bc, snip_len (alleles
+ * in the row), keep (1: the row goes to the MDF).  A data error returns
+ * QLD_ERR_INVALID with the first failing site in *err_site (else -1).
+ */
+typedef struct qld_vcf_site {
+    long long off;      /* first byte of the line's sample fields in text */
+    int len;            /* bytes from there to the end of the line */
+    int gt_pos;         /* index of GT among the FORMAT subfields */
+    int n_states;       /* REF + ALT states */
+    char states[4];     /* REF, then ALT ('.' replaced by REF) */
+} qld_vcf_site;
+typedef unsigned (*qld_rand_fn)(void *user);
+int qld_cuda_vcf_pack(qld_ctx *ctx, const char *text, size_t text_bytes,
+                      const qld_vcf_site *sites, int nsites, const uint8_t *valid, int nsamples,
+                      int ploidy, int K, qld_rand_fn rng, void *rng_user, uint64_t *words,
+                      uint32_t *bc, int *snip_len, uint8_t *keep, int *err_site);
+
+/*
  * Windowed (band) LD over one region: r^2 only for SNP pairs (i, j) with
  * 1 <= j - i <= band.  Output is the m x band array r2_band[i*band + d] =
  * r^2(SNP i, SNP i+1+d) (entries with i+1+d >= m are unspecified); counts_band

@@ -1,6 +1,7 @@
 /*
  * qld_host.h -- C host layer of the -cuda mode: MDF dataset loading into
- * pinned memory and the text report, both multithreaded (libqld_host.so).
+ * pinned memory and the text report, both multithreaded, and the host half
+ * of VCF -> MDF conversion (libqld_host.so).
  *
  * Formats are qLD's own:
  *  - an MDF dataset is a directory with <id>_header.vcf.gz (VCF meta line,
@@ -53,9 +54,11 @@ int qld_mdf_read_header(const char *dir, qld_mdf_header *h);
 /*
  * Rows with pos_min <= POS <= pos_max of every part of the dataset, in file
  * order, K words per row (K = ceil(valid samples / 64)); words past K on a
- * line must be zero (qLD-parse-2MDF's diploid default writes such padding).
- * Parts are parsed by `threads` threads and assembled in pinned memory from
- * `ctx` (ctx NULL: pageable memory, no GPU needed).  Replaces findFiles() + readTable_x64() (correlate_IO.c:294-376,
+ * line are ignored, as qLD-compute ignores them (qLD-parse-2MDF's diploid
+ * default pads haploid rows with words it does not initialise).  Parts are
+ * parsed by `threads` threads and assembled in pinned memory from `ctx`
+ * (ctx NULL: pageable memory, no GPU needed).  Replaces findFiles() +
+ * readTable_x64() (correlate_IO.c:294-376,
  * correlate_IOx64.c:351-461) for MDF input; returns QLD_ERR_INVALID with a
  * message (qld_host_last_error) for malformed files instead of exiting.
  */
@@ -92,6 +95,54 @@ int qld_report_open(qld_report **rep, FILE *fp, const qld_table *A, const qld_ta
                     int snip_size, int threads);
 int qld_report_hits(qld_report *rep, const qld_hits_block *block);
 int qld_report_close(qld_report *rep);
+
+/*
+ * VCF -> MDF (qLD-parse-2MDF, src/mdf_extension/src): the host reads a
+ * qLD-parse-VCF dataset -- a "*header*" file and parts <id>_<i0>_<i1>_<p0>_
+ * <p1>.vcf.gz -- and filters each data line on its fixed fields; the GPU
+ * turns the surviving lines' sample fields into packed rows
+ * (qld_cuda_vcf_pack); the host writes the MDF parts.
+ */
+typedef struct qld_vcf_header {
+    char id[256];          /* alignment id: the header file name up to '_' */
+    char path[4096];       /* the header file (copied next to the MDF parts) */
+    char *line1, *line2;   /* the first line and the #CHROM line every part repeats */
+    int nsamples;          /* sample names on the #CHROM line */
+    uint8_t *valid;        /* per sample: 1 if selected (no sample list: all) */
+    int valid_count;       /* selected samples x ploidy: K = ceil(valid_count / 64) */
+    int snips_per_file, snip_size, total_snips;
+} qld_vcf_header;
+
+int qld_vcf_read_header(const char *dir, int ploidy, const char *const *sample_list, int nlist,
+                        qld_vcf_header *h);
+void qld_vcf_header_free(qld_vcf_header *h);
+/* The dataset's part files in qLD's order (the first number after '_'). */
+int qld_vcf_list_parts(const char *dir, const qld_vcf_header *h, char ***paths, int *n);
+void qld_vcf_list_free(char **paths, int n);
+
+typedef struct qld_vcf_part {
+    char *text;            /* decompressed part (pinned when loaded with a context) */
+    size_t bytes;
+    int pinned;
+    int lines;             /* data lines read */
+    int skipped;           /* lines dropped on their fixed fields */
+    int nsites;            /* the other lines: sites for qld_cuda_vcf_pack */
+    qld_vcf_site *sites;
+    uint32_t *pos;         /* per site: POS */
+    size_t *ids;           /* per site: offset of its ID in id_pool */
+    char *id_pool;
+} qld_vcf_part;
+
+int qld_vcf_load_part(qld_ctx *ctx, const char *path, const qld_vcf_header *h,
+                      qld_vcf_part *out);
+void qld_vcf_part_free(qld_ctx *ctx, qld_vcf_part *p);
+const char *qld_vcf_site_id(const qld_vcf_part *p, int site);
+
+/* <out_dir>/<part name without ".vcf.gz">.mdf, and the MDF text of the kept
+ * sites (process_data.c:441-460). */
+int qld_mdf_part_path(const char *out_dir, const char *part_path, char *buf, size_t cap);
+int qld_mdf_write_part(const char *path, const char *id, const qld_vcf_part *p, int K,
+                       const uint64_t *words, const uint32_t *bc, const uint8_t *keep);
 
 const char *qld_host_last_error(void);
 

@@ -72,6 +72,11 @@ def _lib(name: str) -> ct.CDLL:
                 ct.c_char_p, ct.c_size_t, _u32p, ct.POINTER(ct.c_char_p), ct.c_int,
                 _u32p, ct.POINTER(ct.c_char_p), ct.c_int, ct.c_void_p, ct.c_int]
             lib.qo_write_states.restype = ct.c_size_t
+            lib.qo_srand.argtypes = [ct.c_uint]
+            lib.qo_vcf_pack.argtypes = [ct.c_char_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int,
+                                        ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                        ct.c_void_p, ct.POINTER(ct.c_char_p)]
+            lib.qo_vcf_pack.restype = ct.c_int
         elif name == "ref":
             path = os.path.join(_HERE, "_ref", "libqldref.so")
             if not os.path.exists(path):
@@ -195,6 +200,35 @@ def write_states(posA, idA, posB, idB, states, posWset2) -> bytes:
     buf = ct.create_string_buffer(need + 1)
     lib.qo_write_states(buf, need + 1, *args)
     return buf.raw[:need]
+
+
+VCF_SITE = np.dtype([("off", np.int64), ("len", np.int32), ("gt_pos", np.int32),
+                     ("n_states", np.int32), ("states", "S4")], align=True)
+
+
+def vcf_seed(seed: int) -> None:
+    """srand() of the C library the oracle calls rand() from."""
+    _lib("oracle").qo_srand(int(seed))
+
+
+def vcf_pack(text: bytes, sites: np.ndarray, valid, ploidy: int, K: int):
+    """qLD-parse-2MDF's per-site processing of `sites` (VCF_SITE records over
+    `text`): (words (n, K) uint64, bc, snip_len, keep), or raises ValueError
+    naming the first site qLD stops on."""
+    sites = np.ascontiguousarray(sites, VCF_SITE)
+    valid = np.ascontiguousarray(valid, np.uint8)
+    n = len(sites)
+    words = np.zeros((max(n, 1), K), np.uint64)
+    bc = np.zeros(max(n, 1), np.uint32)
+    ln = np.zeros(max(n, 1), np.int32)
+    keep = np.zeros(max(n, 1), np.uint8)
+    what = ct.c_char_p()
+    fail = _lib("oracle").qo_vcf_pack(text, sites.ctypes.data, n, valid.ctypes.data, len(valid),
+                                      int(ploidy), int(K), words.ctypes.data, bc.ctypes.data,
+                                      ln.ctypes.data, keep.ctypes.data, ct.byref(what))
+    if fail >= 0:
+        raise ValueError(f"site {fail}: {what.value.decode()}")
+    return words[:n], bc[:n], ln[:n], keep[:n]
 
 
 # --------------------------------------------------------------- reference --

@@ -24,6 +24,11 @@
  *   qo_count_states    <- countStates_mode()  correlate_IO.c:472-516 (the
  *                         COUNTSTATES build), bit loop and all
  *   qo_write_states    <- writeStateCount()   correlate_IO.c:430-470
+ *   qo_vcf_pack        <- qLD-parse-2MDF's per-site processing: getGTfield,
+ *                         getGTdata, determineStates,
+ *                         removeNonPolymorphicSite, binaryDeduction,
+ *                         compressSnip_x64 (src/mdf_extension/src/
+ *                         process_data.c:152-328, snip_processing.c:270-797)
  *
  * Build with -ffp-contract=off: every fused multiply-add below is written as
  * an explicit fmaf() so the rounding never depends on compiler flags.
@@ -328,4 +333,281 @@ QO_EXPORT size_t qo_write_states(char *buf, size_t cap, const uint32_t *posA, ch
         }
     }
     return s.len;
+}
+
+/* ------------------------------------------------------------ VCF -> MDF -- */
+
+/*
+ * qLD-parse-2MDF's per-site processing (src/mdf_extension/src/process_data.c:
+ * 152-328, snip_processing.c:270-797), restated step by step for the sites a
+ * host parser hands over (sample fields of one VCF line, GT position, REF/ALT
+ * states).  Random draws use libc rand() as qLD does; seed with qo_srand.
+ * Returns 0, or the index of the first site qLD would stop on (with *what
+ * set to a short reason).
+ */
+typedef struct qo_site {
+    long long off;
+    int len, gt_pos, n_states;
+    char states[4];
+} qo_site;
+
+QO_EXPORT void qo_srand(unsigned seed) { srand(seed); }
+
+/* getGTfield: keep subfield `pos` in place; returns separators + 1. */
+static int qo_gt_field(char *s, int pos)
+{
+    int len = (int)strlen(s), j = 0, counter = 0;
+    for (int i = 0; i < len; i++) {
+        if (s[i] != ':') {
+            if (pos == 0) {
+                s[j++] = s[i];
+                if (s[i] == '|' || s[i] == '/')
+                    counter++;
+            }
+        } else {
+            pos--;
+            if (pos == -1) {
+                s[j] = 0;
+                break;
+            }
+        }
+    }
+    return counter + 1;
+}
+
+static void qo_shuffle(char *d, int start, int end)
+{
+    if (start == end)
+        return;
+    for (int i = end; i > start; i--) {
+        int idx = start + (rand() % (i - start + 1));
+        char t = d[idx];
+        d[idx] = d[i];
+        d[i] = t;
+    }
+}
+
+/* getGTdata; returns 0 or an error reason. */
+static const char *qo_gt_data(const char *s, const char *states, int nstates, char *out)
+{
+    int len = (int)strlen(s), j = 0, start = 0, end = 0;
+    for (int i = 0; i < len; i++) {
+        if (s[i] >= '0' && s[i] <= '9') {
+            if (s[i] - '0' >= nstates)
+                return "allele index past the REF/ALT states";
+            if (j + 1 >= 4)
+                return "more than three alleles in a genotype";
+            out[j++] = states[s[i] - '0'];
+        } else {
+            if (s[i] == '.') {
+                if (j + 1 >= 4)
+                    return "more than three alleles in a genotype";
+                out[j++] = 'N';
+            }
+            if (s[i] == '/')
+                end++;
+            if (s[i] == '|') {
+                qo_shuffle(out, start, end);
+                start = j;
+                end = j;
+            }
+        }
+    }
+    qo_shuffle(out, start, end);
+    out[j] = 0;
+    return 0;
+}
+
+static int qo_map(char a)
+{
+    switch (a) {
+    case '0': return 0;
+    case '1': return 1;
+    case '-': case 'N': return 2;
+    case 'A': return 3;
+    case 'C': return 4;
+    case 'G': return 5;
+    case 'T': return 6;
+    default: return -1;
+    }
+}
+
+QO_EXPORT int qo_vcf_pack(const char *text, const qo_site *sites, int nsites,
+                          const uint8_t *valid, int nsamples, int ploidy, int K,
+                          uint64_t *words, uint32_t *bc, int *snip_len, uint8_t *keep,
+                          const char **what)
+{
+    static char reason[128];
+    *what = "";
+    size_t cap = (size_t)nsamples * 4 + 16;
+    char *snip = malloc(cap), *word = malloc(1 << 16);
+    int fail = -1;
+    for (int s = 0; s < nsites && fail < 0; s++) {
+        const qo_site *st = &sites[s];
+        char states[5] = {'X', 'X', 'X', 'X', 'X'};
+        for (int k = 0; k < st->n_states && k < 4; k++)
+            states[k] = st->states[k];
+        snip[0] = 0;
+        size_t sl = 0;
+        int sample = 0;
+        const char *t = text + st->off;
+        int i = 0;
+        /* getWordFromString over the segment: runs of spaces/tabs separate */
+        while (i < st->len) {
+            while (i < st->len && (t[i] == ' ' || t[i] == '\t'))
+                i++;
+            if (i >= st->len)
+                break;
+            int w = 0;
+            while (i < st->len && t[i] != ' ' && t[i] != '\t' && w < (1 << 16) - 1)
+                word[w++] = t[i++];
+            word[w] = 0;
+            if (sample >= nsamples) {
+                *what = "more sample fields than header samples";
+                fail = s;
+                break;
+            }
+            if (valid[sample]) {
+                const int size = qo_gt_field(word, st->gt_pos);
+                if (word[0] == 0) {
+                    *what = "empty GT field";
+                    fail = s;
+                    break;
+                }
+                if (size > ploidy) {
+                    *what = "Detected data bigger than the ploidy of input";
+                    fail = s;
+                    break;
+                }
+                char part[8];
+                const char *e = qo_gt_data(word, states, st->n_states, part);
+                if (e) {
+                    *what = e;
+                    fail = s;
+                    break;
+                }
+                if ((int)strlen(part) < size) {
+                    *what = "a genotype with fewer alleles than separators";
+                    fail = s;
+                    break;
+                }
+                memcpy(snip + sl, part, (size_t)size);
+                sl += (size_t)size;
+                snip[sl] = 0;
+            }
+            sample++;
+        }
+        if (fail >= 0)
+            break;
+        const int L = (int)sl;
+        snip_len[s] = L;
+        keep[s] = 0;
+        bc[s] = 0;
+        memset(words + (size_t)s * K, 0, sizeof(uint64_t) * (size_t)K);
+        if (L == 0) {
+            *what = "no alleles (empty alignment)";
+            fail = s;
+            break;
+        }
+        if (L > K * 64) {
+            *what = "Detected data bigger than the ploidy of input";
+            fail = s;
+            break;
+        }
+        /* determineStates / getDataType */
+        int cnt[8] = {0};
+        for (int q = 0; q < L; q++) {
+            const int m = qo_map(snip[q]);
+            if (m < 0) {
+                snprintf(reason, sizeof reason, "a state character qLD cannot map (%c)", snip[q]);
+                *what = reason;
+                fail = s;
+                break;
+            }
+            cnt[m]++;
+        }
+        if (fail >= 0)
+            break;
+        int acgt = cnt[3] + cnt[4] + cnt[5] + cnt[6], type;
+        if ((cnt[0] || cnt[1]) && acgt == 0)
+            type = cnt[2] ? 3 : 2;
+        else if (acgt && cnt[0] + cnt[1] == 0)
+            type = cnt[2] ? 5 : 4;
+        else if (cnt[2])
+            type = 6;
+        else
+            type = 0;
+        /* removeNonPolymorphicSite with filterOut = 0 */
+        int rm = 0;
+        if (type == 4 || type == 5 || type == 2 || type == 3) {
+            int setv[8] = {0};
+            rm = 1;
+            const int dna = type >= 4;
+            for (int q = 0; q < L; q++) {
+                setv[qo_map(snip[q])]++;
+                const int dif = dna ? (setv[3] != 0) + (setv[4] != 0) + (setv[5] != 0) +
+                                          (setv[6] != 0)
+                                    : (setv[0] != 0) + (setv[1] != 0);
+                if (dif >= 2) {
+                    rm = 0;
+                    break;
+                }
+            }
+            if (setv[2])
+                rm = 1;
+        } else if (type == 6) {
+            rm = 1;
+        }
+        if (rm)
+            continue;
+        /* binaryDeduction: two bases here, so minorToMajor changes nothing;
+         * convertAlignmentBIN: the first base -> '0', the other -> '1' */
+        if (type == 4 || type == 5) {
+            char s0 = 'x', s1 = 'x';
+            int distinct = 0;
+            int seen[8] = {0};
+            for (int q = 0; q < L; q++) {
+                const int m = qo_map(snip[q]);
+                if (m >= 3 && !seen[m]) {
+                    seen[m] = 1;
+                    distinct++;
+                }
+            }
+            if (distinct > 2) {
+                *what = "more than two bases at a site";
+                fail = s;
+                break;
+            }
+            if (distinct == 2)
+                for (int q = 0; q < L; q++) {
+                    const char c = snip[q];
+                    if (s0 == 'x' && c != '-' && c != 'N')
+                        s0 = c;
+                    if (s0 != 'x' && s1 == 'x' && c != s0 && c != '-' && c != 'N')
+                        s1 = c;
+                    snip[q] = c == '-' ? '-' : c == 'N' ? 'N' : c == s0 ? '0' : c == s1 ? '1' : 'X';
+                }
+        }
+        /* compressSnip_x64: bit = character & 1, MSB first */
+        uint64_t *w = words + (size_t)s * K, tmp = 0;
+        int nb = 0, wi = 0;
+        uint32_t ones = 0;
+        for (int q = 0; q < L; q++) {
+            const uint64_t b = (uint64_t)((unsigned char)snip[q] & 1u);
+            tmp = (tmp << 1) | b;
+            ones += (uint32_t)b;
+            if (++nb == 64) {
+                w[wi++] = tmp;
+                tmp = 0;
+                nb = 0;
+            }
+        }
+        if (nb)
+            w[wi] = tmp << (64 - nb);
+        bc[s] = ones;
+        keep[s] = 1;
+    }
+    free(snip);
+    free(word);
+    return fail;
 }

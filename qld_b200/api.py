@@ -32,7 +32,7 @@ OPT_KERNEL, OPT_R2_MODE, OPT_PROFILE, OPT_BAND_ROWS, OPT_MMA_TILE = 1, 2, 3, 4, 
 EXPORTED = (
     "qld_cuda_init", "qld_cuda_release", "qld_cuda_last_error", "qld_cuda_set_option",
     "qld_cuda_ld", "qld_cuda_ld_device", "qld_cuda_ld_hits", "qld_cuda_ld_batch",
-    "qld_cuda_count_states", "qld_cuda_count_states_device",
+    "qld_cuda_count_states", "qld_cuda_count_states_device", "qld_cuda_vcf_pack",
     "qld_cuda_ld_band",
     "qld_cuda_ld_band_device", "qld_cuda_sync",
     "qld_cuda_host_alloc",
@@ -82,6 +82,7 @@ class HitsBlock(ct.Structure):
 
 
 HITS_FN = ct.CFUNCTYPE(ct.c_int, ct.c_void_p, ct.POINTER(HitsBlock))
+RAND_FN = ct.CFUNCTYPE(ct.c_uint, ct.c_void_p)
 
 
 class _Query(ct.Structure):
@@ -116,6 +117,8 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.qld_cuda_ld_device.argtypes = [vp, ct.POINTER(_LdArgs), vp]
     lib.qld_cuda_ld_batch.argtypes = [vp, ct.POINTER(_LdArgs), i, vp]
     lib.qld_cuda_count_states.argtypes = [vp, vp, i, vp, i, i, i, vp]
+    lib.qld_cuda_vcf_pack.argtypes = [vp, ct.c_char_p, ct.c_size_t, vp, i, vp, i, i, i, RAND_FN,
+                                      vp, vp, vp, vp, vp, ct.POINTER(i)]
     lib.qld_cuda_count_states_device.argtypes = [vp, vp, i, ll, vp, i, ll, i, i, vp, ll, vp]
     lib.qld_cuda_ld_hits.argtypes = [vp, vp, vp, i, vp, vp, i, i, i, i, i, ct.c_float, HITS_FN, vp]
     lib.qld_cuda_ld_band.argtypes = [vp, vp, vp, i, i, i, i, vp, vp]
@@ -317,6 +320,37 @@ class Context:
         self._check(self.lib.qld_cuda_count_states(self.h, _ptr(A), m, _ptr(B), n, K,
                                                    int(bool(symmetric)), _ptr(out)))
         return out
+
+    def vcf_pack(self, text: bytes, sites: np.ndarray, valid, ploidy: int, K: int,
+                 seed: int | None = 1):
+        """qld_cuda_vcf_pack over qld_vcf_site records `sites` (a numpy array of
+        host_api.VCF_SITE): returns (words (n, K) uint64, bc, snip_len, keep).
+        Unphased genotypes draw from libc rand() after srand(seed), as
+        qLD-parse-2MDF does; seed None leaves the generator unseeded."""
+        sites = np.ascontiguousarray(sites)
+        valid = np.ascontiguousarray(valid, np.uint8)
+        n = len(sites)
+        words = np.zeros((max(n, 1), K), np.uint64)
+        bc = np.zeros(max(n, 1), np.uint32)
+        ln = np.zeros(max(n, 1), np.int32)
+        keep = np.zeros(max(n, 1), np.uint8)
+        libc = ct.CDLL(None)
+        libc.rand.restype = ct.c_int
+        seeded = [seed is None]
+
+        def draw(_user):
+            if not seeded[0]:
+                libc.srand(ct.c_uint(seed))
+                seeded[0] = True
+            return libc.rand()
+
+        fn = RAND_FN(draw)
+        bad = ct.c_int(-1)
+        self._check(self.lib.qld_cuda_vcf_pack(self.h, text, len(text), sites.ctypes.data, n,
+                                               valid.ctypes.data, len(valid), int(ploidy), int(K),
+                                               fn, None, words.ctypes.data, bc.ctypes.data,
+                                               ln.ctypes.data, keep.ctypes.data, ct.byref(bad)))
+        return words[:n], bc[:n], ln[:n], keep[:n]
 
     def count_states_device(self, A, m, lda, B, n, ldb, K, symmetric, out, lds, stream=None):
         self._check(self.lib.qld_cuda_count_states_device(

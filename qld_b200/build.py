@@ -5,9 +5,10 @@
 Every .cu file under csrc/ is compiled for ``-gencode arch=compute_100a,
 code=sm_100a`` and linked into ``qld_b200/libqld_cuda.so`` (static CUDA
 runtime, so the library carries its own runtime independent of torch's).
-The C host layer (host/mdf_loader.c, host/report.c) becomes
-``qld_b200/libqld_host.so`` and host/qld_ld_main.c the ``qld_b200/qld-ld``
-command, both linked against libqld_cuda.so through an $ORIGIN rpath.
+The C host layer (host/mdf_loader.c, host/report.c, host/vcf.c) becomes
+``qld_b200/libqld_host.so``, host/qld_ld_main.c the ``qld_b200/qld-ld`` command
+and host/vcf2mdf_main.c ``qld_b200/qld-vcf2mdf``, all linked against
+libqld_cuda.so through an $ORIGIN rpath.
 """
 from __future__ import annotations
 
@@ -24,6 +25,7 @@ LIB = os.path.join(PKG, "libqld_cuda.so")
 HOST = os.path.join(PKG, "host")
 HOST_LIB = os.path.join(PKG, "libqld_host.so")
 CLI = os.path.join(PKG, "qld-ld")
+VCF2MDF = os.path.join(PKG, "qld-vcf2mdf")
 HOST_FLAGS = ["-O3", "-std=gnu11", "-Wall", "-Wextra", "-Wno-unused-parameter", "-fPIC"]
 
 NVCC_FLAGS = [
@@ -76,22 +78,24 @@ def cc() -> str:
 
 def build_host(force: bool = False) -> str:
     """libqld_host.so and qld-ld (needs libqld_cuda.so first)."""
-    lib_srcs = [os.path.join(HOST, f) for f in ("mdf_loader.c", "report.c")]
-    main = os.path.join(HOST, "qld_ld_main.c")
-    deps = (lib_srcs + [main, LIB] + glob.glob(os.path.join(ROOT, "include", "*.h"))
-            + glob.glob(os.path.join(HOST, "*.h")))
-    if (not force and os.path.exists(HOST_LIB) and os.path.exists(CLI)
-            and all(os.path.getmtime(d) <= min(os.path.getmtime(HOST_LIB), os.path.getmtime(CLI))
-                    for d in deps)):
+    lib_srcs = [os.path.join(HOST, f) for f in ("mdf_loader.c", "report.c", "vcf.c")]
+    mains = {CLI: os.path.join(HOST, "qld_ld_main.c"),
+             VCF2MDF: os.path.join(HOST, "vcf2mdf_main.c")}
+    deps = (lib_srcs + list(mains.values()) + [LIB]
+            + glob.glob(os.path.join(ROOT, "include", "*.h")) + glob.glob(os.path.join(HOST, "*.h")))
+    outs = [HOST_LIB, *mains]
+    if (not force and all(os.path.exists(o) for o in outs)
+            and all(os.path.getmtime(d) <= min(os.path.getmtime(o) for o in outs) for d in deps)):
         return CLI
     inc = ["-I", os.path.join(ROOT, "include")]
     link = ["-L", PKG, "-lqld_cuda", "-Wl,-rpath,$ORIGIN", "-lz", "-lpthread"]
     subprocess.run([cc(), *HOST_FLAGS, *inc, "-shared", "-o", HOST_LIB + ".tmp", *lib_srcs, *link],
                    check=True)
     os.replace(HOST_LIB + ".tmp", HOST_LIB)
-    subprocess.run([cc(), *HOST_FLAGS, *inc, "-o", CLI + ".tmp", main, "-L", PKG, "-lqld_host",
-                    *link], check=True)
-    os.replace(CLI + ".tmp", CLI)
+    for exe, src in mains.items():
+        subprocess.run([cc(), *HOST_FLAGS, *inc, "-o", exe + ".tmp", src, "-L", PKG, "-lqld_host",
+                        *link], check=True)
+        os.replace(exe + ".tmp", exe)
     return CLI
 
 
@@ -101,3 +105,4 @@ if __name__ == "__main__":
     print(LIB)
     print(HOST_LIB)
     print(CLI)
+    print(VCF2MDF)

@@ -61,6 +61,8 @@ struct qld_ctx {
     // and their pinned host mirrors
     DevBuf dMask[2], dHcnt[2], dHoff[2], dHval[2];
     HostBuf hMask[2], hOff[2], hVal[2], hStat;
+    // qld_cuda_vcf_pack
+    DevBuf vText, vSites, vValid, vSlash, vRoff, vRnd, vScratch, vWords, vBc, vLen, vKeep, vErr;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
     size_t prof_used = 0;
     qld_stats stats{};
@@ -401,7 +403,9 @@ int qld_cuda_release(qld_ctx *c) {
     DevBuf *bufs[] = {&c->dA,       &c->dB,       &c->dbcA,     &c->dbcB,     &c->dOut[0],
                       &c->dOut[1],  &c->dCnt[0],  &c->dCnt[1],  &c->dJobs,    &c->dQueue,
                       &c->dMask[0], &c->dMask[1], &c->dHcnt[0], &c->dHcnt[1], &c->dHoff[0],
-                      &c->dHoff[1], &c->dHval[0], &c->dHval[1]};
+                      &c->dHoff[1], &c->dHval[0], &c->dHval[1], &c->vText,    &c->vSites,
+                      &c->vValid,   &c->vSlash,   &c->vRoff,    &c->vRnd,     &c->vScratch,
+                      &c->vWords,   &c->vBc,      &c->vLen,     &c->vKeep,    &c->vErr};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     HostBuf *hbufs[] = {&c->hMask[0], &c->hMask[1], &c->hOff[0], &c->hOff[1],
@@ -696,6 +700,111 @@ int qld_cuda_count_states_device(qld_ctx *c, const uint64_t *A, int m, long long
     Task t{A, nullptr, m, lda, B, nullptr, n, ldb, K, 1, symmetric, 0};
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     return launch_states_range(c, t, 0, n, states, lds, 0, st);
+}
+
+int qld_cuda_vcf_pack(qld_ctx *c, const char *text, size_t text_bytes,
+                      const qld_vcf_site *sites, int nsites, const uint8_t *valid, int nsamples,
+                      int ploidy, int K, qld_rand_fn rng, void *rng_user, uint64_t *words,
+                      uint32_t *bc, int *snip_len, uint8_t *keep, int *err_site) {
+    if (!c) return QLD_ERR_INVALID;
+    if (err_site) *err_site = -1;
+    if (nsites < 0 || nsamples < 1 || ploidy < 1 || K < 1 || (long long)K * 64 > (1LL << 30))
+        return set_err(c, QLD_ERR_INVALID, "bad sizes nsites=%d nsamples=%d ploidy=%d K=%d",
+                       nsites, nsamples, ploidy, K);
+    if (nsites == 0) return QLD_OK;
+    if (!text || !sites || !valid || !words || !bc || !snip_len || !keep)
+        return set_err(c, QLD_ERR_INVALID, "NULL argument");
+    for (int i = 0; i < nsites; ++i) {
+        const qld_vcf_site &v = sites[i];
+        if (v.off < 0 || v.len < 0 || (unsigned long long)v.off + (unsigned)v.len > text_bytes ||
+            v.gt_pos < 0 || v.n_states < 0 || v.n_states > 4)
+            return set_err(c, QLD_ERR_INVALID, "site %d lies outside the text or is malformed", i);
+    }
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const int ctas = nsites < c->sm_count * 8 ? nsites : c->sm_count * 8;
+    const int scratch_cap = K * 64;
+    const size_t ns = (size_t)nsites;
+    int rc;
+    if ((rc = ensure(c, c->vText, text_bytes ? text_bytes : 1)) ||
+        (rc = ensure(c, c->vSites, ns * sizeof(qld_vcf_site))) ||
+        (rc = ensure(c, c->vValid, (size_t)nsamples)) || (rc = ensure(c, c->vSlash, ns * 8)) ||
+        (rc = ensure(c, c->vRoff, ns * 8)) ||
+        (rc = ensure(c, c->vScratch, (size_t)ctas * scratch_cap)) ||
+        (rc = ensure(c, c->vWords, ns * K * 8)) || (rc = ensure(c, c->vBc, ns * 4)) ||
+        (rc = ensure(c, c->vLen, ns * 4)) || (rc = ensure(c, c->vKeep, ns)) ||
+        (rc = ensure(c, c->vErr, ns * 4)))
+        return rc;
+    cudaStream_t st = c->stream;
+    CUDA_TRY(c, cudaMemcpyAsync(c->vText.p, text, text_bytes, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(c, cudaMemcpyAsync(c->vSites.p, sites, ns * sizeof(qld_vcf_site),
+                                cudaMemcpyHostToDevice, st));
+    CUDA_TRY(c, cudaMemcpyAsync(c->vValid.p, valid, (size_t)nsamples, cudaMemcpyHostToDevice, st));
+    const char *dtext = static_cast<const char *>(c->vText.p);
+    const qld_vcf_site *dsites = static_cast<const qld_vcf_site *>(c->vSites.p);
+    const uint8_t *dvalid = static_cast<const uint8_t *>(c->vValid.p);
+    // 1. count: random draws per site
+    cudaError_t e = launch_vcf_sites(dtext, dsites, nsites, dvalid, nsamples, ploidy, K, nullptr,
+                                     nullptr, static_cast<long long *>(c->vSlash.p),
+                                     static_cast<char *>(c->vScratch.p), scratch_cap, ctas,
+                                     static_cast<uint64_t *>(c->vWords.p),
+                                     static_cast<uint32_t *>(c->vBc.p),
+                                     static_cast<int *>(c->vLen.p),
+                                     static_cast<uint8_t *>(c->vKeep.p),
+                                     static_cast<int *>(c->vErr.p), st);
+    if (e != cudaSuccess)
+        return set_err(c, QLD_ERR_CUDA, "VCF count launch failed: %s", cudaGetErrorString(e));
+    std::vector<long long> slash(ns), roff(ns);
+    CUDA_TRY(c, cudaMemcpyAsync(slash.data(), c->vSlash.p, ns * 8, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(c, cudaStreamSynchronize(st));
+    long long total = 0;
+    for (size_t i = 0; i < ns; ++i) {
+        roff[i] = total;
+        total += slash[i] > 0 ? slash[i] : 0;
+    }
+    if (total > 0 && !rng)
+        return set_err(c, QLD_ERR_INVALID,
+                       "unphased genotypes need %lld random draws and no generator was given",
+                       total);
+    std::vector<unsigned> rnd((size_t)(total > 0 ? total : 1));
+    for (long long i = 0; i < total; ++i) rnd[(size_t)i] = rng(rng_user);
+    if ((rc = ensure(c, c->vRnd, rnd.size() * 4))) return rc;
+    CUDA_TRY(c, cudaMemcpyAsync(c->vRnd.p, rnd.data(), rnd.size() * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(c, cudaMemcpyAsync(c->vRoff.p, roff.data(), ns * 8, cudaMemcpyHostToDevice, st));
+    // 2. pack
+    e = launch_vcf_sites(dtext, dsites, nsites, dvalid, nsamples, ploidy, K,
+                         static_cast<const unsigned *>(c->vRnd.p),
+                         static_cast<const long long *>(c->vRoff.p),
+                         static_cast<long long *>(c->vSlash.p), static_cast<char *>(c->vScratch.p),
+                         scratch_cap, ctas, static_cast<uint64_t *>(c->vWords.p),
+                         static_cast<uint32_t *>(c->vBc.p), static_cast<int *>(c->vLen.p),
+                         static_cast<uint8_t *>(c->vKeep.p), static_cast<int *>(c->vErr.p), st);
+    if (e != cudaSuccess)
+        return set_err(c, QLD_ERR_CUDA, "VCF pack launch failed: %s", cudaGetErrorString(e));
+    c->stats.kernel_launches += 2;
+    std::vector<int> err(ns);
+    CUDA_TRY(c, cudaMemcpyAsync(words, c->vWords.p, ns * K * 8, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(c, cudaMemcpyAsync(bc, c->vBc.p, ns * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(c, cudaMemcpyAsync(snip_len, c->vLen.p, ns * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(c, cudaMemcpyAsync(keep, c->vKeep.p, ns, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(c, cudaMemcpyAsync(err.data(), c->vErr.p, ns * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(c, cudaStreamSynchronize(st));
+    static const char *const what[] = {"",
+                                       "empty GT field",
+                                       "allele index past the REF/ALT states",
+                                       "more than three alleles in a genotype",
+                                       "more sample fields than header samples",
+                                       "Detected data bigger than the ploidy of input",
+                                       "a genotype with fewer alleles than separators",
+                                       "no alleles (empty alignment)",
+                                       "a state character qLD cannot map"};
+    for (int i = 0; i < nsites; ++i) {
+        const int code = err[(size_t)i];
+        if (!code) continue;
+        if (err_site) *err_site = i;
+        return set_err(c, QLD_ERR_INVALID, "site %d: %s", i,
+                       code > 0 && code <= 8 ? what[code] : "error");
+    }
+    return QLD_OK;
 }
 
 int qld_cuda_ld_device(qld_ctx *c, const qld_ld_args *a, void *stream) {

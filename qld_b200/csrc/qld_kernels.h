@@ -4,6 +4,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include "qld_cuda.h"
 #include "qld_device.cuh"
 
 namespace qld {
@@ -74,6 +75,29 @@ struct StatesParams {
 extern const KernelShape kStatesShape;
 cudaError_t launch_states(const CUtensorMap &tmA, const CUtensorMap &tmB, const StatesParams &p,
                           int tiles_b, cudaStream_t st);
+
+// VCF sites -> packed rows (vcf_pack.cu).  With rnd_off NULL the launch only
+// counts: per site the random draws its unphased genotypes need
+// (slash_count), its row length and count-stage errors.  Otherwise it packs,
+// drawing site s's numbers from rnd[rnd_off[s]...].  Each CTA uses
+// scratch_cap bytes of scratch (>= K * 64).
+enum VcfError {
+    QLD_VCF_OK = 0,
+    QLD_VCF_EMPTY_GT = 1,     // the GT subfield is empty
+    QLD_VCF_ALLELE = 2,       // an allele index past the REF/ALT states
+    QLD_VCF_ALLELES = 3,      // more than three alleles in a genotype
+    QLD_VCF_SAMPLES = 4,      // more sample fields than header samples
+    QLD_VCF_PLOIDY = 5,       // a genotype bigger than the ploidy
+    QLD_VCF_SHORT_GT = 6,     // fewer alleles than the genotype's separators say
+    QLD_VCF_NO_SAMPLES = 7,   // no alleles at all
+    QLD_VCF_STATE_CHAR = 8,   // a REF/ALT character qLD cannot map (lower case, '.')
+};
+cudaError_t launch_vcf_sites(const char *text, const qld_vcf_site *sites, int nsites,
+                             const uint8_t *valid, int nsamples, int ploidy, int K,
+                             const unsigned *rnd, const long long *rnd_off,
+                             long long *slash_count, char *scratch, int scratch_cap, int ctas,
+                             uint64_t *words, uint32_t *bc, int *snip_len, uint8_t *keep,
+                             int *err, cudaStream_t st);
 
 // Report filter over `rows` r^2 rows (ldr >= m rounded up to 128 floats,
 // 16-byte aligned rows): mask (rows x W words, W = ceil(m / 32)), per-row

@@ -7,8 +7,10 @@
  * file order with their BC field and the first K words (readTable_x64 /
  * writeMDF_x64, correlate_IOx64.c:27-122,351-461) -- but parts are parsed in
  * parallel by worker threads with a hand-written decimal parser instead of
- * strtoul, malformed input returns a status instead of exiting, and words
- * past K on a line must be zero (qLD copies them past the row).
+ * strtoul and malformed input returns a status instead of exiting.  Words
+ * past K on a line are read and ignored: qLD-parse-2MDF pads haploid data to
+ * its diploid default width with words it never initialises, and qLD-compute
+ * copies them past the row, where the next row overwrites them.
  */
 #define _GNU_SOURCE
 #include <dirent.h>
@@ -296,11 +298,6 @@ static int parse_part(part *p, int K, int pos_min, int pos_max)
                         }
                         if (k < K)
                             w[k] = v;
-                        else if (v != 0) {
-                            free(text);
-                            return part_fail(p, "%s line %d: nonzero word %d past the %d the "
-                                                "samples need", p->path, ln + 1, k, K);
-                        }
                         ++k;
                     }
                     if (k < K) {

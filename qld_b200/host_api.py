@@ -248,3 +248,137 @@ def write_states_report(path: str, A: Table, B: Table, states: np.ndarray,
         if libc.fclose(fp) != 0:
             raise OSError(f"cannot close {path}")
     _check(rc)
+
+
+# ------------------------------------------------------------- VCF -> MDF --
+
+class _VcfHeader(ct.Structure):
+    _fields_ = [("id", ct.c_char * 256), ("path", ct.c_char * 4096), ("line1", ct.c_char_p),
+                ("line2", ct.c_char_p), ("nsamples", ct.c_int), ("valid", ct.POINTER(ct.c_uint8)),
+                ("valid_count", ct.c_int), ("snips_per_file", ct.c_int), ("snip_size", ct.c_int),
+                ("total_snips", ct.c_int)]
+
+
+class _VcfPart(ct.Structure):
+    _fields_ = [("text", ct.c_void_p), ("bytes", ct.c_size_t), ("pinned", ct.c_int),
+                ("lines", ct.c_int), ("skipped", ct.c_int), ("nsites", ct.c_int),
+                ("sites", ct.c_void_p), ("pos", ct.POINTER(ct.c_uint32)),
+                ("ids", ct.POINTER(ct.c_size_t)), ("id_pool", ct.c_void_p)]
+
+
+# one qld_vcf_site record (include/qld_cuda.h)
+VCF_SITE = np.dtype([("off", np.int64), ("len", np.int32), ("gt_pos", np.int32),
+                     ("n_states", np.int32), ("states", "S4")], align=True)
+
+
+def _vcf_lib() -> ct.CDLL:
+    L = lib()
+    if not hasattr(L, "_vcf_bound"):
+        L.qld_vcf_read_header.argtypes = [ct.c_char_p, ct.c_int, ct.POINTER(ct.c_char_p), ct.c_int,
+                                          ct.POINTER(_VcfHeader)]
+        L.qld_vcf_read_header.restype = ct.c_int
+        L.qld_vcf_header_free.argtypes = [ct.POINTER(_VcfHeader)]
+        L.qld_vcf_header_free.restype = None
+        L.qld_vcf_list_parts.argtypes = [ct.c_char_p, ct.POINTER(_VcfHeader),
+                                         ct.POINTER(ct.POINTER(ct.c_char_p)), ct.POINTER(ct.c_int)]
+        L.qld_vcf_list_parts.restype = ct.c_int
+        L.qld_vcf_list_free.argtypes = [ct.POINTER(ct.c_char_p), ct.c_int]
+        L.qld_vcf_list_free.restype = None
+        L.qld_vcf_load_part.argtypes = [ct.c_void_p, ct.c_char_p, ct.POINTER(_VcfHeader),
+                                        ct.POINTER(_VcfPart)]
+        L.qld_vcf_load_part.restype = ct.c_int
+        L.qld_vcf_part_free.argtypes = [ct.c_void_p, ct.POINTER(_VcfPart)]
+        L.qld_vcf_part_free.restype = None
+        L.qld_vcf_site_id.argtypes = [ct.POINTER(_VcfPart), ct.c_int]
+        L.qld_vcf_site_id.restype = ct.c_char_p
+        L.qld_mdf_part_path.argtypes = [ct.c_char_p, ct.c_char_p, ct.c_char_p, ct.c_size_t]
+        L.qld_mdf_part_path.restype = ct.c_int
+        L.qld_mdf_write_part.argtypes = [ct.c_char_p, ct.c_char_p, ct.POINTER(_VcfPart), ct.c_int,
+                                         ct.c_void_p, ct.c_void_p, ct.c_void_p]
+        L.qld_mdf_write_part.restype = ct.c_int
+        L._vcf_bound = True
+    return L
+
+
+class VcfHeader:
+    """A qLD-parse-VCF dataset's header (qld_vcf_read_header)."""
+
+    def __init__(self, path: str, ploidy: int, sample_list=None):
+        names = list(sample_list or [])
+        arr = (ct.c_char_p * max(len(names), 1))(*[n.encode() for n in names])
+        self._h = _VcfHeader()
+        _check(_vcf_lib().qld_vcf_read_header(os.fsencode(path), int(ploidy), arr, len(names),
+                                              ct.byref(self._h)))
+        h = self._h
+        self.id = h.id.decode()
+        self.path = h.path.decode()
+        self.nsamples = h.nsamples
+        self.valid = np.ctypeslib.as_array(h.valid, (h.nsamples,)).copy()
+        self.valid_count = h.valid_count
+        self.K = (h.valid_count + 63) // 64
+        self.snip_size = h.snip_size
+
+    def parts(self, path: str) -> list[str]:
+        pp = ct.POINTER(ct.c_char_p)()
+        n = ct.c_int()
+        _check(_vcf_lib().qld_vcf_list_parts(os.fsencode(path), ct.byref(self._h), ct.byref(pp),
+                                             ct.byref(n)))
+        out = [pp[i].decode() for i in range(n.value)]
+        _vcf_lib().qld_vcf_list_free(pp, n.value)
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _vcf_lib().qld_vcf_header_free(ct.byref(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class VcfPart:
+    """One part file read and filtered on its fixed fields (qld_vcf_load_part)."""
+
+    def __init__(self, path: str, header: VcfHeader):
+        self.path = path
+        self._p = _VcfPart()
+        _check(_vcf_lib().qld_vcf_load_part(None, os.fsencode(path), ct.byref(header._h),
+                                            ct.byref(self._p)))
+        p = self._p
+        self.text = ct.string_at(p.text, p.bytes)
+        self.lines, self.skipped, self.nsites = p.lines, p.skipped, p.nsites
+        n = p.nsites
+        self.sites = (np.frombuffer(ct.string_at(p.sites, n * VCF_SITE.itemsize), VCF_SITE).copy()
+                      if n else np.zeros(0, VCF_SITE))
+        self.pos = np.ctypeslib.as_array(p.pos, (n,)).copy() if n else np.zeros(0, np.uint32)
+        self.ids = [_vcf_lib().qld_vcf_site_id(ct.byref(p), i).decode() for i in range(n)]
+
+    def write_mdf(self, out_dir: str, header: VcfHeader, words, bc, keep) -> str:
+        """The part's MDF file in out_dir (qld_mdf_write_part); returns its path."""
+        buf = ct.create_string_buffer(8192)
+        _check(_vcf_lib().qld_mdf_part_path(os.fsencode(out_dir), os.fsencode(self.path), buf,
+                                            8192))
+        words = np.ascontiguousarray(words, np.uint64)
+        bc = np.ascontiguousarray(bc, np.uint32)
+        keep = np.ascontiguousarray(keep, np.uint8)
+        _check(_vcf_lib().qld_mdf_write_part(buf.value, header.id.encode(), ct.byref(self._p),
+                                             int(header.K), words.ctypes.data, bc.ctypes.data,
+                                             keep.ctypes.data))
+        return buf.value.decode()
+
+    def close(self):
+        if getattr(self, "_p", None) is not None:
+            _vcf_lib().qld_vcf_part_free(None, ct.byref(self._p))
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+VCF2MDF_PATH = os.path.join(_PKG, "qld-vcf2mdf")

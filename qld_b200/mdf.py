@@ -114,9 +114,7 @@ def read_region(path: str, pos_min=None, pos_max=None):
                     continue
                 pos = int(fields[1])
                 if pos_min <= pos <= pos_max:
-                    words = [int(w) for w in fields[4:4 + K]]
-                    if any(int(w) for w in fields[4 + K:]):
-                        raise ValueError(f"{fn}: nonzero words past the {K} the samples need")
+                    words = [int(w) for w in fields[4:4 + K]]   # words past K: ignored
                     rows.append(words + [0] * (K - len(words)))
                     bcs.append(int(fields[3]))
                     poss.append(pos)
