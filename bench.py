@@ -1,7 +1,7 @@
 """Benchmark of the LD hot path (AND+popcount counts + fused r^2) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload single_region|all_pairs] [--kernel auto|popc|mma]
+                    [--workload single_region|all_pairs] [--kernel auto|popc|mma|fp4]
 
 Workload (default): the dataset-shaped single region -- 29,817 SNPs x 16,622
 haploid sequences (K = 260 words per SNP), allele frequencies Beta(0.1, 1)
@@ -53,7 +53,7 @@ def parse():
                     help="served workload: offered load as a fraction of measured capacity")
     ap.add_argument("--band", type=int, default=5000, help="windowed workload: band width")
     ap.add_argument("--jobs", type=int, default=4096, help="batched workload: number of tasks")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma", "fp4"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mma-tile", type=int, default=0, choices=[0, 128, 256],
@@ -156,12 +156,46 @@ class ClockSampler:
                 "window": "timed region" if inside else "whole run (no sample inside the region)"}
 
 
+def kernel_roofline(ctx, variant, bitops, kern_ms, dev):
+    """Roofline of the counts kernel against the measured rate of the pipe it
+    runs on: the tensor pipe of its MMA kind (qld_cuda_measure_mma_peak,
+    2 ops per bit-pair), or the popcount pipe (1 bit-op per bit-pair)."""
+    if variant in (api.KERNEL_MMA, api.KERNEL_FP4):
+        peak = ctx.measure_mma_peak(variant) / 1e12
+        achieved = 2 * bitops / (kern_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak,
+                "unit": "TFLOPS (E2M1 dense)" if variant == api.KERNEL_FP4 else "TOPS (int8)",
+                "frac": achieved / peak,
+                "peak_source": "measured: qld_cuda_measure_mma_peak, back-to-back 128x256 "
+                               + ("kind::mxf4 MMAs (K=64)" if variant == api.KERNEL_FP4
+                                  else "kind::i8 MMAs (K=32)") + ", one CTA per SM"}
+        # for context: the int8 rate a library GEMM reaches on this GPU
+        a = torch.randint(-2, 2, (8192, 8192), dtype=torch.int8, device=dev)
+        b = torch.randint(-2, 2, (8192, 8192), dtype=torch.int8, device=dev).t()
+        for _ in range(3):
+            torch._int_mm(a, b)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            torch._int_mm(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        roof["int8_gemm_torch_tops"] = 2 * 8192 ** 3 * 10 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+        return roof
+    popc_peak = ctx.measure_popc_peak() / 1e12
+    achieved = bitops / (kern_ms * 1e-3) / 1e12
+    return {"bound": "popc", "achieved": achieved, "peak": popc_peak, "unit": "Tbit-op/s",
+            "frac": achieved / popc_peak,
+            "peak_source": "measured: qld_cuda_measure_popc_peak (register-only AND+POPC)"}
+
+
 def measured_traffic(variant, workload):
     """DRAM bytes per launch of the counts kernel from the ncu capture
     summarised under profiles/ (None when no capture covers this case)."""
-    if variant != 2 or workload != "single_region_29817x16622_lower_triangle":
+    names = {2: "k_ld_mma_wide_traffic_16384.md", 3: "k_ld_mxf4_traffic_16384.md"}
+    if variant not in names or workload != "single_region_29817x16622_lower_triangle":
         return None
-    path = os.path.join(ROOT, "profiles", "k_ld_mma_wide_traffic_16384.md")
+    path = os.path.join(ROOT, "profiles", names[variant])
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch_full:"):
@@ -269,7 +303,8 @@ def ours_arm(args, rank, world, local_rank):
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
 
     ctx = api.Context(local_rank)
-    kern = {"auto": api.KERNEL_AUTO, "popc": api.KERNEL_POPC, "mma": api.KERNEL_MMA}[args.kernel]
+    kern = {"auto": api.KERNEL_AUTO, "popc": api.KERNEL_POPC, "mma": api.KERNEL_MMA,
+            "fp4": api.KERNEL_FP4}[args.kernel]
     ctx.set_option(api.OPT_KERNEL, kern)
     ctx.set_option(api.OPT_MMA_TILE, args.mma_tile)
     ctx.set_option(api.OPT_PROFILE, 1)
@@ -322,27 +357,7 @@ def ours_arm(args, rank, world, local_rank):
     kern_ms = stats.counts_kernel_ms / max(1, stats.counts_launches)
     bitops = pairs * 64 * K
     variant = stats.last_kernel
-    popc_peak = ctx.measure_popc_peak()
-    if variant == api.KERNEL_MMA:
-        a = torch.randint(-2, 2, (8192, 8192), dtype=torch.int8, device=dev)
-        b = torch.randint(-2, 2, (8192, 8192), dtype=torch.int8, device=dev).t()
-        for _ in range(3):
-            torch._int_mm(a, b)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(10):
-            torch._int_mm(a, b)
-        e1.record()
-        torch.cuda.synchronize()
-        i8_tops = 2 * 8192 ** 3 * 10 / (e0.elapsed_time(e1) * 1e-3) / 1e12
-        achieved = 2 * bitops / (kern_ms * 1e-3) / 1e12
-        roof = {"bound": "tensor", "achieved": achieved, "peak": i8_tops, "unit": "TOPS (int8)",
-                "frac": achieved / i8_tops, "peak_source": "measured: torch._int_mm int8 8192^3"}
-    else:
-        achieved = bitops / (kern_ms * 1e-3) / 1e12
-        roof = {"bound": "popc", "achieved": achieved, "peak": popc_peak / 1e12,
-                "unit": "Tbit-op/s", "frac": achieved / (popc_peak / 1e12),
-                "peak_source": "measured: qld_cuda_measure_popc_peak (register-only AND+POPC)"}
+    roof = kernel_roofline(ctx, variant, bitops, kern_ms, dev)
     alg_bytes = m * K * 8 * 2 + pairs * 4
     roof["traffic"] = measured_traffic(variant, cfg["workload"])
     roof["algorithmic_bytes_per_launch"] = alg_bytes
@@ -507,7 +522,8 @@ def windowed_arm(args, rank, world, local_rank):
     pairs = sum(min(W, m - 1 - i) for i in range(0, m)) if m < 50_000 else \
         W * (m - W) + W * (W - 1) // 2
     ctx = api.Context(local_rank)
-    kern = {"auto": api.KERNEL_AUTO, "popc": api.KERNEL_POPC, "mma": api.KERNEL_MMA}[args.kernel]
+    kern = {"auto": api.KERNEL_AUTO, "popc": api.KERNEL_POPC, "mma": api.KERNEL_MMA,
+            "fp4": api.KERNEL_FP4}[args.kernel]
     ctx.set_option(api.OPT_KERNEL, kern)
     ctx.set_option(api.OPT_MMA_TILE, args.mma_tile)
     ctx.set_option(api.OPT_PROFILE, 1)
@@ -549,8 +565,8 @@ def windowed_arm(args, rank, world, local_rank):
             "bitops_per_s": bitops * args.steps / (total_ms * 1e-3),
             "gpu_launches": stats.kernel_launches // max(1, args.steps),
             "kernel_variant": stats.last_kernel,
-            "roofline": {"bound": "tensor", "achieved": 2 * bitops / (kern_ms * 1e-3) / 1e12,
-                         "unit": "TOPS (int8)", "kernel_ms": kern_ms},
+            "roofline": dict(kernel_roofline(ctx, stats.last_kernel, bitops, kern_ms, dev),
+                             kernel_ms=kern_ms),
             "clocks": clk.summary()}
     if not args.no_e2e:
         Th = ctx.pinned_empty((m, K), np.uint64)

@@ -64,6 +64,7 @@ extern "C" {
 #define QLD_KERNEL_AUTO   0  /* per-shape choice                                 */
 #define QLD_KERNEL_POPC   1  /* LOP3 + POPC on the CUDA cores                     */
 #define QLD_KERNEL_MMA    2  /* bit -> int8 unpack + tcgen05 i8 MMA (TMEM)        */
+#define QLD_KERNEL_FP4    3  /* bit -> E2M1 unpack + tcgen05 block-scaled MXF4 MMA */
 
 /* qld_cuda_set_option() keys */
 #define QLD_OPT_KERNEL    1  /* QLD_KERNEL_*                                      */
@@ -323,6 +324,11 @@ int qld_cuda_ld_noalloc(const uint64_t *A, const uint32_t *bcA, int m,
  * QLD_KERNEL_POPC variant.  Runs a register-only kernel for ~0.1 s.
  * No counterpart in the reference (its roofline is not measured). */
 int qld_cuda_measure_popc_peak(qld_ctx *ctx, double *bitops_per_s);
+/* The tensor pipe's dense rate for kernel QLD_KERNEL_MMA (kind::i8) or
+ * QLD_KERNEL_FP4 (kind::mxf4) in operations (2 per multiply-accumulate) per
+ * second: back-to-back 128 x 256 MMAs on a fixed tile, one CTA per SM.  The
+ * denominator of those kernels' roofline.  Runs ~10 ms. */
+int qld_cuda_measure_mma_peak(qld_ctx *ctx, int kernel, double *ops_per_s);
 
 #ifdef __cplusplus
 }

@@ -26,7 +26,7 @@ OK = 0
 ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NODEVICE, ERR_TIMEOUT, ERR_BUSY, ERR_UNSUPPORTED = (
     -1, -2, -3, -4, -5, -6, -7)
 R2_EXACT, R2_REFERENCE = 0, 1
-KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA = 0, 1, 2
+KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA, KERNEL_FP4 = 0, 1, 2, 3
 OPT_KERNEL, OPT_R2_MODE, OPT_PROFILE, OPT_BAND_ROWS, OPT_MMA_TILE = 1, 2, 3, 4, 5
 
 EXPORTED = (
@@ -37,6 +37,7 @@ EXPORTED = (
     "qld_cuda_ld_band_device", "qld_cuda_sync",
     "qld_cuda_host_alloc",
     "qld_cuda_host_free", "qld_cuda_get_stats", "qld_cuda_measure_popc_peak",
+    "qld_cuda_measure_mma_peak",
     "qld_srv_create", "qld_srv_add_table", "qld_srv_submit", "qld_srv_poll", "qld_srv_fetch",
     "qld_srv_release", "qld_srv_destroy", "qld_srv_last_error",
 )
@@ -128,6 +129,7 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.qld_cuda_host_free.argtypes = [vp, vp]
     lib.qld_cuda_get_stats.argtypes = [vp, ct.POINTER(_Stats), i]
     lib.qld_cuda_measure_popc_peak.argtypes = [vp, ct.POINTER(ct.c_double)]
+    lib.qld_cuda_measure_mma_peak.argtypes = [vp, i, ct.POINTER(ct.c_double)]
     lib.qld_srv_create.argtypes = [i, ct.c_size_t, i, ct.POINTER(vp)]
     lib.qld_srv_add_table.argtypes = [vp, vp, vp, i, i, i, ct.POINTER(i)]
     lib.qld_srv_submit.argtypes = [vp, ct.POINTER(_Query), ct.POINTER(ll)]
@@ -199,6 +201,13 @@ class Context:
         """Measured popcount-pipe peak in bit-ops/s."""
         v = ct.c_double()
         self._check(self.lib.qld_cuda_measure_popc_peak(self.h, ct.byref(v)))
+        return v.value
+
+    def measure_mma_peak(self, kernel: int) -> float:
+        """Measured dense tensor-pipe rate in ops/s (2 per multiply-accumulate)
+        for KERNEL_MMA (kind::i8) or KERNEL_FP4 (kind::mxf4)."""
+        v = ct.c_double()
+        self._check(self.lib.qld_cuda_measure_mma_peak(self.h, int(kernel), ct.byref(v)))
         return v.value
 
     # -------------------------------------------------------------- host --

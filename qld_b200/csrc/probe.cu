@@ -66,3 +66,121 @@ extern "C" int qld_cuda_measure_popc_peak(qld_ctx *ctx, double *bitops_per_s) {
     cudaFree(d);
     return rc;
 }
+
+// ---------------------------------------------------------------- MMA peak --
+//
+// Self-measurement of the tensor pipe for the two MMA kinds the counts
+// kernels issue: one CTA per SM, one thread issuing back-to-back 128 x 256
+// MMAs (kind::i8, K = 32; kind::mxf4, K = 64 with 1.0 scale factors) on a
+// fixed shared-memory tile into one TMEM accumulator, as the kernels do, with
+// no unpack and no epilogue.  The wait for the last MMA is bounded.
+#include "qld_device.cuh"
+#include "tcgen05.cuh"
+
+namespace {
+
+using namespace qld;
+using namespace qld::tc;
+
+template <int KIND>   // 0: kind::i8, 1: kind::mxf4
+__global__ void __launch_bounds__(128, 1)
+k_mma_peak(int iters, unsigned *status, long long timeout) {
+    extern __shared__ uint8_t raw[];
+    uint8_t *sm = reinterpret_cast<uint8_t *>(
+        (reinterpret_cast<uintptr_t>(raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + 49152);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(sm + 49152 + 16);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    // operands: a fixed, non-zero pattern (every E2M1 code is finite)
+    for (int i = tid; i < 49152 / 4; i += 128)
+        reinterpret_cast<uint32_t *>(sm)[i] = 0x9E3779B9u * (uint32_t)(i + 1);
+    if (tid == 0) {
+        mbar_init(smem_u32(bar), 1);
+        fence_barrier_init();
+    }
+    fence_proxy_async_smem();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(slot)),
+                     "r"(512)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+    if (KIND == 1)   // scale factors 1.0 at columns 256-271, one lane quarter per warp
+        tc_st_32x32b_x16_fill(tmem + ((uint32_t)(warp * 32) << 16) + 256, 0x7F7F7F7Fu);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+        const uint32_t a0 = smem_u32(sm), b0 = smem_u32(sm + 16384);
+        for (int i = 0; i < iters; ++i)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const uint32_t acc = (i > 0 || kk > 0) ? 1u : 0u;
+                if (KIND == 0)
+                    tc_mma_i8(tmem, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32),
+                              idesc_i8(128, 256), acc);
+                else
+                    tc_mma_mxf4(tmem, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32),
+                                idesc_mxf4(128, 256), acc, tmem + 256, tmem + 256);
+            }
+        tc_commit(smem_u32(bar));
+        if (!mbar_wait(smem_u32(bar), 0, timeout, status)) flag_error(status, ST_TIMEOUT_MMA);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512)
+                     : "memory");
+    }
+}
+
+}  // namespace
+
+extern "C" int qld_cuda_measure_mma_peak(qld_ctx *ctx, int kernel, double *ops_per_s) {
+    if (!ctx || !ops_per_s || (kernel != QLD_KERNEL_MMA && kernel != QLD_KERNEL_FP4))
+        return QLD_ERR_INVALID;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return QLD_ERR_CUDA;
+    unsigned *status = nullptr;
+    if (cudaMalloc(&status, sizeof(unsigned)) != cudaSuccess) return QLD_ERR_NOMEM;
+    cudaMemset(status, 0, sizeof(unsigned));
+    const int smem = 49152 + 64 + 1024, iters = 4096;
+    auto kern = kernel == QLD_KERNEL_FP4 ? k_mma_peak<1> : k_mma_peak<0>;
+    int rc = QLD_OK;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        cudaSuccess)
+        rc = QLD_ERR_CUDA;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 4 && rc == QLD_OK; ++rep) {
+        cudaEventRecord(e0);
+        kern<<<sms, 128, smem>>>(iters, status, 4000000000LL);
+        cudaEventRecord(e1);
+        if (cudaEventSynchronize(e1) != cudaSuccess) { rc = QLD_ERR_CUDA; break; }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && ms < best) best = ms;
+    }
+    unsigned st = 0;
+    if (rc == QLD_OK && cudaMemcpy(&st, status, sizeof st, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = QLD_ERR_CUDA;
+    if (rc == QLD_OK && st) rc = QLD_ERR_TIMEOUT;
+    if (rc == QLD_OK) {
+        const double k = kernel == QLD_KERNEL_FP4 ? 64.0 : 32.0;
+        *ops_per_s = 2.0 * 128 * 256 * k * 4.0 * iters * sms / (best * 1e-3);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(status);
+    return rc;
+}

@@ -150,16 +150,20 @@ struct Task {
 };
 
 bool mma_exact_for(const Task &t) { return (long long)t.K * 64 <= kMmaMaxSamples; }
+bool fp4_exact_for(const Task &t) { return (long long)t.K * 64 <= kMxf4MaxSamples; }
 
-// Per-shape variant: the tensor-core kernel wherever its s32 accumulators
-// stay exact, the popcount kernel otherwise.
+// Per-shape variant: the 4-bit tensor-core kernel wherever its F32
+// accumulators stay exact (K * 64 <= 2^24 samples: measured faster than the
+// i8 kernels on large and small tasks alike), the popcount kernel otherwise.
 int choose_kernel(qld_ctx *c, const Task &t) {
     (void)c;
-    return mma_exact_for(t) ? QLD_KERNEL_MMA : QLD_KERNEL_POPC;
+    return fp4_exact_for(t) ? QLD_KERNEL_FP4 : QLD_KERNEL_POPC;
 }
 
 long long tile_count(const Task &t, int bm, int bn, int b0, int b1) {
     const int tb0 = b0 / bn, tiles_b = (b1 - b0 + bn - 1) / bn;
+    if (bm == 256 && bn == 240)
+        return tc::TileList<256, 240>{(t.m + 255) / 256, tb0, tiles_b, t.symmetric, t.band}.count();
     if (bm == 256 && bn == 256)
         return tc::TileList<256, 256>{(t.m + 255) / 256, tb0, tiles_b, t.symmetric, t.band}.count();
     if (bm == 128 && bn == 256)
@@ -177,7 +181,20 @@ const KernelShape &mma_shape(qld_ctx *c, const Task &t, int b0, int b1) {
 }
 
 const KernelShape &shape_of(qld_ctx *c, int variant, const Task &t, int b0, int b1) {
+    if (variant == QLD_KERNEL_FP4) return kMxf4Shape;
     return variant == QLD_KERNEL_MMA ? mma_shape(c, t, b0, b1) : kPopcShape;
+}
+
+int variant_of(qld_ctx *c, const Task &t) {
+    return c->kernel == QLD_KERNEL_AUTO ? choose_kernel(c, t) : c->kernel;
+}
+
+// B rows per streamed band: the context's band size rounded down to whole
+// tile rows of the task's kernel (240 for the 4-bit kernel, else 256).
+int band_rows_for(qld_ctx *c, const Task &t) {
+    const int unit = variant_of(c, t) == QLD_KERNEL_FP4 ? kMxf4Shape.bn : 256;
+    const int b = c->band_rows / unit * unit;
+    return b > unit ? b : unit;
 }
 
 // With QLD_OPT_PROFILE: an event pair around the next launch on `st`
@@ -197,14 +214,19 @@ int prof_begin(qld_ctx *c, cudaStream_t st, cudaEvent_t *end) {
     return QLD_OK;
 }
 
-// Launch the counts kernel over B rows [b0, b1) (b0 a multiple of 256),
-// writing r2/counts rows relative to out_row0.
+// Launch the counts kernel over B rows [b0, b1) (b0 a multiple of the
+// kernel's tile rows: band_rows_for), writing r2/counts rows relative to
+// out_row0.
 int launch_counts(qld_ctx *c, const Task &t, int b0, int b1, float *r2, long long ldr,
                   uint32_t *cnt, long long ldc, int out_row0, cudaStream_t st) {
-    const int variant = c->kernel == QLD_KERNEL_AUTO ? choose_kernel(c, t) : c->kernel;
+    const int variant = variant_of(c, t);
     if (variant == QLD_KERNEL_MMA && !mma_exact_for(t))
         return set_err(c, QLD_ERR_UNSUPPORTED,
                        "tensor-core kernel needs K*64 <= %d samples (K=%d)", kMmaMaxSamples, t.K);
+    if (variant == QLD_KERNEL_FP4 && !fp4_exact_for(t))
+        return set_err(c, QLD_ERR_UNSUPPORTED,
+                       "4-bit tensor-core kernel needs K*64 <= %d samples (K=%d)",
+                       kMxf4MaxSamples, t.K);
     const KernelShape &ks = shape_of(c, variant, t, b0, b1);
     CUtensorMap tmA, tmB;
     int rc;
@@ -235,9 +257,10 @@ int launch_counts(qld_ctx *c, const Task &t, int b0, int b1, float *r2, long lon
         cudaEvent_t e1 = nullptr;
         if (int rc = prof_begin(c, st, &e1)) return rc;
         cudaError_t e =
-            variant != QLD_KERNEL_MMA ? launch_popc(tmA, tmB, p, nb, c->r2_mode, st)
-            : &ks == &kMmaWideShape   ? launch_mma_wide(tmA, tmB, p, nb, c->r2_mode, st)
-                                      : launch_mma(tmA, tmB, p, nb, c->r2_mode, st);
+            variant == QLD_KERNEL_FP4 ? launch_mxf4(tmA, tmB, p, nb, c->r2_mode, st)
+            : variant != QLD_KERNEL_MMA ? launch_popc(tmA, tmB, p, nb, c->r2_mode, st)
+            : &ks == &kMmaWideShape     ? launch_mma_wide(tmA, tmB, p, nb, c->r2_mode, st)
+                                        : launch_mma(tmA, tmB, p, nb, c->r2_mode, st);
         if (e != cudaSuccess)
             return set_err(c, QLD_ERR_CUDA, "counts kernel launch failed: %s", cudaGetErrorString(e));
         if (e1) CUDA_TRY(c, cudaEventRecord(e1, st));
@@ -435,7 +458,7 @@ int qld_cuda_set_option(qld_ctx *c, int option, long long value) {
     if (!c) return QLD_ERR_INVALID;
     switch (option) {
     case QLD_OPT_KERNEL:
-        if (value < QLD_KERNEL_AUTO || value > QLD_KERNEL_MMA)
+        if (value < QLD_KERNEL_AUTO || value > QLD_KERNEL_FP4)
             return set_err(c, QLD_ERR_INVALID, "bad kernel variant %lld", value);
         c->kernel = (int)value;
         return QLD_OK;
@@ -505,7 +528,7 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
     int rc;
     if ((rc = stage_tables(c, A, bcA, m, B, bcB, n, K, S, symmetric, &t))) return rc;
 
-    const int band = c->band_rows;  // multiple of 256: whole tile rows of every variant
+    const int band = band_rows_for(c, t);   // whole tile rows of the task's kernel
     const int nbands = (n + band - 1) / band;
     const size_t slot_rows = (size_t)(n < band ? n : band);
     for (int s = 0; s < 2 && s < nbands; ++s) {
@@ -565,8 +588,9 @@ int qld_cuda_ld_hits(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m,
     int rc;
     if ((rc = stage_tables(c, A, bcA, m, B, bcB, n, K, S, symmetric, &t))) return rc;
 
-    const int rows_blk = n < c->band_rows ? n : c->band_rows;
-    const int nblk = (n + c->band_rows - 1) / c->band_rows;
+    const int BR = band_rows_for(c, t);      // whole tile rows of the task's kernel
+    const int rows_blk = n < BR ? n : BR;
+    const int nblk = (n + BR - 1) / BR;
     const long long ldr = ((long long)m + 127) / 128 * 128;   // float4 groups of 128 columns
     const int W = (m + 31) / 32;
     for (int s = 0; s < 2 && s < nblk; ++s) {
@@ -586,7 +610,7 @@ int qld_cuda_ld_hits(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m,
     // the offsets, the mask and the status word to the host.
     auto issue = [&](int bi) -> int {
         const int s = bi & 1;
-        const int b0 = bi * c->band_rows, b1 = b0 + c->band_rows < n ? b0 + c->band_rows : n;
+        const int b0 = bi * BR, b1 = b0 + BR < n ? b0 + BR : n;
         float *r2s = static_cast<float *>(c->dOut[s].p);
         int rc2;
         if ((rc2 = launch_counts(c, t, b0, b1, r2s, ldr, nullptr, 0, b0, c->stream))) return rc2;
@@ -612,7 +636,7 @@ int qld_cuda_ld_hits(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m,
     // Wait for block bi's offsets and mask, fetch its values, call fn.
     auto consume = [&](int bi) -> int {
         const int s = bi & 1;
-        const int b0 = bi * c->band_rows, b1 = b0 + c->band_rows < n ? b0 + c->band_rows : n;
+        const int b0 = bi * BR, b1 = b0 + BR < n ? b0 + BR : n;
         CUDA_TRY(c, cudaEventSynchronize(c->ev_copy[s]));
         if (hstat[s]) return QLD_ERR_TIMEOUT;
         const long long *off = static_cast<const long long *>(c->hOff[s].p);
@@ -854,7 +878,9 @@ int qld_cuda_ld_band(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, 
     if ((rc = ensure(c, c->dA, (size_t)m * Kp * 8)) || (rc = ensure(c, c->dbcA, (size_t)m * 4)))
         return rc;
     uint64_t *dA = static_cast<uint64_t *>(c->dA.p);
-    const int rows_blk = c->band_rows;                       // multiple of 256
+    Task t{dA, static_cast<const uint32_t *>(c->dbcA.p), m, Kp, dA,
+           static_cast<const uint32_t *>(c->dbcA.p), m, Kp, K, S, 1, band};
+    const int rows_blk = band_rows_for(c, t);                // whole tile rows of the kernel
     const int nblk = (m + rows_blk - 1) / rows_blk;
     for (int s = 0; s < 2 && s < nblk; ++s) {
         if ((rc = ensure(c, c->dOut[s], (size_t)rows_blk * band * 4))) return rc;
@@ -874,8 +900,6 @@ int qld_cuda_ld_band(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, 
                                       cudaMemcpyHostToDevice, c->h2d));
         CUDA_TRY(c, cudaEventRecord(c->h2d_ev[i], c->h2d));
     }
-    Task t{dA, static_cast<const uint32_t *>(c->dbcA.p), m, Kp, dA,
-           static_cast<const uint32_t *>(c->dbcA.p), m, Kp, K, S, 1, band};
     for (int bi = 0; bi < nblk; ++bi) {
         const int s = bi & 1;
         const int b0 = bi * rows_blk, b1 = b0 + rows_blk < m ? b0 + rows_blk : m;

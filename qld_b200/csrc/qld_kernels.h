@@ -35,6 +35,13 @@ cudaError_t launch_mma(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdP
 cudaError_t launch_mma_wide(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
                             int tiles_b, int r2_mode, cudaStream_t st);
 
+// Variant (c): bits as E2M1 on tcgen05.mma.kind::mxf4 with F32 accumulators,
+// 256 x 240 tiles.  Exact while K * 64 <= kMxf4MaxSamples.
+extern const KernelShape kMxf4Shape;
+extern const int kMxf4MaxSamples;
+cudaError_t launch_mxf4(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
+                        int tiles_b, int r2_mode, cudaStream_t st);
+
 // One task of a batched launch: its tensor maps (kBatchShape boxes), sizes,
 // output, and the number of work items (output tiles) of the tasks before it.
 struct BatchJob {

@@ -17,6 +17,15 @@ constexpr uint32_t idesc_i8(int M, int N) {
 
 constexpr int COUNT_SHIFT = 14;   // log2(0x80 * 0x80): accumulators hold 2^14 * count
 
+// Instruction descriptor, kind::mxf4 (block-scaled 4-bit): B scale-factor
+// byte 0 (bits 4-5), A and B E2M1 (bits 7-9, 10-12 = 1), both K-major,
+// N >> 3 at bits 17-22, UE8M0 scale factors (bit 23), M >> 4 at bits 24-28,
+// A scale-factor byte 0 (bits 29-30), MMA-K 64 (bit 31 = 0); D is F32.
+constexpr uint32_t idesc_mxf4(int M, int N) {
+    return (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | (1u << 23) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
 // Shared-memory matrix descriptor for a K-major operand in the 128-byte
 // swizzled canonical layout: rows of 128 bytes, 8-row atoms 1024 bytes apart
 // (stride byte offset), fixed-constant bit 46, swizzle mode 2 (128 B).
@@ -48,6 +57,28 @@ __device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint6
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
         ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
+}
+
+// D += A x B over K = 64 E2M1 elements (32 bytes per row in each operand),
+// with the scale factors read from TMEM at sfa / sfb (block of 32 elements).
+__device__ __forceinline__ void tc_mma_mxf4(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                            uint32_t idesc, uint32_t accumulate, uint32_t sfa,
+                                            uint32_t sfb) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%5], [%6], p;\n\t}"
+        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(sfa), "r"(sfb)
+        : "memory");
+}
+
+// Write one 32-bit value to 16 consecutive TMEM columns of the warp's 32 lanes.
+__device__ __forceinline__ void tc_st_32x32b_x16_fill(uint32_t taddr, uint32_t x) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};"
+        ::"r"(taddr), "r"(x) : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 __device__ __forceinline__ void tc_commit(uint32_t bar) {

@@ -49,7 +49,7 @@ def test_hits_equal_dense(gpu_ctx, mode, lim, form):
 
 
 @pytest.mark.parametrize("m,n", [(1, 1), (33, 5), (129, 300), (257, 1), (640, 1025)])
-@pytest.mark.parametrize("kernel", [api.KERNEL_POPC, api.KERNEL_MMA])
+@pytest.mark.parametrize("kernel", [api.KERNEL_POPC, api.KERNEL_MMA, api.KERNEL_FP4])
 def test_hits_ragged_shapes(gpu_ctx, m, n, kernel):
     gpu_ctx.set_option(api.OPT_KERNEL, kernel)
     try:

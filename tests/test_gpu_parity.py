@@ -15,12 +15,13 @@ from qld_b200 import api, synth
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = ["popc", "mma128", "mma256"]
+KERNELS = ["popc", "mma128", "mma256", "fp4"]
 
 
 def set_kernel(ctx, name):
-    ctx.set_option(api.OPT_KERNEL, api.KERNEL_POPC if name == "popc" else api.KERNEL_MMA)
-    ctx.set_option(api.OPT_MMA_TILE, {"popc": 0, "mma128": 128, "mma256": 256}[name])
+    ctx.set_option(api.OPT_KERNEL, {"popc": api.KERNEL_POPC, "mma128": api.KERNEL_MMA,
+                                    "mma256": api.KERNEL_MMA, "fp4": api.KERNEL_FP4}[name])
+    ctx.set_option(api.OPT_MMA_TILE, {"popc": 0, "mma128": 128, "mma256": 256, "fp4": 0}[name])
     assert ctx.stats(reset=True) is not None
 
 
@@ -171,22 +172,58 @@ def test_invalid_arguments_return_codes(gpu_ctx):
     assert e.value.code == api.ERR_INVALID
 
 
-def test_tensor_core_limit_routes_to_popc(gpu_ctx):
-    """K * 64 above 131071 samples: AUTO takes the popcount kernel (exact),
-    an explicit tensor-core request is refused with UNSUPPORTED."""
-    N = 131_200
-    t, _ = synth.all_pairs_workload(m=40, n=N, seed=31)
+def test_tensor_core_limits(gpu_ctx):
+    """Each tensor-core kernel refuses tasks past its exact range with
+    UNSUPPORTED; AUTO takes the 4-bit kernel up to 2^24 samples and the
+    popcount kernel beyond."""
+    gpu_ctx.set_option(api.OPT_MMA_TILE, 0)
+    try:
+        N = 131_200                          # past the i8 kernels' 131,071
+        t, _ = synth.all_pairs_workload(m=40, n=N, seed=31)
+        A = t.numpy().view(np.uint64)
+        bc = oracle.bitcounts(A)
+        gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
+        gpu_ctx.stats(reset=True)
+        r2, cnt = gpu_ctx.ld(A, bc, S=N, counts=True)
+        assert gpu_ctx.stats().last_kernel == api.KERNEL_FP4
+        mask = lower_mask(40, 40)
+        assert np.array_equal(cnt[mask], oracle.counts(A)[mask])
+        gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_MMA)
+        with pytest.raises(api.QldError) as e:
+            gpu_ctx.ld(A, bc, S=N)
+        assert e.value.code == api.ERR_UNSUPPORTED
+        # past 2^24 samples: the F32 accumulators would round
+        K = (1 << 24) // 64 + 1
+        rng = np.random.default_rng(32)
+        A = rng.integers(0, 2**63, size=(20, K), dtype=np.uint64)
+        bc = oracle.bitcounts(A)
+        gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
+        gpu_ctx.stats(reset=True)
+        r2, cnt = gpu_ctx.ld(A, bc, S=K * 64, counts=True)
+        assert gpu_ctx.stats().last_kernel == api.KERNEL_POPC
+        mask = lower_mask(20, 20)
+        assert np.array_equal(cnt[mask], oracle.counts(A)[mask])
+        gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_FP4)
+        with pytest.raises(api.QldError) as e:
+            gpu_ctx.ld(A, bc, S=K * 64)
+        assert e.value.code == api.ERR_UNSUPPORTED
+    finally:
+        gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
+
+
+def test_fp4_past_the_int8_limit(gpu_ctx):
+    """The 4-bit kernel's F32 accumulators stay exact far past the i8
+    kernels' 131,071-sample limit (up to 2^24): 200,000 samples here."""
+    N = 200_000
+    t, _ = synth.all_pairs_workload(m=300, n=N, seed=33)
     A = t.numpy().view(np.uint64)
     bc = oracle.bitcounts(A)
-    gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
-    gpu_ctx.set_option(api.OPT_MMA_TILE, 0)
-    gpu_ctx.stats(reset=True)
-    r2, cnt = gpu_ctx.ld(A, bc, S=N, counts=True)
-    assert gpu_ctx.stats().last_kernel == api.KERNEL_POPC
-    mask = lower_mask(40, 40)
-    assert np.array_equal(cnt[mask], oracle.counts(A)[mask])
-    gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_MMA)
-    with pytest.raises(api.QldError) as e:
-        gpu_ctx.ld(A, bc, S=N)
-    assert e.value.code == api.ERR_UNSUPPORTED
-    gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
+    set_kernel(gpu_ctx, "fp4")
+    try:
+        r2, cnt = gpu_ctx.ld(A[:130], bc[:130], A[130:], bc[130:], S=N, counts=True)
+        want = oracle.counts(A[:130], A[130:])
+        assert np.array_equal(cnt, want)
+        assert_r2_close(r2, oracle.r2_exact(bc[:130], bc[130:], want, N))
+        assert gpu_ctx.stats().last_kernel == api.KERNEL_FP4
+    finally:
+        gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
