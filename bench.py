@@ -160,6 +160,8 @@ def kernel_roofline(ctx, variant, bitops, kern_ms, dev):
     """Roofline of the counts kernel against the measured rate of the pipe it
     runs on: the tensor pipe of its MMA kind (qld_cuda_measure_mma_peak,
     2 ops per bit-pair), or the popcount pipe (1 bit-op per bit-pair)."""
+    import torch
+    from qld_b200 import api
     if variant in (api.KERNEL_MMA, api.KERNEL_FP4):
         peak = ctx.measure_mma_peak(variant) / 1e12
         achieved = 2 * bitops / (kern_ms * 1e-3) / 1e12

@@ -70,7 +70,8 @@ extern "C" {
 #define QLD_OPT_KERNEL    1  /* QLD_KERNEL_*                                      */
 #define QLD_OPT_R2_MODE   2  /* QLD_R2_*                                          */
 #define QLD_OPT_PROFILE   3  /* 1: time every counts-kernel launch with events    */
-#define QLD_OPT_BAND_ROWS 4  /* B rows per streamed output band (host-buffer calls) */
+#define QLD_OPT_BAND_ROWS 4  /* B rows per streamed output band (host-buffer calls);
+                                rounded down to whole tile rows of the kernel */
 #define QLD_OPT_MMA_TILE  5  /* QLD_KERNEL_MMA output tile rows: 128, 256, 0 = per shape */
 
 typedef struct qld_ctx qld_ctx;
