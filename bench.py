@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--band", type=int, default=5000, help="windowed workload: band width")
     ap.add_argument("--jobs", type=int, default=4096, help="batched workload: number of tasks")
     ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma", "fp4"])
+    ap.add_argument("--sm-pair", type=int, default=0, choices=[0, 1, 2],
+                    help="4-bit kernel: SMs per output tile (0 = automatic)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mma-tile", type=int, default=0, choices=[0, 128, 256],
@@ -309,6 +311,7 @@ def ours_arm(args, rank, world, local_rank):
             "fp4": api.KERNEL_FP4}[args.kernel]
     ctx.set_option(api.OPT_KERNEL, kern)
     ctx.set_option(api.OPT_MMA_TILE, args.mma_tile)
+    ctx.set_option(api.OPT_SM_PAIR, args.sm_pair)
     ctx.set_option(api.OPT_PROFILE, 1)
     # A dedicated stream: torch's default stream is the legacy NULL stream,
     # which the C ABI reads as "the context's own stream".
@@ -528,6 +531,7 @@ def windowed_arm(args, rank, world, local_rank):
             "fp4": api.KERNEL_FP4}[args.kernel]
     ctx.set_option(api.OPT_KERNEL, kern)
     ctx.set_option(api.OPT_MMA_TILE, args.mma_tile)
+    ctx.set_option(api.OPT_SM_PAIR, args.sm_pair)
     ctx.set_option(api.OPT_PROFILE, 1)
     st = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(st)

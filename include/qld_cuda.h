@@ -73,6 +73,8 @@ extern "C" {
 #define QLD_OPT_BAND_ROWS 4  /* B rows per streamed output band (host-buffer calls);
                                 rounded down to whole tile rows of the kernel */
 #define QLD_OPT_MMA_TILE  5  /* QLD_KERNEL_MMA output tile rows: 128, 256, 0 = per shape */
+#define QLD_OPT_SM_PAIR   6  /* QLD_KERNEL_FP4 SMs per output tile: 1, 2 (a cluster of two
+                                CTAs, tcgen05 cta_group::2), 0 = automatic (2) */
 
 typedef struct qld_ctx qld_ctx;
 

@@ -128,5 +128,118 @@ __device__ __forceinline__ void chunk(const uint32_t (&v)[32], const ARow &ra, c
     }
 }
 
+// ------------------------------------------------ 4-bit kernels, R2_EXACT --
+//
+// The 4-bit kernels' accumulators hold each count as an exact F32 integer
+// (below 2^24, as are S, cA and cB), so D = S*c - cA*cB can be evaluated in
+// FP32 with a tight bound: split cA*cB = hi + lo exactly (hi = fl(cA*cB),
+// lo = fma(cA, cB, -hi), the FMA TwoProduct; lo is an integer, |lo| <= 2^23),
+// then D = fl(fl(S*c - hi) - lo) with S*c - hi rounded once by an FMA.  If
+// |S*c - hi| < 2^24 the FMA is exact and D is rounded once; otherwise
+// |D| >= |S*c - hi| / 2 and D carries at most 3 * 2^-24 relative error.  Then r^2 = (D*D) * (invA*invB) with
+// invA = fl(1/(cA(S-cA))) rounded from FP64: at most 11 * 2^-24 (6.6e-7)
+// relative error against the FP64 value, a dozen FP32 instructions per pair
+// instead of a chain of FP64 ones.  Exact zeros (D = 0), the 0 rule for
+// empty SNPs and NaN for 0/0 match the FP64 evaluation; values above 1.00009
+// (possible only when the bit counts do not match the data) are re-evaluated
+// in FP64 so the 123.456 rule decides exactly as in the other kernels.
+struct ColsF {
+    float2 *f;   // (cB as float, 1/(cB(S-cB)) rounded to float) per column
+    __device__ __forceinline__ ColsF(uint8_t *base, int) : f(reinterpret_cast<float2 *>(base)) {}
+};
+
+__device__ __forceinline__ double inv_var64(double c, double S) { return 1.0 / (c * (S - c)); }
+
+__device__ __forceinline__ void store_col_f32(const ColsF &f, int bl, uint32_t c, int S) {
+    f.f[bl] = make_float2((float)c, __double2float_rn(inv_var64((double)c, (double)S)));
+}
+
+struct ARowF {
+    float ca, inv;
+    bool zero;
+};
+
+__device__ __forceinline__ ARowF make_arow_f32(uint32_t c, int S) {
+    ARowF r;
+    r.ca = (float)c;
+    r.inv = __double2float_rn(inv_var64((double)c, (double)S));
+    r.zero = c == 0u;
+    return r;
+}
+
+__device__ __forceinline__ float pair_r2_f32(float c, float S_f, const ARowF &ra, float2 col) {
+    const float hi = __fmul_rn(ra.ca, col.x);
+    const float lo = __fmaf_rn(ra.ca, col.x, -hi);
+    const float D = __fsub_rn(__fmaf_rn(S_f, c, -hi), lo);
+    const float r = __fmul_rn(__fmul_rn(D, D), __fmul_rn(ra.inv, col.y));
+    return (ra.zero || col.x == 0.0f) ? 0.0f : r;
+}
+
+// The FP64 evaluation (pair_r2<R2_EXACT>) from the same exact inputs.
+__device__ __forceinline__ float pair_r2_f64(float c, float ca, float cb, int S) {
+    if (ca == 0.0f || cb == 0.0f) return 0.0f;
+    const double Sd = (double)S, a = (double)ca, b = (double)cb;
+    const double D = fma(Sd, (double)c, -(a * b));
+    const double r = (D * D) * (inv_var64(a, Sd) * inv_var64(b, Sd));
+    if (r > 1.0001) return 123.456f;
+    return __double2float_rn(r);
+}
+
+// One 32-column chunk of F32 accumulators v[t] (count c as float bits), as
+// chunk<R2_EXACT, 0> with the FP32 evaluation above.  taddr is the TMEM
+// address the chunk was loaded from: the rare pairs whose FP32 value lies
+// above 1.00009 are re-evaluated in FP64 from their count, reloaded one
+// column at a time (warp-uniform loads, off the common path).
+__device__ __forceinline__ void chunk_f32(uint32_t (&v)[32], uint32_t taddr, const ARowF &ra,
+                                          const ColsF &f, int bl0, int b0, int a, bool a_ok,
+                                          int n, int dlo, int dhi, float *r2, long long ldr,
+                                          uint32_t *counts, long long ldc, int row0, int S) {
+    const float S_f = (float)S;
+    if (counts && a_ok) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+            const int b = b0 + t;
+            if (b < n && a - b >= dlo && a - b <= dhi)
+                counts[(long long)(b - row0) * ldc + a] = (uint32_t)__uint_as_float(v[t]);
+        }
+    }
+    float rmax = 0.0f;
+#pragma unroll
+    for (int t = 0; t < 32; ++t) {
+        const float r = pair_r2_f32(__uint_as_float(v[t]), S_f, ra, f.f[bl0 + t]);
+        rmax = fmaxf(rmax, r);
+        v[t] = __float_as_uint(r);
+    }
+    if (__any_sync(0xffffffffu, rmax > 1.00009f)) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+            const bool redo = __uint_as_float(v[t]) > 1.00009f;
+            if (__any_sync(0xffffffffu, redo)) {
+                uint32_t w;
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];"
+                             : "=r"(w)
+                             : "r"(taddr + (uint32_t)t));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (redo)
+                    v[t] = __float_as_uint(
+                        pair_r2_f64(__uint_as_float(w), ra.ca, f.f[bl0 + t].x, S));
+            }
+        }
+    }
+    if (!a_ok) return;
+    float *o = r2 + (long long)(b0 - row0) * ldr + a;
+    const bool interior = (b0 + 31 < n) && (a - (b0 + 31) >= dlo) && (a - b0 <= dhi);
+    if (interior) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) o[(long long)t * ldr] = __uint_as_float(v[t]);
+    } else {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+            const int b = b0 + t;
+            if (b < n && a - b >= dlo && a - b <= dhi) o[(long long)t * ldr] = __uint_as_float(v[t]);
+        }
+    }
+}
+
 }  // namespace epi
 }  // namespace qld

@@ -3,18 +3,21 @@
 //
 // The counts C[a][b] = sum_k popc(A[a][k] & B[b][k]) (qLD's blis_gemm /
 // bin_gemm_2x2, src/correlator/src/gemm_cpu.c:125-341) are a dot product of
-// 0/1 vectors.  Here every bit becomes an E2M1 element -- 1.0 (0b0010) or
-// 0.0 -- packed two per byte, every scale factor is 1.0 (UE8M0 127), and
-// tcgen05.mma.kind::mxf4 accumulates 1.0 x 1.0 products in F32, which is
-// exact while a count stays below 2^24.  Against the kind::i8 kernels this
-// halves the bytes the unpack writes per bit (4 bits instead of 8), needs
-// 7 instead of 16 ALU instructions per 32 bits, and runs the MMA at the
-// 4-bit rate.
+// 0/1 vectors.  Here every bit becomes an E2M1 element -- zero or one
+// power of two, chosen per scale block so the spread is five ALU
+// instructions per 32 bits (tcgen05.cuh: spread_e2m1) -- packed two per
+// byte, with UE8M0 scale factors that make every 1 x 1 product exactly 1.0;
+// tcgen05.mma.kind::mxf4 accumulates them in F32, exact while a count stays
+// below 2^24.  Against the kind::i8 kernels this halves the bytes the unpack
+// writes per bit (4 bits instead of 8), needs 5 instead of 16 ALU
+// instructions per 32 bits, and runs the MMA at the 4-bit rate.  With
+// R2_EXACT the epilogue evaluates r^2 in FP32 from the exact F32 counts
+// (epilogue.cuh: chunk_f32).
 //
 // Tile and roles as ld_mma_wide.cu: 256 A rows x 240 B rows per CTA tile as
 // two 128 x 240 accumulators sharing every unpacked B stage.  TMEM: the
-// accumulators at columns 0 and 256, the scale factors (0x7F bytes) at
-// columns 496-511, written once at start and shared by A and B.
+// accumulators at columns 0 and 256, the scale factors at columns 496-511,
+// written once at start and shared by A and B.
 //   warp 0       TMA producer: 8 packed words (512 samples) of 256 A + 240 B
 //                rows per packed stage, 64-byte swizzle.
 //   warp 1       TMEM owner and MMA issuer: per unpacked stage (256 samples)
@@ -55,7 +58,8 @@ constexpr int TASKS = (NTASK + WORKERS - 1) / WORKERS;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t ACC1 = 256;           // TMEM column of accumulator 1
 constexpr uint32_t SF_COL = 496;         // 16 columns of scale factors
-constexpr uint32_t IDESC = idesc_mxf4(HM, BN);
+constexpr uint32_t IDESC_EVEN = idesc_mxf4_sf(HM, BN, 0);   // k-steps 0, 2: scale bytes 0-1
+constexpr uint32_t IDESC_ODD = idesc_mxf4_sf(HM, BN, 2);    // k-steps 1, 3: scale bytes 2-3
 constexpr int COLS_N = 256;              // epilogue column factors (BN used)
 
 constexpr int OFF_UA = 0;
@@ -80,21 +84,12 @@ struct Task {
 };
 
 // Output word t of input word x: bit 4n + t of x to bit 4n + 1 (E2M1 1.0).
-template <int T>
-__device__ __forceinline__ uint32_t spread(uint32_t x) {
-    constexpr uint32_t M = 0x22222222u;
-    if (T == 0) return (x << 1) & M;
-    if (T == 1) return x & M;
-    if (T == 2) return (x >> 1) & M;
-    return (x >> 2) & M;
-}
-
 __device__ __forceinline__ uint4 spread4(const uint4 &w, int t) {
     switch (t) {
-    case 0: return make_uint4(spread<0>(w.x), spread<0>(w.y), spread<0>(w.z), spread<0>(w.w));
-    case 1: return make_uint4(spread<1>(w.x), spread<1>(w.y), spread<1>(w.z), spread<1>(w.w));
-    case 2: return make_uint4(spread<2>(w.x), spread<2>(w.y), spread<2>(w.z), spread<2>(w.w));
-    default: return make_uint4(spread<3>(w.x), spread<3>(w.y), spread<3>(w.z), spread<3>(w.w));
+    case 0: return make_uint4(spread_e2m1<0>(w.x), spread_e2m1<0>(w.y), spread_e2m1<0>(w.z), spread_e2m1<0>(w.w));
+    case 1: return make_uint4(spread_e2m1<1>(w.x), spread_e2m1<1>(w.y), spread_e2m1<1>(w.z), spread_e2m1<1>(w.w));
+    case 2: return make_uint4(spread_e2m1<2>(w.x), spread_e2m1<2>(w.y), spread_e2m1<2>(w.z), spread_e2m1<2>(w.w));
+    default: return make_uint4(spread_e2m1<3>(w.x), spread_e2m1<3>(w.y), spread_e2m1<3>(w.z), spread_e2m1<3>(w.w));
     }
 }
 
@@ -134,6 +129,7 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
     uint64_t *mma_done = accempty + 1;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + OFF_TMEM);
     const epi::Cols cols(smem + OFF_ROWS, COLS_N);
+    const epi::ColsF colsf(smem + OFF_ROWS, COLS_N);   // R2_EXACT: FP32 factors
 
     if (grid_failed(p.status)) return;
     const TileList<BM, BN> tl{(p.m + BM - 1) / BM, p.tb0, tiles_b, p.symmetric, p.band};
@@ -171,10 +167,11 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    // Scale factors: every byte of columns SF_COL.. is UE8M0 127 (1.0); the
+    // Scale factors: every column SF_COL.. holds the four UE8M0 scales of the
+    // spread (kSpreadScales) in every lane, for A and B alike; the
     // four warps 2-5 cover the four TMEM lane quarters.
     if (warp >= FIRST_WORKER_WARP && warp < FIRST_WORKER_WARP + 4)
-        tc_st_32x32b_x16_fill(tmem + ((uint32_t)((warp & 3) * 32) << 16) + SF_COL, 0x7F7F7F7Fu);
+        tc_st_32x32b_x16_fill(tmem + ((uint32_t)((warp & 3) * 32) << 16) + SF_COL, kSpreadScales);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -238,8 +235,9 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
                     for (int kk = 0; kk < 4; ++kk) {
                         const uint64_t bd = sw128_desc(b0 + kk * 32);
                         const uint32_t acc = (u > 0 || kk > 0) ? 1u : 0u;
-                        tc_mma_mxf4(tmem, sw128_desc(a0 + kk * 32), bd, IDESC, acc, sf, sf);
-                        tc_mma_mxf4(tmem + ACC1, sw128_desc(a0 + HM * 128 + kk * 32), bd, IDESC,
+                        const uint32_t id = (kk & 1) ? IDESC_ODD : IDESC_EVEN;
+                        tc_mma_mxf4(tmem, sw128_desc(a0 + kk * 32), bd, id, acc, sf, sf);
+                        tc_mma_mxf4(tmem + ACC1, sw128_desc(a0 + HM * 128 + kk * 32), bd, id,
                                     acc, sf, sf);
                     }
                     tc_commit(smem_u32(&uempty[s]));
@@ -318,7 +316,11 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
             produce_until(lim < total_u ? lim : total_u);
             if (wt < BN) {
                 const int b = tb * BN + wt;
-                epi::store_col<MODE>(cols, wt, b < p.n ? p.bcB[b] : 0u, p.S);
+                const uint32_t cb = b < p.n ? p.bcB[b] : 0u;
+                if constexpr (MODE == R2_EXACT)
+                    epi::store_col_f32(colsf, wt, cb, p.S);
+                else
+                    epi::store_col<MODE>(cols, wt, cb, p.S);
             }
             named_bar_sync(1, WORKERS);
             bool ready = ok && !failed && mbar_wait(smem_u32(accfull), it & 1, p.timeout_cycles,
@@ -333,7 +335,9 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
                 tc_fence_after();
                 const int a = ta * BM + acc_i * HM + q * 32 + lane;
                 const bool a_ok = a < p.m;
-                const epi::ARow ra = epi::make_arow<MODE>(a_ok ? p.bcA[a] : 0u, p.S);
+                const uint32_t ca = a_ok ? p.bcA[a] : 0u;
+                const epi::ARow ra = epi::make_arow<MODE>(ca, p.S);
+                const epi::ARowF raf = epi::make_arow_f32(ca, p.S);
                 const uint32_t tbase =
                     tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)acc_i * ACC1;
                 // columns past the tile's 240 B rows are read but not written
@@ -343,11 +347,18 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
                     uint32_t v[32];
                     __syncwarp();
                     tc_ld_32x32b_x32(tbase + (uint32_t)(c * 32), v);
+                    if constexpr (MODE == R2_EXACT) {
+                        epi::chunk_f32(v, tbase + (uint32_t)(c * 32), raf, colsf, c * 32,
+                                       tb * BN + c * 32, a, a_ok, n_tile,
+                                       dlo, dhi, p.r2, p.ldr, p.counts, p.ldc, p.out_row0, p.S);
+                    } else {
 #pragma unroll
-                    for (int t = 0; t < 32; ++t)     // F32 accumulator -> count
-                        v[t] = (uint32_t)__uint_as_float(v[t]);
-                    epi::chunk<MODE, 0>(v, ra, cols, c * 32, tb * BN + c * 32, a, a_ok, n_tile,
-                                        dlo, dhi, p.r2, p.ldr, p.counts, p.ldc, p.out_row0, p.S);
+                        for (int t = 0; t < 32; ++t)     // F32 accumulator -> count
+                            v[t] = (uint32_t)__uint_as_float(v[t]);
+                        epi::chunk<MODE, 0>(v, ra, cols, c * 32, tb * BN + c * 32, a, a_ok,
+                                            n_tile, dlo, dhi, p.r2, p.ldr, p.counts, p.ldc,
+                                            p.out_row0, p.S);
+                    }
                 }
                 tc_fence_before();
                 __syncwarp();

@@ -41,6 +41,11 @@ extern const KernelShape kMxf4Shape;
 extern const int kMxf4MaxSamples;
 cudaError_t launch_mxf4(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
                         int tiles_b, int r2_mode, cudaStream_t st);
+// The same tiles computed by clusters of two CTAs (one per SM, 128 A rows and
+// 120 B rows each), with the epilogue overlapping the next tile's MMAs.
+extern const KernelShape kMxf4PairShape;
+cudaError_t launch_mxf4_pair(const CUtensorMap &tmA, const CUtensorMap &tmB, const LdParams &p,
+                             int tiles_b, int r2_mode, cudaStream_t st);
 
 // One task of a batched launch: its tensor maps (kBatchShape boxes), sizes,
 // output, and the number of work items (output tiles) of the tasks before it.

@@ -26,6 +26,32 @@ constexpr uint32_t idesc_mxf4(int M, int N) {
            ((uint32_t)(M >> 4) << 24);
 }
 
+// The same with both operands' scale factors read from byte `sf_byte` (0 or
+// 2) of their TMEM columns: an MMA of K = 64 uses two scale bytes per row,
+// for its first and second block of 32 elements.
+constexpr uint32_t idesc_mxf4_sf(int M, int N, uint32_t sf_byte) {
+    return idesc_mxf4(M, N) | (sf_byte << 29) | (sf_byte << 4);
+}
+
+// Bit -> E2M1 spread of the 4-bit kernels.  A 32-bit packed word x becomes
+// four words t = 0..3 of eight nibbles, nibble n of word t non-zero iff bit
+// 4n + t of x is set: the bit kept in place where it is a valid E2M1 code
+// (t = 0: 0b0001 = 0.5, t = 1: 0b0010 = 1.0, t = 2: 0b0100 = 2.0) and bit 3
+// (the sign) moved down to 2.0, five ALU instructions per word.  Each 16-byte
+// chunk of an unpacked row holds one word t of four packed words: 32
+// elements, exactly one scale block, whose UE8M0 scale factor (2, 1, 1/2,
+// 1/2 for t = 0..3) makes every 1 x 1 product exactly 1.  MMA k-step kk
+// covers chunks 2kk and 2kk + 1, i.e. t = 0, 1 for even kk (scale bytes 0-1
+// of a column) and t = 2, 3 for odd kk (bytes 2-3).
+template <int T>
+__device__ __forceinline__ uint32_t spread_e2m1(uint32_t x) {
+    if (T == 0) return x & 0x11111111u;
+    if (T == 1) return x & 0x22222222u;
+    if (T == 2) return x & 0x44444444u;
+    return (x >> 1) & 0x44444444u;
+}
+constexpr uint32_t kSpreadScales = 0x7E7E7F80u;   // bytes 0x80, 0x7F, 0x7E, 0x7E
+
 // Shared-memory matrix descriptor for a K-major operand in the 128-byte
 // swizzled canonical layout: rows of 128 bytes, 8-row atoms 1024 bytes apart
 // (stride byte offset), fixed-constant bit 46, swizzle mode 2 (128 B).
@@ -84,6 +110,71 @@ __device__ __forceinline__ void tc_st_32x32b_x16_fill(uint32_t taddr, uint32_t x
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
     asm volatile(
         "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        : "memory");
+}
+
+// ----------------------------------------------------- CTA-pair (2 SM) forms --
+//
+// A cluster of two CTAs (ranks 0 and 1) runs one MMA of M = 256 rows: rank r
+// holds A rows [128 r, 128 r + 128) and B rows [N/2 r, N/2 r + N/2) in its
+// shared memory at the same offsets, and its 128 x N accumulator in its own
+// TMEM.  Rank 0 issues the MMAs.
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_id_x() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_count_x() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+    return r;
+}
+
+// Every thread of both CTAs: shared-memory writes before it are visible to
+// the whole cluster after it.
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\t"
+                 "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Arrive on the mbarrier at the same offset in the shared memory of CTA
+// `rank`.  The default (release, CTA-scope) semantics suffice for the two
+// handshakes that use it: unpacked stages, written by the generic proxy and
+// handed to the tensor core after fence.proxy.async, and accumulators read
+// by tcgen05.ld before tcgen05.fence::before_thread_sync.  Cluster-scope
+// release/acquire on these barriers made the pair kernel twice as slow.
+__device__ __forceinline__ void mbar_arrive_rank(uint32_t bar, uint32_t rank) {
+    asm volatile(
+        "{\n\t.reg .b32 ra;\n\t"
+        "mapa.shared::cluster.u32 ra, %0, %1;\n\t"
+        "mbarrier.arrive.shared::cluster.b64 _, [ra];\n\t}"
+        ::"r"(bar), "r"(rank)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_mma_mxf4_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                                 uint32_t idesc, uint32_t accumulate,
+                                                 uint32_t sfa, uint32_t sfb) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%5], [%6], p;\n\t}"
+        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(sfa), "r"(sfb)
+        : "memory");
+}
+
+// Arrive once on the mbarrier at offset `bar` of every CTA in `mask` when the
+// pair MMAs issued so far have completed.
+__device__ __forceinline__ void tc_commit_pair(uint32_t bar, uint16_t mask) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+        " [%0], %1;" ::"r"(bar), "h"(mask)
         : "memory");
 }
 

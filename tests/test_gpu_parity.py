@@ -15,13 +15,16 @@ from qld_b200 import api, synth
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = ["popc", "mma128", "mma256", "fp4"]
+KERNELS = ["popc", "mma128", "mma256", "fp4", "fp4pair"]
 
 
 def set_kernel(ctx, name):
+    """fp4: the 4-bit kernel on one SM per tile; fp4pair: on a cluster of two."""
     ctx.set_option(api.OPT_KERNEL, {"popc": api.KERNEL_POPC, "mma128": api.KERNEL_MMA,
-                                    "mma256": api.KERNEL_MMA, "fp4": api.KERNEL_FP4}[name])
-    ctx.set_option(api.OPT_MMA_TILE, {"popc": 0, "mma128": 128, "mma256": 256, "fp4": 0}[name])
+                                    "mma256": api.KERNEL_MMA, "fp4": api.KERNEL_FP4,
+                                    "fp4pair": api.KERNEL_FP4}[name])
+    ctx.set_option(api.OPT_MMA_TILE, {"mma128": 128, "mma256": 256}.get(name, 0))
+    ctx.set_option(api.OPT_SM_PAIR, {"fp4": 1, "fp4pair": 2}.get(name, 0))
     assert ctx.stats(reset=True) is not None
 
 
@@ -218,12 +221,59 @@ def test_fp4_past_the_int8_limit(gpu_ctx):
     t, _ = synth.all_pairs_workload(m=300, n=N, seed=33)
     A = t.numpy().view(np.uint64)
     bc = oracle.bitcounts(A)
-    set_kernel(gpu_ctx, "fp4")
+    want = oracle.counts(A[:130], A[130:])
     try:
-        r2, cnt = gpu_ctx.ld(A[:130], bc[:130], A[130:], bc[130:], S=N, counts=True)
-        want = oracle.counts(A[:130], A[130:])
-        assert np.array_equal(cnt, want)
-        assert_r2_close(r2, oracle.r2_exact(bc[:130], bc[130:], want, N))
-        assert gpu_ctx.stats().last_kernel == api.KERNEL_FP4
+        for name in ("fp4", "fp4pair"):
+            set_kernel(gpu_ctx, name)
+            r2, cnt = gpu_ctx.ld(A[:130], bc[:130], A[130:], bc[130:], S=N, counts=True)
+            assert np.array_equal(cnt, want), name
+            assert_r2_close(r2, oracle.r2_exact(bc[:130], bc[130:], want, N))
+            assert gpu_ctx.stats().last_kernel == api.KERNEL_FP4
     finally:
         gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
+        gpu_ctx.set_option(api.OPT_SM_PAIR, 0)
+
+
+# (count, bcA, bcB) with S = 1000 whose FP64 r^2 lies around the 1.0001
+# sentinel threshold: bit counts that do not match the rows (a caller's error
+# the reference does not check) are the only way past r^2 = 1.
+THRESHOLD_CASES = [
+    (297, 299, 295),   # 1.0000918: kept (the 4-bit kernels re-evaluate in FP64)
+    (666, 624, 718),   # 1.0000909: kept
+    (512, 409, 702),   # 1.0001041: 123.456
+    (628, 745, 552),   # 1.0001030: 123.456
+    (476, 817, 779),   # 1.0000890: kept
+    (501, 850, 767),   # 1.0000110
+    (297, 470, 920),   # 0.9999673
+    (900, 100, 100),   # far above: 123.456
+    (300, 1000, 250),  # cA = S, D != 0: inf -> 123.456
+    (250, 1000, 250),  # cA = S, D = 0: NaN
+    (10, 0, 250),      # cA = 0: 0
+]
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_threshold_with_inconsistent_bitcounts(gpu_ctx, kernel):
+    """Every kernel classifies r^2 against the 1.0001 sentinel exactly as the
+    FP64 oracle does, including the 4-bit kernels' FP32 evaluation."""
+    S, K = 1000, 16
+    n = len(THRESHOLD_CASES)
+    bits = np.zeros((n, K * 64), np.uint8)
+    for i, (c, _, _) in enumerate(THRESHOLD_CASES):
+        bits[i, :c] = 1
+    rows = np.packbits(bits, axis=1).reshape(n, K, 8)
+    rows = rows.view(">u8").reshape(n, K).astype(np.uint64)   # bit 0 = MSB of word 0
+    bcA = np.array([t[1] for t in THRESHOLD_CASES], np.uint32)
+    bcB = np.array([t[2] for t in THRESHOLD_CASES], np.uint32)
+    set_kernel(gpu_ctx, kernel)
+    try:
+        r2, cnt = gpu_ctx.ld(rows, bcA, rows.copy(), bcB, S=S, counts=True)
+    finally:
+        gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
+        gpu_ctx.set_option(api.OPT_SM_PAIR, 0)
+    want_c = oracle.counts(rows, rows)
+    assert np.array_equal(cnt, want_c)
+    want = oracle.r2_exact(bcA, bcB, want_c, S)
+    d = np.diag(want)
+    assert (d == 123.456).sum() == 4 and np.isnan(d).sum() == 1 and (d == 0).sum() == 1
+    assert_r2_close(r2, want)
