@@ -193,10 +193,11 @@ def kernel_roofline(ctx, variant, bitops, kern_ms, dev):
             "peak_source": "measured: qld_cuda_measure_popc_peak (register-only AND+POPC)"}
 
 
-def measured_traffic(variant, workload):
+def measured_traffic(variant, workload, sm_pair=0):
     """DRAM bytes per launch of the counts kernel from the ncu capture
     summarised under profiles/ (None when no capture covers this case)."""
-    names = {2: "k_ld_mma_wide_traffic_16384.md", 3: "k_ld_mxf4_traffic_16384.md"}
+    names = {2: "k_ld_mma_wide_traffic_16384.md",
+             3: "k_ld_mxf4_traffic_16384.md" if sm_pair == 1 else "k_ld_mxf4_pair_traffic_16384.md"}
     if variant not in names or workload != "single_region_29817x16622_lower_triangle":
         return None
     path = os.path.join(ROOT, "profiles", names[variant])
@@ -364,7 +365,7 @@ def ours_arm(args, rank, world, local_rank):
     variant = stats.last_kernel
     roof = kernel_roofline(ctx, variant, bitops, kern_ms, dev)
     alg_bytes = m * K * 8 * 2 + pairs * 4
-    roof["traffic"] = measured_traffic(variant, cfg["workload"])
+    roof["traffic"] = measured_traffic(variant, cfg["workload"], args.sm_pair)
     roof["algorithmic_bytes_per_launch"] = alg_bytes
     roof["kernel_ms"] = kern_ms
     roof["hbm_frac_of_measured"] = (alg_bytes / (kern_ms * 1e-3) / 1e9) / 6538.9

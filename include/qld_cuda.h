@@ -25,8 +25,12 @@
  *
  * r^2 modes (per entry, cA = bcA[j], cB = bcB[i], c = count, S = snp_size):
  *   QLD_R2_EXACT      r^2 = D^2 / (cA(S-cA) cB(S-cB)) with the exact integer
- *                     D = S*c - cA*cB, evaluated in FP64 and rounded once to
- *                     FP32 (relative error <= 2^-24 against an FP64 oracle).
+ *                     D = S*c - cA*cB; relative error <= 1e-6 against an
+ *                     FP64 oracle.  The popcount and int8 kernels evaluate in
+ *                     FP64 and round once (<= 2^-24); the 4-bit kernels in
+ *                     FP32 from their exact F32 counts, D to 3 * 2^-24 and
+ *                     r^2 to 11 * 2^-24 (6.6e-7).  Zeros, NaN and 123.456
+ *                     are identical in every kernel.
  *   QLD_R2_REFERENCE  bit-identical to get_pairwise_ld_score()
  *                     (gemm_cpu.c:343-404): FP32 frequencies, FP32 numerator,
  *                     FP64 denominator, no fused multiply-add.

@@ -24,7 +24,7 @@
 //   warps 2-9    unpack (w -> four words of nibbles, as ld_mxf4.cu) into the
 //                CTA's stage; they arrive on rank 0's "full" barrier.  Two
 //                groups of four warps take alternate unpacked stages (each
-//                warp 4 rows of every other stage): two stages in flight per
+//                thread 2 rows of every other stage): two stages in flight per
 //                CTA, which the per-warp latency of a stage (load, spread,
 //                store, proxy fence, remote arrive) needs to keep up with the
 //                MMAs.
@@ -63,7 +63,7 @@ constexpr int UNPACKERS = UNPACK_WARPS * 32;
 constexpr int EPILOGUE = EPI_WARPS * 32;
 constexpr int THREADS = (FIRST_EPI_WARP + EPI_WARPS) * 32;   // 576
 constexpr int GROUP_THREADS = UNPACKERS / 2;                 // unpackers per stage
-constexpr int NTASK = 2 * (HM + HN);                         // (row, half) tasks
+constexpr int NTASK = HM + HN;                               // row tasks
 constexpr int TASKS = (NTASK + GROUP_THREADS - 1) / GROUP_THREADS;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t ACC_STRIDE = 256;     // accumulator buffers at columns 0 and 256
@@ -88,39 +88,48 @@ static_assert(OFF_UB % 1024 == 0 && UB_BYTES % 1024 == 0 && OFF_PA % 1024 == 0 &
                   OFF_PB % 1024 == 0 && PB_TX <= PB_BYTES,
               "swizzled stages must start on 1024-byte boundaries");
 static_assert(ACC_STRIDE + BN <= SF_COL && SF_COL + 16 <= TMEM_COLS, "TMEM map");
-static_assert(TASKS == 4 && SUB == 2 && UST % 2 == 0 && EPILOGUE >= BN, "work split");
+static_assert(TASKS == 2 && SUB == 2 && UST % 2 == 0 && EPILOGUE >= BN, "work split");
 
-struct Task {
-    uint32_t src, xr, dst, is_a, valid, half;
-    uint32_t chunk_off[4];
+// One unpack task: one packed row (A or B) of the CTA, both 16-byte halves of
+// the 32 bytes (256 samples) a sub-stage takes from each 64-byte packed row.
+// A quarter-warp then covers 8 consecutive rows, so its 16-byte loads from
+// the 64-byte-swizzled packed stage and its stores into the 128-byte-swizzled
+// unpacked stage both touch all 32 banks once.
+struct RowTask {
+    uint32_t src, xr, is_a, valid;
+    uint32_t off[8];     // destination: row base + swizzled offset of chunk 0..7
 };
 
-__device__ __forceinline__ uint4 spread4(const uint4 &w, int t) {
-    switch (t) {
-    case 0: return make_uint4(spread_e2m1<0>(w.x), spread_e2m1<0>(w.y), spread_e2m1<0>(w.z), spread_e2m1<0>(w.w));
-    case 1: return make_uint4(spread_e2m1<1>(w.x), spread_e2m1<1>(w.y), spread_e2m1<1>(w.z), spread_e2m1<1>(w.w));
-    case 2: return make_uint4(spread_e2m1<2>(w.x), spread_e2m1<2>(w.y), spread_e2m1<2>(w.z), spread_e2m1<2>(w.w));
-    default: return make_uint4(spread_e2m1<3>(w.x), spread_e2m1<3>(w.y), spread_e2m1<3>(w.z), spread_e2m1<3>(w.w));
-    }
+template <int T>
+__device__ __forceinline__ uint4 spread4(const uint4 &w) {
+    return make_uint4(spread_e2m1<T>(w.x), spread_e2m1<T>(w.y), spread_e2m1<T>(w.z),
+                      spread_e2m1<T>(w.w));
 }
 
-__device__ __forceinline__ void unpack_stage(const Task (&task)[TASKS], const uint8_t *pa,
-                                             const uint8_t *pb, uint8_t *ua, uint8_t *ub,
-                                             int sub) {
-    uint4 w[TASKS];
+__device__ __forceinline__ void unpack_rows(const RowTask (&task)[TASKS], const uint8_t *pa,
+                                            const uint8_t *pb, uint8_t *ua, uint8_t *ub,
+                                            int sub) {
+    uint4 w[TASKS][2];
 #pragma unroll
     for (int j = 0; j < TASKS; ++j)
-        if (task[j].valid)
-            w[j] = *reinterpret_cast<const uint4 *>(
-                (task[j].is_a ? pa : pb) + task[j].src +
-                ((((uint32_t)sub * 2 + task[j].half) ^ task[j].xr) << 4));
+        if (task[j].valid) {
+            const uint8_t *row = (task[j].is_a ? pa : pb) + task[j].src;
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                w[j][h] = *reinterpret_cast<const uint4 *>(
+                    row + ((((uint32_t)sub * 2 + h) ^ task[j].xr) << 4));
+        }
 #pragma unroll
     for (int j = 0; j < TASKS; ++j) {
         if (!task[j].valid) continue;
-        uint8_t *dst = (task[j].is_a ? ua : ub) + task[j].dst;
+        uint8_t *dst = task[j].is_a ? ua : ub;
 #pragma unroll
-        for (int cc = 0; cc < 4; ++cc)
-            *reinterpret_cast<uint4 *>(dst + task[j].chunk_off[cc]) = spread4(w[j], cc);
+        for (int h = 0; h < 2; ++h) {
+            *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 0]) = spread4<0>(w[j][h]);
+            *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 1]) = spread4<1>(w[j][h]);
+            *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 2]) = spread4<2>(w[j][h]);
+            *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 3]) = spread4<3>(w[j][h]);
+        }
     }
 }
 
@@ -264,22 +273,19 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         // every packed stage
         const int grp = (warp - FIRST_UNPACK_WARP) / (UNPACK_WARPS / 2);
         const int wt = ((warp - FIRST_UNPACK_WARP) % (UNPACK_WARPS / 2)) * 32 + lane;
-        Task task[TASKS];
+        RowTask task[TASKS];
 #pragma unroll
         for (int j = 0; j < TASKS; ++j) {
-            const int t = wt + j * GROUP_THREADS;  // (row, half) over 128 A + 120 B rows
-            const int row = t >> 1, half = t & 1;
+            const int row = wt + j * GROUP_THREADS;   // over 128 A + 120 B rows
             const bool isA = row < HM;
             const int r = isA ? row : row - HM;
-            task[j].valid = t < NTASK;
+            task[j].valid = row < NTASK;
             task[j].is_a = isA;
-            task[j].half = (uint32_t)half;
             task[j].src = (uint32_t)(r * 64);
             task[j].xr = (uint32_t)((r >> 1) & 3);
-            task[j].dst = (uint32_t)(r * 128);
 #pragma unroll
-            for (int cc = 0; cc < 4; ++cc)
-                task[j].chunk_off[cc] = (uint32_t)(((half * 4 + cc) ^ (r & 7)) << 4);
+            for (int c = 0; c < 8; ++c)
+                task[j].off[c] = (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
         }
         const int total_u = my_tiles * nu;
         for (int gu = grp; gu < total_u; gu += 2) {
@@ -298,8 +304,8 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 if (lane == 0) flag_error(p.status, ST_TIMEOUT_MMA);
                 break;
             }
-            unpack_stage(task, smem + OFF_PA + ps * PA_BYTES, smem + OFF_PB + ps * PB_BYTES,
-                         smem + OFF_UA + us * UA_BYTES, smem + OFF_UB + us * UB_BYTES, grp);
+            unpack_rows(task, smem + OFF_PA + ps * PA_BYTES, smem + OFF_PB + ps * PB_BYTES,
+                        smem + OFF_UA + us * UA_BYTES, smem + OFF_UB + us * UB_BYTES, grp);
             fence_proxy_async_smem();
             __syncwarp();
             if (lane == 0) {

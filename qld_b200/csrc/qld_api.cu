@@ -541,9 +541,18 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
     if (!A || !bcA || !B || !bcB || !r2_out)
         return set_err(c, QLD_ERR_INVALID, "NULL table, bit-count or output pointer");
     CUDA_TRY(c, cudaSetDevice(c->device));
-    Task t;
+    const long long Kp = K + (K & 1);
     int rc;
-    if ((rc = stage_tables(c, A, bcA, m, B, bcB, n, K, S, symmetric, &t))) return rc;
+    if ((rc = ensure(c, c->dA, (size_t)m * Kp * 8)) || (rc = ensure(c, c->dbcA, (size_t)m * 4)))
+        return rc;
+    if (!symmetric && ((rc = ensure(c, c->dB, (size_t)n * Kp * 8)) ||
+                       (rc = ensure(c, c->dbcB, (size_t)n * 4))))
+        return rc;
+    uint64_t *dA = static_cast<uint64_t *>(c->dA.p);
+    uint64_t *dB = symmetric ? dA : static_cast<uint64_t *>(c->dB.p);
+    const uint32_t *dbcA = static_cast<const uint32_t *>(c->dbcA.p);
+    const uint32_t *dbcB = symmetric ? dbcA : static_cast<const uint32_t *>(c->dbcB.p);
+    const Task t{dA, dbcA, m, Kp, dB, dbcB, n, Kp, K, S, symmetric, 0};
 
     const int band = band_rows_for(c, t);   // whole tile rows of the task's kernel
     const int nbands = (n + band - 1) / band;
@@ -552,10 +561,40 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
         if ((rc = ensure(c, c->dOut[s], slot_rows * m * 4))) return rc;
         if (counts_out && (rc = ensure(c, c->dCnt[s], slot_rows * m * 4))) return rc;
     }
-    for (int bi = 0; bi < nbands; ++bi) {
-        const int s = bi & 1;
+    // Tables go up in chunks of `band` rows on the h2d stream, an event after
+    // each, so each band's kernel starts once the rows it reads are resident
+    // and the host->device copies overlap the device->host results.  A single
+    // region runs its bands last to first: band [b0, b1) reads table rows
+    // from b0 (less one A tile) to m, which the chunks uploaded last-first
+    // provide early, and its small last bands start the result copies at once.
+    while ((int)c->h2d_ev.size() < nbands) {
+        cudaEvent_t e;
+        CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->h2d_ev.push_back(e);
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(c->dbcA.p, bcA, (size_t)m * 4, cudaMemcpyHostToDevice, c->h2d));
+    if (!symmetric) {
+        CUDA_TRY(c, cudaMemcpyAsync(c->dbcB.p, bcB, (size_t)n * 4, cudaMemcpyHostToDevice, c->h2d));
+        CUDA_TRY(c, cudaMemcpy2DAsync(dA, Kp * 8, A, (size_t)K * 8, (size_t)K * 8, m,
+                                      cudaMemcpyHostToDevice, c->h2d));
+    }
+    for (int k = 0; k < nbands; ++k) {
+        const int i = symmetric ? nbands - 1 - k : k;
+        const int r0 = i * band, r1 = r0 + band < n ? r0 + band : n;
+        CUDA_TRY(c, cudaMemcpy2DAsync(dB + (size_t)r0 * Kp, Kp * 8, B + (size_t)r0 * K,
+                                      (size_t)K * 8, (size_t)K * 8, r1 - r0,
+                                      cudaMemcpyHostToDevice, c->h2d));
+        CUDA_TRY(c, cudaEventRecord(c->h2d_ev[i], c->h2d));
+    }
+    for (int k = 0; k < nbands; ++k) {
+        const int bi = symmetric ? nbands - 1 - k : k;
+        const int s = k & 1;
         const int b0 = bi * band, b1 = b0 + band < n ? b0 + band : n;
-        if (bi >= 2) CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_copy[s], 0));
+        // symmetric: the chunk holding row b0 - 256 (A tiles start at multiples
+        // of 256), uploaded after every chunk above it
+        const int need = symmetric ? (b0 >= 256 ? (b0 - 256) / band : 0) : bi;
+        CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->h2d_ev[need], 0));
+        if (k >= 2) CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_copy[s], 0));
         float *r2s = static_cast<float *>(c->dOut[s].p);
         uint32_t *cs = counts_out ? static_cast<uint32_t *>(c->dCnt[s].p) : nullptr;
         if ((rc = launch_counts(c, t, b0, b1, r2s, m, cs, m, b0, c->stream))) return rc;
@@ -569,10 +608,10 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
                                             (size_t)(b1 - b0) * m * 4, cudaMemcpyDeviceToHost,
                                             c->copy));
         } else {
-            // Per 128 rows: columns [r0, m) hold every entry j >= i.
-            for (int r0 = b0; r0 < b1; r0 += 128) {
-                const int r1 = r0 + 128 < b1 ? r0 + 128 : b1;
-                if (r0 >= m) break;
+            // Per 512 rows: columns [r0, m) hold every entry j >= i (fewer,
+            // larger 2-D copies run closer to the link rate than per 128 rows).
+            for (int r0 = b0; r0 < b1; r0 += 512) {
+                const int r1 = r0 + 512 < b1 ? r0 + 512 : b1;
                 const size_t w = (size_t)(m - r0) * 4;
                 CUDA_TRY(c, cudaMemcpy2DAsync(r2_out + (size_t)r0 * m + r0, (size_t)m * 4,
                                               r2s + (size_t)(r0 - b0) * m + r0, (size_t)m * 4, w,
@@ -586,6 +625,7 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
         CUDA_TRY(c, cudaEventRecord(c->ev_copy[s], c->copy));
     }
     CUDA_TRY(c, cudaStreamSynchronize(c->copy));
+    CUDA_TRY(c, cudaStreamSynchronize(c->h2d));
     return finish(c, c->stream);
 }
 
