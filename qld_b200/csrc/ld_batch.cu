@@ -1,15 +1,17 @@
 // ld_batch.cu -- many independent LD tasks (region pairs of uneven SNP and
 // sample counts) in one persistent launch fed by a device work queue.
 //
-// Per-task arithmetic is that of ld_mma.cu (128 x 256 output tiles, bits
-// unpacked to {0, 0x80} bytes, tcgen05.mma.kind::i8 into s32 TMEM
-// accumulators holding 2^14 * count, fused r^2 epilogue of qLD
-// gemm_cpu.c:343-404); qLD itself runs such task lists one task at a time
-// (-inputList, src/correlator/src/input_list.c:205-323 and
-// correlate_function.c:59-83).  Here every output tile of every task is a
-// work item.  The device job table holds per task its tensor maps, sizes and
-// output, and the item prefix offsets; items are numbered task by task
-// (tasks sorted by cost on the host, most expensive first).
+// Per-task arithmetic is that of the 4-bit kernels (ld_mxf4.cu): bits spread
+// to E2M1 with normalising UE8M0 scale factors (tcgen05.cuh: spread_e2m1),
+// tcgen05.mma.kind::mxf4 into F32 TMEM accumulators that hold the counts
+// exactly (K * 64 <= 2^24), fused r^2 epilogue of qLD gemm_cpu.c:343-404
+// (R2_EXACT in FP32 from the exact counts, epilogue.cuh: chunk_f32).  qLD
+// itself runs such task lists one task at a time (-inputList,
+// src/correlator/src/input_list.c:205-323 and correlate_function.c:59-83).
+// Here every 128 x 240 output tile of every task is a work item.  The device
+// job table holds per task its tensor maps, sizes and output, and the item
+// prefix offsets; items are numbered task by task (tasks sorted by cost on
+// the host, most expensive first).
 //
 // Work queue: the producer thread of each CTA claims the next item with an
 // atomic ticket on a global counter, decodes it into (task, A tile, B tile),
@@ -17,6 +19,12 @@
 // stages.  The MMA thread, the unpack warps and the epilogue warps pop the
 // same items in the same order; each of them releases a ring slot when done
 // with its item.  A ticket past the last item pushes an end marker.
+//
+// Roles (576 threads): warp 0 queue + TMA, warp 1 TMEM + MMA, warps 2-9
+// unpack in two groups taking alternate 256-sample stages (each thread whole
+// rows: conflict-free), warps 10-17 epilogue (two per TMEM lane quarter).
+// TMEM: two 240-column accumulators (columns 0 and 256) so a tile's epilogue
+// overlaps the next tile's MMAs, the scale factors at columns 496-511.
 #include "epilogue.cuh"
 #include "qld_kernels.h"
 #include "tcgen05.cuh"
@@ -27,26 +35,30 @@ namespace {
 
 using namespace tc;
 
-constexpr int BM = 128, BN = 256;
-constexpr int PW = 8;
-constexpr int SUB = PW / 2;
-constexpr int PST = 3;
-constexpr int UST = 3;
-constexpr int PA_BYTES = BM * PW * 8;
-constexpr int PB_BYTES = BN * PW * 8;
-constexpr int UA_BYTES = BM * 128;
-constexpr int UB_BYTES = BN * 128;
-constexpr int UNPACK_WARPS = 12;
-constexpr int UNPACK_THREADS = UNPACK_WARPS * 32;
-constexpr int EPI_WARPS = 4;
+constexpr int BM = 128, BN = 240;
+constexpr int PW = 8;                       // packed words per row per packed stage
+constexpr int SUB = 2;                      // unpacked stages (256 samples) per packed stage
+constexpr int PST = 4;
+constexpr int UST = 2;                      // one unpacked stage per unpack group
+constexpr int PA_BYTES = BM * PW * 8;       // 8 KB
+constexpr int PB_BYTES = BN * PW * 8;       // 15 KB
+constexpr int UA_BYTES = BM * 128;          // 16 KB: 256 E2M1 per row
+constexpr int UB_BYTES = BN * 128;          // 30 KB
+constexpr int UNPACK_WARPS = 8;
+constexpr int GROUP_THREADS = UNPACK_WARPS * 32 / 2;
+constexpr int EPI_WARPS = 8;
 constexpr int EPI_THREADS = EPI_WARPS * 32;
 constexpr int FIRST_UNPACK_WARP = 2;
 constexpr int FIRST_EPI_WARP = FIRST_UNPACK_WARP + UNPACK_WARPS;
 constexpr int THREADS = (FIRST_EPI_WARP + EPI_WARPS) * 32;   // 576
-constexpr int TASKS = 2 * (BM + BN) / UNPACK_THREADS;
-static_assert(TASKS * UNPACK_THREADS == 2 * (BM + BN), "unpack tasks must divide evenly");
+constexpr int NROWS = BM + BN;                                // row tasks per stage
+constexpr int TASKS = (NROWS + GROUP_THREADS - 1) / GROUP_THREADS;
 constexpr uint32_t TMEM_COLS = 512;
-constexpr uint32_t IDESC = idesc_i8(BM, BN);
+constexpr uint32_t ACC_STRIDE = 256;
+constexpr uint32_t SF_COL = 496;
+constexpr uint32_t IDESC_EVEN = idesc_mxf4_sf(BM, BN, 0);   // k-steps 0, 2: scale bytes 0-1
+constexpr uint32_t IDESC_ODD = idesc_mxf4_sf(BM, BN, 2);    // k-steps 1, 3: scale bytes 2-3
+constexpr int COLS_N = 256;                                  // epilogue column factors (BN used)
 constexpr int QSLOTS = 4;                                    // item ring depth
 constexpr int ITEM_USERS = 1 + UNPACK_WARPS + EPI_WARPS;     // arrivals freeing a slot
 
@@ -55,23 +67,35 @@ constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
 constexpr int OFF_PA = OFF_UB + UST * UB_BYTES;
 constexpr int OFF_PB = OFF_PA + PST * PA_BYTES;
 constexpr int OFF_ROWS = OFF_PB + PST * PB_BYTES;
-constexpr int ROWS_BYTES = BN * epi::COL_BYTES;
+constexpr int ROWS_BYTES = COLS_N * epi::COL_BYTES;
 constexpr int OFF_ITEMS = OFF_ROWS + ROWS_BYTES;
 constexpr int OFF_BAR = OFF_ITEMS + QSLOTS * 16;
 constexpr int NBARS = 2 * PST + 2 * UST + 2 + 2 + 1 + 2 * QSLOTS;
 constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
 constexpr int SMEM_BYTES = OFF_TMEM + 16 + 1024;
 static_assert(SMEM_BYTES <= 232448, "shared memory budget");
+static_assert(OFF_UB % 1024 == 0 && UB_BYTES % 1024 == 0 && OFF_PA % 1024 == 0 &&
+                  OFF_PB % 1024 == 0 && PB_BYTES % 1024 == 0,
+              "swizzled stages must start on 1024-byte boundaries");
+static_assert(ACC_STRIDE + BN <= SF_COL && SF_COL + 16 <= TMEM_COLS, "TMEM map");
+static_assert(TASKS == 3 && SUB == 2 && UST == 2 && EPI_THREADS == COLS_N, "work split");
 
 struct Item {
     int job, ta, tb, np;   // job < 0: end of the queue
 };
 
-struct Task {
-    uint32_t src, xr, dst, is_a;
-    uint32_t chunk_off[4];
-    uint32_t pow2[4];
+// One unpack task: one packed row, both 16-byte halves of the 32 bytes a
+// 256-sample stage takes from it (ld_mxf4_pair.cu: RowTask).
+struct RowTask {
+    uint32_t src, xr, is_a, valid;
+    uint32_t off[8];     // destination: row base + swizzled offset of chunk 0..7
 };
+
+template <int T>
+__device__ __forceinline__ uint4 spread4(const uint4 &w) {
+    return make_uint4(spread_e2m1<T>(w.x), spread_e2m1<T>(w.y), spread_e2m1<T>(w.z),
+                      spread_e2m1<T>(w.w));
+}
 
 // (job, ta, tb) of global item g: binary search of the item prefix, then the
 // job's own B-tile-row-first tile list.
@@ -106,7 +130,8 @@ k_ld_batch(const BatchParams bp) {
     uint64_t *ifull = mma_done + 1, *iempty = ifull + QSLOTS;
     Item *items = reinterpret_cast<Item *>(smem + OFF_ITEMS);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + OFF_TMEM);
-    const epi::Cols cols(smem + OFF_ROWS, BN);
+    const epi::Cols cols(smem + OFF_ROWS, COLS_N);
+    const epi::ColsF colsf(smem + OFF_ROWS, COLS_N);   // R2_EXACT: FP32 factors
 
     if (grid_failed(bp.status)) return;
     const int tid = threadIdx.x;
@@ -116,10 +141,10 @@ k_ld_batch(const BatchParams bp) {
     if (tid == 0) {
         for (int s = 0; s < PST; ++s) {
             mbar_init(smem_u32(&pfull[s]), 1);
-            mbar_init(smem_u32(&pempty[s]), UNPACK_WARPS);
+            mbar_init(smem_u32(&pempty[s]), UNPACK_WARPS);   // both groups, once each
         }
         for (int s = 0; s < UST; ++s) {
-            mbar_init(smem_u32(&ufull[s]), UNPACK_WARPS);
+            mbar_init(smem_u32(&ufull[s]), UNPACK_WARPS / 2);   // one group per stage
             mbar_init(smem_u32(&uempty[s]), 1);
         }
         for (int s = 0; s < 2; ++s) {
@@ -144,6 +169,13 @@ k_ld_batch(const BatchParams bp) {
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    // the spread's scale factors in columns SF_COL.. of every lane (warps 2-5
+    // cover the four TMEM lane quarters)
+    if (warp >= FIRST_UNPACK_WARP && warp < FIRST_UNPACK_WARP + 4)
+        tc_st_32x32b_x16_fill(tmem + ((uint32_t)((warp & 3) * 32) << 16) + SF_COL, kSpreadScales);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
 
     if (warp == 0) {
         // --------------------------------------- work queue + TMA producer --
@@ -191,6 +223,7 @@ k_ld_batch(const BatchParams bp) {
     } else if (warp == 1) {
         // ----------------------------------------------------- MMA issuer --
         if (lane == 0) {
+            const uint32_t sf = tmem + SF_COL;
             int gu = 0, it_n = 0;
             bool ok = true;
             for (int qi = 0; ok; ++qi, ++it_n) {
@@ -208,7 +241,7 @@ k_ld_batch(const BatchParams bp) {
                     break;
                 }
                 tc_fence_after();
-                const uint32_t d = tmem + (uint32_t)(ab * BN);
+                const uint32_t d = tmem + (uint32_t)ab * ACC_STRIDE;
                 for (int u = 0; u < it.np * SUB; ++u, ++gu) {
                     const int s = gu % UST;
                     if (!mbar_wait(smem_u32(&ufull[s]), (gu / UST) & 1, limit, bp.status)) {
@@ -221,8 +254,9 @@ k_ld_batch(const BatchParams bp) {
                     const uint32_t b0 = smem_u32(smem + OFF_UB + s * UB_BYTES);
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk)
-                        tc_mma_i8(d, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), IDESC,
-                                  (u > 0 || kk > 0) ? 1u : 0u);
+                        tc_mma_mxf4(d, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32),
+                                    (kk & 1) ? IDESC_ODD : IDESC_EVEN, (u > 0 || kk > 0) ? 1u : 0u,
+                                    sf, sf);
                     tc_commit(smem_u32(&uempty[s]));
                 }
                 tc_commit(smem_u32(&accfull[ab]));
@@ -232,26 +266,26 @@ k_ld_batch(const BatchParams bp) {
         }
     } else if (warp < FIRST_EPI_WARP) {
         // --------------------------------------------------------- unpack --
-        const int ut = tid - FIRST_UNPACK_WARP * 32;
-        Task task[TASKS];
+        // group g takes sub-stage g of every packed stage (unpacked stage g)
+        const int grp = (warp - FIRST_UNPACK_WARP) / (UNPACK_WARPS / 2);
+        const int wt = ((warp - FIRST_UNPACK_WARP) % (UNPACK_WARPS / 2)) * 32 + lane;
+        RowTask task[TASKS];
 #pragma unroll
         for (int j = 0; j < TASKS; ++j) {
-            const int t = ut + j * UNPACK_THREADS;
-            const int row = t >> 1, half = t & 1;
+            const int row = wt + j * GROUP_THREADS;   // over 128 A + 240 B rows
             const bool isA = row < BM;
             const int r = isA ? row : row - BM;
+            task[j].valid = row < NROWS;
             task[j].is_a = isA;
             task[j].src = (uint32_t)(r * 64);
             task[j].xr = (uint32_t)((r >> 1) & 3);
-            task[j].dst = (uint32_t)(r * 128);
 #pragma unroll
-            for (int cc = 0; cc < 4; ++cc) {
-                const int c = half * 4 + cc;
-                task[j].chunk_off[cc] = (uint32_t)((c ^ (r & 7)) << 4);
-                task[j].pow2[cc] = 1u << (7 - c);
-            }
+            for (int c = 0; c < 8; ++c)
+                task[j].off[c] = (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
         }
-        int gp = 0, gu = 0;
+        uint8_t *ua = smem + OFF_UA + grp * UA_BYTES;
+        uint8_t *ub = smem + OFF_UB + grp * UB_BYTES;
+        int gp = 0, nst = 0;   // packed stages seen; stages this group unpacked
         bool ok = true;
         for (int qi = 0; ok; ++qi) {
             const int slot = qi % QSLOTS;
@@ -263,7 +297,7 @@ k_ld_batch(const BatchParams bp) {
             }
             const Item it = items[slot];
             if (it.job < 0) break;
-            for (int kp = 0; kp < it.np && ok; ++kp, ++gp) {
+            for (int kp = 0; kp < it.np; ++kp, ++gp, ++nst) {
                 const int ps = gp % PST;
                 const bool got = mbar_wait(smem_u32(&pfull[ps]), (gp / PST) & 1, limit, bp.status);
                 if (!__all_sync(0xffffffffu, got)) {
@@ -271,53 +305,58 @@ k_ld_batch(const BatchParams bp) {
                     ok = false;
                     break;
                 }
+                const bool freed = nst == 0 || mbar_wait(smem_u32(&uempty[grp]), (nst - 1) & 1,
+                                                         limit, bp.status);
+                if (!__all_sync(0xffffffffu, freed)) {
+                    if (lane == 0) flag_error(bp.status, ST_TIMEOUT_MMA);
+                    ok = false;
+                    break;
+                }
                 const uint8_t *pa = smem + OFF_PA + ps * PA_BYTES;
                 const uint8_t *pb = smem + OFF_PB + ps * PB_BYTES;
-                for (int sub = 0; sub < SUB; ++sub, ++gu) {
-                    const int us = gu % UST;
-                    const bool freed = gu < UST || mbar_wait(smem_u32(&uempty[us]),
-                                                             ((gu / UST) - 1) & 1, limit,
-                                                             bp.status);
-                    if (!__all_sync(0xffffffffu, freed)) {
-                        if (lane == 0) flag_error(bp.status, ST_TIMEOUT_MMA);
-                        ok = false;
-                        break;
+                uint4 w[TASKS][2];
+#pragma unroll
+                for (int j = 0; j < TASKS; ++j)
+                    if (task[j].valid) {
+                        const uint8_t *row = (task[j].is_a ? pa : pb) + task[j].src;
+#pragma unroll
+                        for (int h = 0; h < 2; ++h)
+                            w[j][h] = *reinterpret_cast<const uint4 *>(
+                                row + ((((uint32_t)grp * 2 + h) ^ task[j].xr) << 4));
                     }
-                    uint8_t *ua = smem + OFF_UA + us * UA_BYTES;
-                    uint8_t *ub = smem + OFF_UB + us * UB_BYTES;
-                    uint4 w[TASKS];
 #pragma unroll
-                    for (int j = 0; j < TASKS; ++j)
-                        w[j] = *reinterpret_cast<const uint4 *>(
-                            (task[j].is_a ? pa : pb) + task[j].src + ((sub ^ task[j].xr) << 4));
+                for (int j = 0; j < TASKS; ++j) {
+                    if (!task[j].valid) continue;
+                    uint8_t *dst = task[j].is_a ? ua : ub;
 #pragma unroll
-                    for (int j = 0; j < TASKS; ++j) {
-                        uint8_t *dst = (task[j].is_a ? ua : ub) + task[j].dst;
-#pragma unroll
-                        for (int cc = 0; cc < 4; ++cc)
-                            *reinterpret_cast<uint4 *>(dst + task[j].chunk_off[cc]) =
-                                unpack_chunk(w[j], task[j].pow2[cc]);
+                    for (int h = 0; h < 2; ++h) {
+                        *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 0]) = spread4<0>(w[j][h]);
+                        *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 1]) = spread4<1>(w[j][h]);
+                        *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 2]) = spread4<2>(w[j][h]);
+                        *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 3]) = spread4<3>(w[j][h]);
                     }
-                    fence_proxy_async_smem();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(smem_u32(&ufull[us]));
                 }
-                if (!ok) break;
+                fence_proxy_async_smem();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(smem_u32(&pempty[ps]));
+                if (lane == 0) {
+                    mbar_arrive(smem_u32(&ufull[grp]));
+                    mbar_arrive(smem_u32(&pempty[ps]));
+                }
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&iempty[slot]));
         }
     } else {
         // ------------------------------------------------------- epilogue --
-        // The four epilogue warps meet at named barriers, so they must leave
-        // the loop together: a failure is recorded in a shared flag that is
-        // only read right after the first barrier of an item (every write to
-        // it happens before that barrier or between the second and third).
+        // The epilogue warps meet at named barriers, so they must leave the
+        // loop together: a failure is recorded in a shared flag that is only
+        // read right after the first barrier of an item (every write to it
+        // happens before that barrier or between the second and third).
         volatile int *epi_fail = reinterpret_cast<volatile int *>(smem + OFF_TMEM + 8);
         const int et = tid - FIRST_EPI_WARP * 32;
-        const int q = warp & 3;
+        const int ew = warp - FIRST_EPI_WARP;
+        const int q = warp & 3;             // TMEM lane quarter
+        const int colh = ew >> 2;           // chunks colh, colh + 2, colh + 4, colh + 6
         if (et == 0) *epi_fail = 0;
         named_bar_sync(1, EPI_THREADS);
         for (int qi = 0;; ++qi) {
@@ -333,11 +372,13 @@ k_ld_batch(const BatchParams bp) {
             if (*epi_fail || it.job < 0) break;
             const BatchJob &J = bp.jobs[it.job];
             const int ab = qi & 1;
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int bl = et + k * EPI_THREADS;
-                const int b = it.tb * BN + bl;
-                epi::store_col<MODE>(cols, bl, b < J.n ? J.bcB[b] : 0u, J.S);
+            {   // every column factor the chunks read; 0 past the tile and the task
+                const int b = it.tb * BN + et;
+                const uint32_t cb = (et < BN && b < J.n) ? J.bcB[b] : 0u;
+                if constexpr (MODE == R2_EXACT)
+                    epi::store_col_f32(colsf, et, cb, J.S);
+                else
+                    epi::store_col<MODE>(cols, et, cb, J.S);
             }
             named_bar_sync(1, EPI_THREADS);
             bool ready = mbar_wait(smem_u32(&accfull[ab]), (qi >> 1) & 1, limit, bp.status);
@@ -352,16 +393,31 @@ k_ld_batch(const BatchParams bp) {
                 tc_fence_after();
                 const int a = it.ta * BM + q * 32 + lane;
                 const bool a_ok = a < J.m;
-                const epi::ARow ra = epi::make_arow<MODE>(a_ok ? J.bcA[a] : 0u, J.S);
-                const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * BN);
+                const uint32_t ca = a_ok ? J.bcA[a] : 0u;
+                const epi::ARow ra = epi::make_arow<MODE>(ca, J.S);
+                const epi::ARowF raf = epi::make_arow_f32(ca, J.S);
+                const uint32_t tbase =
+                    tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)ab * ACC_STRIDE;
+                // columns past the tile's 240 B rows are read but not written
+                const int n_tile = it.tb * BN + BN < J.n ? it.tb * BN + BN : J.n;
+                const int dlo = diag_lo(J.symmetric, 0), dhi = diag_hi(0);
 #pragma unroll 1
-                for (int col0 = 0; col0 < BN; col0 += 32) {
+                for (int c = colh; c < 8; c += 2) {
                     uint32_t v[32];
                     __syncwarp();
-                    tc_ld_32x32b_x32(tbase + (uint32_t)col0, v);
-                    epi::chunk<MODE, COUNT_SHIFT>(v, ra, cols, col0, it.tb * BN + col0, a, a_ok,
-                                                  J.n, diag_lo(J.symmetric, 0), diag_hi(0), J.r2,
-                                                  J.ldr, J.counts, J.ldc, 0, J.S);
+                    tc_ld_32x32b_x32(tbase + (uint32_t)(c * 32), v);
+                    if constexpr (MODE == R2_EXACT) {
+                        epi::chunk_f32(v, tbase + (uint32_t)(c * 32), raf, colsf, c * 32,
+                                       it.tb * BN + c * 32, a, a_ok, n_tile, dlo, dhi, J.r2,
+                                       J.ldr, J.counts, J.ldc, 0, J.S);
+                    } else {
+#pragma unroll
+                        for (int t = 0; t < 32; ++t)     // F32 accumulator -> count
+                            v[t] = (uint32_t)__uint_as_float(v[t]);
+                        epi::chunk<MODE, 0>(v, ra, cols, c * 32, it.tb * BN + c * 32, a, a_ok,
+                                            n_tile, dlo, dhi, J.r2, J.ldr, J.counts, J.ldc, 0,
+                                            J.S);
+                    }
                 }
                 tc_fence_before();
                 __syncwarp();
@@ -369,7 +425,7 @@ k_ld_batch(const BatchParams bp) {
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&iempty[slot]));
-            named_bar_sync(1, EPI_THREADS);   // row factors may be rewritten
+            named_bar_sync(1, EPI_THREADS);   // column factors may be rewritten
         }
     }
 
@@ -411,6 +467,7 @@ cudaError_t launch_mode(const BatchParams &bp, int max_ctas, cudaStream_t st) {
 }  // namespace
 
 const KernelShape kBatchShape = {BM, BN, PW, BM, BN, 64};
+const int kBatchMaxSamples = 1 << 24;
 
 cudaError_t launch_batch(const BatchParams &bp, int r2_mode, int max_ctas, cudaStream_t st) {
     return r2_mode == R2_REFERENCE ? launch_mode<R2_REFERENCE>(bp, max_ctas, st)

@@ -314,9 +314,9 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
             tl.decode(tile, ta, tb);
             const int lim = (it + 1) * nu + UST;
             produce_until(lim < total_u ? lim : total_u);
-            if (wt < BN) {
+            if (wt < COLS_N) {   // every column factor the chunks read; 0 past the tile
                 const int b = tb * BN + wt;
-                const uint32_t cb = b < p.n ? p.bcB[b] : 0u;
+                const uint32_t cb = (wt < BN && b < p.n) ? p.bcB[b] : 0u;
                 if constexpr (MODE == R2_EXACT)
                     epi::store_col_f32(colsf, wt, cb, p.S);
                 else

@@ -88,7 +88,7 @@ static_assert(OFF_UB % 1024 == 0 && UB_BYTES % 1024 == 0 && OFF_PA % 1024 == 0 &
                   OFF_PB % 1024 == 0 && PB_TX <= PB_BYTES,
               "swizzled stages must start on 1024-byte boundaries");
 static_assert(ACC_STRIDE + BN <= SF_COL && SF_COL + 16 <= TMEM_COLS, "TMEM map");
-static_assert(TASKS == 2 && SUB == 2 && UST % 2 == 0 && EPILOGUE >= BN, "work split");
+static_assert(TASKS == 2 && SUB == 2 && UST % 2 == 0 && EPILOGUE == COLS_N, "work split");
 
 // One unpack task: one packed row (A or B) of the CTA, both 16-byte halves of
 // the 32 bytes (256 samples) a sub-stage takes from each 64-byte packed row.
@@ -324,9 +324,9 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             int ta, tb;
             tl.decode(pair + it * npairs, ta, tb);
             const int ab = it & 1;
-            if (et < BN) {
+            {   // every column factor the chunks read; 0 past the tile and the task
                 const int b = tb * BN + et;
-                const uint32_t cb = b < p.n ? p.bcB[b] : 0u;
+                const uint32_t cb = (et < BN && b < p.n) ? p.bcB[b] : 0u;
                 if constexpr (MODE == R2_EXACT)
                     epi::store_col_f32(colsf, et, cb, p.S);
                 else

@@ -165,6 +165,8 @@ long long tile_count(const Task &t, int bm, int bn, int b0, int b1) {
     const int tb0 = b0 / bn, tiles_b = (b1 - b0 + bn - 1) / bn;
     if (bm == 256 && bn == 240)
         return tc::TileList<256, 240>{(t.m + 255) / 256, tb0, tiles_b, t.symmetric, t.band}.count();
+    if (bm == 128 && bn == 240)
+        return tc::TileList<128, 240>{(t.m + 127) / 128, tb0, tiles_b, t.symmetric, t.band}.count();
     if (bm == 256 && bn == 256)
         return tc::TileList<256, 256>{(t.m + 255) / 256, tb0, tiles_b, t.symmetric, t.band}.count();
     if (bm == 128 && bn == 256)
@@ -997,10 +999,10 @@ int qld_cuda_ld_batch(qld_ctx *c, const qld_ld_args *jobs, int njobs, void *stre
             (a.lda & 1) || (a.ldb & 1) || a.ldr < a.m || (a.counts && a.ldc < a.m) || !a.A ||
             !a.B || !a.bcA || !a.bcB || !a.r2 || !aligned16(a.A) || !aligned16(a.B))
             return set_err(c, QLD_ERR_INVALID, "batch job %d: bad sizes, strides or pointers", j);
-        if ((long long)a.K * 64 > kMmaMaxSamples)
+        if ((long long)a.K * 64 > kBatchMaxSamples)
             return set_err(c, QLD_ERR_UNSUPPORTED,
                            "batch job %d: K*64 > %d samples (use qld_cuda_ld_device)", j,
-                           kMmaMaxSamples);
+                           kBatchMaxSamples);
         Task t{a.A, a.bcA, a.m, a.lda, a.B, a.bcB, a.n, a.ldb, a.K, a.S, a.symmetric, 0};
         tiles[j] = (a.m == 0 || a.n == 0) ? 0 : tile_count(t, ks.bm, ks.bn, 0, a.n);
         cost[j] = tiles[j] * (long long)a.K;

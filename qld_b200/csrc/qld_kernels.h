@@ -68,7 +68,8 @@ struct BatchParams {
     long long timeout_cycles;
 };
 
-extern const KernelShape kBatchShape;
+extern const KernelShape kBatchShape;   // 128 x 240 tiles, the 4-bit path
+extern const int kBatchMaxSamples;      // K * 64 limit of a batched task (2^24)
 
 // Persistent batched launch over all items of bp.jobs (max_ctas > 0 caps the grid).
 cudaError_t launch_batch(const BatchParams &bp, int r2_mode, int max_ctas, cudaStream_t st);

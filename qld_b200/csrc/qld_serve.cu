@@ -240,7 +240,7 @@ int launch_slot(qld_server *s, int si) {
         const Query &q = sl.qs[i];
         const int m = q.q.a1 - q.q.a0, n = q.q.b1 - q.q.b0;
         const int sym = (q.q.a0 == q.q.b0 && q.q.a1 == q.q.b1);
-        tiles[i] = tc::TileList<128, 256>{(m + 127) / 128, 0, (n + 255) / 256, sym, 0}.count();
+        tiles[i] = tc::TileList<128, 240>{(m + 127) / 128, 0, (n + 239) / 240, sym, 0}.count();
         cost[i] = tiles[i] * (long long)tables[q.q.table].K;
         order[i] = i;
     }
@@ -469,8 +469,8 @@ int qld_srv_add_table(qld_server *s, const uint64_t *A, const uint32_t *bc, int 
                       int *table_id) {
     if (!s || !A || !bc || !table_id || m < 1 || K < 1 || S < 1)
         return srv_err(s, QLD_ERR_INVALID, "bad table arguments");
-    if ((long long)K * 64 > kMmaMaxSamples)
-        return srv_err(s, QLD_ERR_UNSUPPORTED, "K*64 > %d samples", kMmaMaxSamples);
+    if ((long long)K * 64 > kBatchMaxSamples)
+        return srv_err(s, QLD_ERR_UNSUPPORTED, "K*64 > %d samples", kBatchMaxSamples);
     cudaSetDevice(s->device);
     Table T;
     T.m = m; T.K = K; T.S = S;

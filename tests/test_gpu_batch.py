@@ -69,8 +69,9 @@ def test_batch_matches_single_tasks_and_oracle(gpu_ctx, mode):
         gpu_ctx.sync(stream=st)
         batch_r2 = [j["r2"].clone() for j in jobs]
         batch_cnt = [j["counts"].clone() for j in jobs]
-        gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_MMA)
-        gpu_ctx.set_option(api.OPT_MMA_TILE, 128)
+        # the single-task 4-bit kernel does the batch's arithmetic (F32 counts,
+        # the same r^2 evaluation), so the r^2 bits must agree
+        gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_FP4)
         for j in jobs:
             j["r2"].fill_(-5.0)
             if j["m"] and j["n"]:
@@ -81,7 +82,6 @@ def test_batch_matches_single_tasks_and_oracle(gpu_ctx, mode):
     finally:
         gpu_ctx.set_option(api.OPT_R2_MODE, api.R2_EXACT)
         gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
-        gpu_ctx.set_option(api.OPT_MMA_TILE, 0)
     for j, (A, B, bcA, bcB, N, sym), r2b, cb in zip(jobs, host, batch_r2, batch_cnt):
         m, n = j["m"], j["n"]
         if not (m and n):
@@ -124,3 +124,53 @@ def test_batch_rejects_bad_job(gpu_ctx):
     with pytest.raises(api.QldError) as e:
         gpu_ctx.ld_batch(jobs)
     assert e.value.code == api.ERR_INVALID
+
+
+def test_batch_past_the_int8_limit(gpu_ctx):
+    """Tasks of 140,000 and 200,000 samples (past 131,071, the int8 kernels'
+    exact range) in one batch: counts exact, r^2 within the FP64 bar."""
+    dev = torch.device("cuda", 0)
+    jobs, host = [], []
+    for seed, (m, N, sym) in enumerate([(300, 140_000, True), (130, 200_000, False)]):
+        t, _ = synth.all_pairs_workload(m=m + (0 if sym else 90), n=N, seed=60 + seed)
+        T = t.numpy().view(np.uint64)
+        K = T.shape[1]
+        lda = K + (K & 1)
+        A, B = T[:m], (T[:m] if sym else T[m:])
+        dA = torch.zeros(m, lda, dtype=torch.int64, device=dev)
+        dA[:, :K] = torch.from_numpy(A.view(np.int64)).to(dev)
+        dB = dA
+        if not sym:
+            dB = torch.zeros(B.shape[0], lda, dtype=torch.int64, device=dev)
+            dB[:, :K] = torch.from_numpy(np.ascontiguousarray(B).view(np.int64)).to(dev)
+        bcA, bcB = oracle.bitcounts(A), oracle.bitcounts(B)
+        n = B.shape[0]
+        r2 = torch.full((n, m), -5.0, dtype=torch.float32, device=dev)
+        cnt = torch.zeros((n, m), dtype=torch.int32, device=dev)
+        jobs.append(dict(A=dA, bcA=torch.from_numpy(bcA.view(np.int32).copy()).to(dev), m=m,
+                         lda=lda, B=dB, bcB=torch.from_numpy(bcB.view(np.int32).copy()).to(dev),
+                         n=n, ldb=lda, K=K, S=N, symmetric=sym, r2=r2, ldr=m, counts=cnt, ldc=m))
+        host.append((A, B, bcA, bcB, N, sym))
+    st = torch.cuda.current_stream()
+    gpu_ctx.ld_batch(jobs, stream=st)
+    gpu_ctx.sync(stream=st)
+    for j, (A, B, bcA, bcB, N, sym) in zip(jobs, host):
+        n, m = j["n"], j["m"]
+        mask = lower_mask(n, m) if sym else np.ones((n, m), bool)
+        want_c = oracle.counts(A, B)
+        assert np.array_equal(j["counts"].cpu().numpy().view(np.uint32)[mask], want_c[mask])
+        assert_r2_close(j["r2"].cpu().numpy(), oracle.r2_exact(bcA, bcB, want_c, N), mask=mask)
+
+
+def test_batch_rejects_past_2_24_samples(gpu_ctx):
+    """K * 64 > 2^24: the F32 accumulators would round; refused before launch."""
+    dev = torch.device("cuda", 0)
+    K = (1 << 24) // 64 + 2
+    A = torch.zeros(2, K, dtype=torch.int64, device=dev)
+    bc = torch.zeros(2, dtype=torch.int32, device=dev)
+    r2 = torch.zeros(2, 2, dtype=torch.float32, device=dev)
+    job = dict(A=A, bcA=bc, m=2, lda=K, B=A, bcB=bc, n=2, ldb=K, K=K, S=K * 64, symmetric=True,
+               r2=r2, ldr=2, counts=None, ldc=2)
+    with pytest.raises(api.QldError) as e:
+        gpu_ctx.ld_batch([job])
+    assert e.value.code == api.ERR_UNSUPPORTED
