@@ -1,30 +1,37 @@
 // ld_batch.cu -- many independent LD tasks (region pairs of uneven SNP and
 // sample counts) in one persistent launch fed by a device work queue.
 //
-// Per-task arithmetic is that of the 4-bit kernels (ld_mxf4.cu): bits spread
-// to E2M1 with normalising UE8M0 scale factors (tcgen05.cuh: spread_e2m1),
-// tcgen05.mma.kind::mxf4 into F32 TMEM accumulators that hold the counts
-// exactly (K * 64 <= 2^24), fused r^2 epilogue of qLD gemm_cpu.c:343-404
-// (R2_EXACT in FP32 from the exact counts, epilogue.cuh: chunk_f32).  qLD
-// itself runs such task lists one task at a time (-inputList,
-// src/correlator/src/input_list.c:205-323 and correlate_function.c:59-83).
-// Here every 128 x 240 output tile of every task is a work item.  The device
-// job table holds per task its tensor maps, sizes and output, and the item
-// prefix offsets; items are numbered task by task (tasks sorted by cost on
-// the host, most expensive first).
+// Per-task arithmetic is that of the 4-bit kernels on SM pairs
+// (ld_mxf4_pair.cu): bits spread to E2M1 with normalising UE8M0 scale
+// factors (tcgen05.cuh: spread_e2m1), tcgen05.mma.cta_group::2.kind::mxf4
+// into F32 TMEM accumulators that hold the counts exactly (K * 64 <= 2^24),
+// fused r^2 epilogue of qLD gemm_cpu.c:343-404 (R2_EXACT in FP32 from the
+// exact counts, epilogue.cuh: chunk_f32).  qLD itself runs such task lists
+// one task at a time (-inputList, src/correlator/src/input_list.c:205-323
+// and correlate_function.c:59-83).  Here every 256 x 240 output tile of every
+// task is a work item, computed by a cluster of two CTAs (rank r: A rows
+// 128 r.., B rows 120 r.. of the tile).  The device job table holds per task
+// its tensor maps, sizes and output, and the item prefix offsets; items are
+// numbered task by task (tasks sorted by cost on the host, most expensive
+// first).
 //
-// Work queue: the producer thread of each CTA claims the next item with an
-// atomic ticket on a global counter, decodes it into (task, A tile, B tile),
-// pushes it into a 4-slot item ring in shared memory, and streams its packed
-// stages.  The MMA thread, the unpack warps and the epilogue warps pop the
-// same items in the same order; each of them releases a ring slot when done
-// with its item.  A ticket past the last item pushes an end marker.
+// Work queue: rank 0's producer thread claims the next item with an atomic
+// ticket on a global counter, decodes it into (task, A tile, B tile) and
+// writes it into the 4-slot item ring of both CTAs (the peer's copy through
+// st.shared::cluster, published by a cluster-scope release arrive).  In each
+// CTA the TMA thread, the unpack warps and the epilogue warps (and in rank 0
+// the MMA thread) pop the same items in the same order, and each releases
+// the slot on rank 0's barrier when done with its item.  A ticket past the
+// last item pushes an end marker.
 //
-// Roles (576 threads): warp 0 queue + TMA, warp 1 TMEM + MMA, warps 2-9
-// unpack in two groups taking alternate 256-sample stages (each thread whole
-// rows: conflict-free), warps 10-17 epilogue (two per TMEM lane quarter).
-// TMEM: two 240-column accumulators (columns 0 and 256) so a tile's epilogue
-// overlaps the next tile's MMAs, the scale factors at columns 496-511.
+// Roles per CTA (576 threads): warp 0 queue (rank 0) and TMA of the CTA's
+// rows, warp 1 TMEM and (rank 0) the MMAs, warps 2-9 unpack in two groups
+// taking alternate 256-sample stages (each thread whole rows), warps 10-17
+// epilogue (two per TMEM lane quarter).  TMEM: two 240-column accumulators
+// (columns 0 and 256), so a tile's epilogue overlaps the next tile's MMAs,
+// and the scale factors at columns 496-511.  Every wait is bounded and no
+// thread returns early: both CTAs meet at the cluster barriers at start and
+// end on every path.
 #include "epilogue.cuh"
 #include "qld_kernels.h"
 #include "tcgen05.cuh"
@@ -35,15 +42,17 @@ namespace {
 
 using namespace tc;
 
-constexpr int BM = 128, BN = 240;
+constexpr int BM = 256, BN = 240;           // work item: output tile of a pair
+constexpr int HM = 128, HN = 120;           // A and B rows held by each CTA
 constexpr int PW = 8;                       // packed words per row per packed stage
 constexpr int SUB = 2;                      // unpacked stages (256 samples) per packed stage
 constexpr int PST = 4;
-constexpr int UST = 2;                      // one unpacked stage per unpack group
-constexpr int PA_BYTES = BM * PW * 8;       // 8 KB
-constexpr int PB_BYTES = BN * PW * 8;       // 15 KB
-constexpr int UA_BYTES = BM * 128;          // 16 KB: 256 E2M1 per row
-constexpr int UB_BYTES = BN * 128;          // 30 KB
+constexpr int UST = 4;                      // two unpacked stages per unpack group
+constexpr int PA_BYTES = HM * PW * 8;       // 8 KB
+constexpr int PB_TX = HN * PW * 8;          // 7.5 KB delivered per stage
+constexpr int PB_BYTES = 8192;              // stage stride, 1024-byte aligned
+constexpr int UA_BYTES = HM * 128;          // 16 KB: 256 E2M1 per row
+constexpr int UB_BYTES = HN * 128;          // 15 KB
 constexpr int UNPACK_WARPS = 8;
 constexpr int GROUP_THREADS = UNPACK_WARPS * 32 / 2;
 constexpr int EPI_WARPS = 8;
@@ -51,7 +60,7 @@ constexpr int EPI_THREADS = EPI_WARPS * 32;
 constexpr int FIRST_UNPACK_WARP = 2;
 constexpr int FIRST_EPI_WARP = FIRST_UNPACK_WARP + UNPACK_WARPS;
 constexpr int THREADS = (FIRST_EPI_WARP + EPI_WARPS) * 32;   // 576
-constexpr int NROWS = BM + BN;                                // row tasks per stage
+constexpr int NROWS = HM + HN;                                // row tasks per stage
 constexpr int TASKS = (NROWS + GROUP_THREADS - 1) / GROUP_THREADS;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t ACC_STRIDE = 256;
@@ -59,8 +68,11 @@ constexpr uint32_t SF_COL = 496;
 constexpr uint32_t IDESC_EVEN = idesc_mxf4_sf(BM, BN, 0);   // k-steps 0, 2: scale bytes 0-1
 constexpr uint32_t IDESC_ODD = idesc_mxf4_sf(BM, BN, 2);    // k-steps 1, 3: scale bytes 2-3
 constexpr int COLS_N = 256;                                  // epilogue column factors (BN used)
+constexpr uint16_t BOTH = 0x3;                               // CTA mask of a commit to both ranks
 constexpr int QSLOTS = 4;                                    // item ring depth
-constexpr int ITEM_USERS = 1 + UNPACK_WARPS + EPI_WARPS;     // arrivals freeing a slot
+// arrivals on rank 0's slot-free barrier per item: rank 0's MMA thread,
+// unpack and epilogue warps; rank 1's TMA thread, unpack and epilogue warps
+constexpr int ITEM_USERS = 2 * (1 + UNPACK_WARPS + EPI_WARPS);
 
 constexpr int OFF_UA = 0;
 constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
@@ -75,14 +87,15 @@ constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
 constexpr int SMEM_BYTES = OFF_TMEM + 16 + 1024;
 static_assert(SMEM_BYTES <= 232448, "shared memory budget");
 static_assert(OFF_UB % 1024 == 0 && UB_BYTES % 1024 == 0 && OFF_PA % 1024 == 0 &&
-                  OFF_PB % 1024 == 0 && PB_BYTES % 1024 == 0,
+                  OFF_PB % 1024 == 0 && PB_TX <= PB_BYTES && OFF_ITEMS % 16 == 0,
               "swizzled stages must start on 1024-byte boundaries");
 static_assert(ACC_STRIDE + BN <= SF_COL && SF_COL + 16 <= TMEM_COLS, "TMEM map");
-static_assert(TASKS == 3 && SUB == 2 && UST == 2 && EPI_THREADS == COLS_N, "work split");
+static_assert(TASKS == 2 && SUB == 2 && UST % 2 == 0 && EPI_THREADS == COLS_N, "work split");
 
 struct Item {
     int job, ta, tb, np;   // job < 0: end of the queue
 };
+static_assert(sizeof(Item) == 16, "an item is one 16-byte record");
 
 // One unpack task: one packed row, both 16-byte halves of the 32 bytes a
 // 256-sample stage takes from it (ld_mxf4_pair.cu: RowTask).
@@ -116,7 +129,7 @@ __device__ __forceinline__ Item decode_item(const BatchJob *jobs, int njobs, lon
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
 k_ld_batch(const BatchParams bp) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -133,10 +146,18 @@ k_ld_batch(const BatchParams bp) {
     const epi::Cols cols(smem + OFF_ROWS, COLS_N);
     const epi::ColsF colsf(smem + OFF_ROWS, COLS_N);   // R2_EXACT: FP32 factors
 
-    if (grid_failed(bp.status)) return;
+    const uint32_t rank = cluster_rank();
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const long long limit = bp.timeout_cycles;
+    // the item ring is written by rank 0; rank 1 reads it under cluster-scope acquire
+    auto wait_item = [&](int qi) {
+        const uint32_t b = smem_u32(&ifull[qi % QSLOTS]);
+        const uint32_t par = (uint32_t)(qi / QSLOTS) & 1u;
+        return rank == 0 ? mbar_wait(b, par, limit, bp.status)
+                         : mbar_wait_acq_cluster(b, par, limit, bp.status);
+    };
+    auto release_item = [&](int qi) { mbar_arrive_rank(smem_u32(&iempty[qi % QSLOTS]), 0); };
 
     if (tid == 0) {
         for (int s = 0; s < PST; ++s) {
@@ -144,12 +165,12 @@ k_ld_batch(const BatchParams bp) {
             mbar_init(smem_u32(&pempty[s]), UNPACK_WARPS);   // both groups, once each
         }
         for (int s = 0; s < UST; ++s) {
-            mbar_init(smem_u32(&ufull[s]), UNPACK_WARPS / 2);   // one group per stage
+            mbar_init(smem_u32(&ufull[s]), UNPACK_WARPS);    // one group in each CTA
             mbar_init(smem_u32(&uempty[s]), 1);
         }
         for (int s = 0; s < 2; ++s) {
             mbar_init(smem_u32(&accfull[s]), 1);
-            mbar_init(smem_u32(&accempty[s]), EPI_WARPS);
+            mbar_init(smem_u32(&accempty[s]), 2 * EPI_WARPS);   // both CTAs' epilogues
         }
         mbar_init(smem_u32(mma_done), 1);
         for (int s = 0; s < QSLOTS; ++s) {
@@ -159,46 +180,60 @@ k_ld_batch(const BatchParams bp) {
         fence_barrier_init();
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(tmem_slot)),
                      "r"(TMEM_COLS)
                      : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    // the spread's scale factors in columns SF_COL.. of every lane (warps 2-5
-    // cover the four TMEM lane quarters)
+    // the spread's scale factors in columns SF_COL.. of every lane, in both
+    // CTAs (warps 2-5 cover the four TMEM lane quarters)
     if (warp >= FIRST_UNPACK_WARP && warp < FIRST_UNPACK_WARP + 4)
         tc_st_32x32b_x16_fill(tmem + ((uint32_t)((warp & 3) * 32) << 16) + SF_COL, kSpreadScales);
     tc_fence_before();
-    __syncthreads();
+    // barrier initialisation and both CTAs' scale factors, cluster-wide
+    cluster_sync_all();
     tc_fence_after();
 
     if (warp == 0) {
-        // --------------------------------------- work queue + TMA producer --
+        // ------------------------------- work queue (rank 0) + TMA producer --
         if (lane == 0) {
             int gp = 0;
             bool ok = true;
             for (int qi = 0;; ++qi) {
                 const int slot = qi % QSLOTS;
-                if (qi >= QSLOTS && !mbar_wait(smem_u32(&iempty[slot]), ((qi / QSLOTS) - 1) & 1,
-                                               limit, bp.status)) {
-                    flag_error(bp.status, ST_TIMEOUT_EMPTY);
-                    ok = false;
-                }
-                const long long g =
-                    ok ? (long long)atomicAdd(bp.queue, 1ull) : (long long)bp.nitems;
                 Item it;
-                if (g < bp.nitems) it = decode_item(bp.jobs, bp.njobs, g);
-                else it.job = -1, it.ta = it.tb = it.np = 0;
-                items[slot] = it;
-                mbar_arrive(smem_u32(&ifull[slot]));   // release: the item is visible
+                if (rank == 0) {
+                    if (qi >= QSLOTS &&
+                        !mbar_wait_acq_cluster(smem_u32(&iempty[slot]), ((qi / QSLOTS) - 1) & 1,
+                                               limit, bp.status)) {
+                        flag_error(bp.status, ST_TIMEOUT_EMPTY);
+                        ok = false;
+                    }
+                    const long long g =
+                        ok ? (long long)atomicAdd(bp.queue, 1ull) : (long long)bp.nitems;
+                    if (g < bp.nitems) it = decode_item(bp.jobs, bp.njobs, g);
+                    else it.job = -1, it.ta = it.tb = it.np = 0;
+                    items[slot] = it;
+                    mbar_arrive(smem_u32(&ifull[slot]));   // release: the item is visible
+                    st_rank_and_arrive(smem_u32(&items[slot]),
+                                       make_int4(it.job, it.ta, it.tb, it.np),
+                                       smem_u32(&ifull[slot]), 1);
+                } else {
+                    if (!wait_item(qi)) {
+                        flag_error(bp.status, ST_TIMEOUT_FULL);
+                        break;
+                    }
+                    it = items[slot];
+                }
                 if (it.job < 0) break;
                 const BatchJob &J = bp.jobs[it.job];
-                for (int kp = 0; kp < it.np; ++kp, ++gp) {
+                const int ra = it.ta * BM + (int)rank * HM, rb = it.tb * BN + (int)rank * HN;
+                for (int kp = 0; kp < it.np && ok; ++kp, ++gp) {
                     const int s = gp % PST;
                     if (gp >= PST && !mbar_wait(smem_u32(&pempty[s]), ((gp / PST) - 1) & 1,
                                                 limit, bp.status)) {
@@ -207,11 +242,13 @@ k_ld_batch(const BatchParams bp) {
                         break;
                     }
                     const uint32_t fb = smem_u32(&pfull[s]);
-                    mbar_arrive_expect_tx(fb, PA_BYTES + PB_BYTES);
-                    tma_load_2d(smem_u32(smem + OFF_PA + s * PA_BYTES), &J.tmA, kp * PW,
-                                it.ta * BM, fb);
-                    tma_load_2d(smem_u32(smem + OFF_PB + s * PB_BYTES), &J.tmB, kp * PW,
-                                it.tb * BN, fb);
+                    mbar_arrive_expect_tx(fb, PA_BYTES + PB_TX);
+                    tma_load_2d(smem_u32(smem + OFF_PA + s * PA_BYTES), &J.tmA, kp * PW, ra, fb);
+                    tma_load_2d(smem_u32(smem + OFF_PB + s * PB_BYTES), &J.tmB, kp * PW, rb, fb);
+                }
+                if (rank == 1) {
+                    release_item(qi);
+                    if (!ok) break;
                 }
             }
             for (int g = gp > PST ? gp - PST : 0; g < gp; ++g)
@@ -221,14 +258,14 @@ k_ld_batch(const BatchParams bp) {
                 }
         }
     } else if (warp == 1) {
-        // ----------------------------------------------------- MMA issuer --
-        if (lane == 0) {
+        // ------------------------------------------- MMA issuer (rank 0) --
+        if (lane == 0 && rank == 0) {
             const uint32_t sf = tmem + SF_COL;
             int gu = 0, it_n = 0;
             bool ok = true;
             for (int qi = 0; ok; ++qi, ++it_n) {
                 const int slot = qi % QSLOTS;
-                if (!mbar_wait(smem_u32(&ifull[slot]), (qi / QSLOTS) & 1, limit, bp.status)) {
+                if (!wait_item(qi)) {
                     flag_error(bp.status, ST_TIMEOUT_UNPACK);
                     break;
                 }
@@ -254,27 +291,27 @@ k_ld_batch(const BatchParams bp) {
                     const uint32_t b0 = smem_u32(smem + OFF_UB + s * UB_BYTES);
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk)
-                        tc_mma_mxf4(d, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32),
-                                    (kk & 1) ? IDESC_ODD : IDESC_EVEN, (u > 0 || kk > 0) ? 1u : 0u,
-                                    sf, sf);
-                    tc_commit(smem_u32(&uempty[s]));
+                        tc_mma_mxf4_pair(d, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32),
+                                         (kk & 1) ? IDESC_ODD : IDESC_EVEN,
+                                         (u > 0 || kk > 0) ? 1u : 0u, sf, sf);
+                    tc_commit_pair(smem_u32(&uempty[s]), BOTH);
                 }
-                tc_commit(smem_u32(&accfull[ab]));
-                mbar_arrive(smem_u32(&iempty[slot]));
+                tc_commit_pair(smem_u32(&accfull[ab]), BOTH);
+                release_item(qi);
             }
-            tc_commit(smem_u32(mma_done));
+            tc_commit_pair(smem_u32(mma_done), BOTH);
         }
     } else if (warp < FIRST_EPI_WARP) {
         // --------------------------------------------------------- unpack --
-        // group g takes sub-stage g of every packed stage (unpacked stage g)
+        // group g takes sub-stage g of every packed stage
         const int grp = (warp - FIRST_UNPACK_WARP) / (UNPACK_WARPS / 2);
         const int wt = ((warp - FIRST_UNPACK_WARP) % (UNPACK_WARPS / 2)) * 32 + lane;
         RowTask task[TASKS];
 #pragma unroll
         for (int j = 0; j < TASKS; ++j) {
-            const int row = wt + j * GROUP_THREADS;   // over 128 A + 240 B rows
-            const bool isA = row < BM;
-            const int r = isA ? row : row - BM;
+            const int row = wt + j * GROUP_THREADS;   // over 128 A + 120 B rows
+            const bool isA = row < HM;
+            const int r = isA ? row : row - HM;
             task[j].valid = row < NROWS;
             task[j].is_a = isA;
             task[j].src = (uint32_t)(r * 64);
@@ -283,21 +320,17 @@ k_ld_batch(const BatchParams bp) {
             for (int c = 0; c < 8; ++c)
                 task[j].off[c] = (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
         }
-        uint8_t *ua = smem + OFF_UA + grp * UA_BYTES;
-        uint8_t *ub = smem + OFF_UB + grp * UB_BYTES;
-        int gp = 0, nst = 0;   // packed stages seen; stages this group unpacked
+        int gp = 0;
         bool ok = true;
         for (int qi = 0; ok; ++qi) {
-            const int slot = qi % QSLOTS;
-            const bool got_item =
-                mbar_wait(smem_u32(&ifull[slot]), (qi / QSLOTS) & 1, limit, bp.status);
+            const bool got_item = wait_item(qi);
             if (!__all_sync(0xffffffffu, got_item)) {
                 if (lane == 0) flag_error(bp.status, ST_TIMEOUT_FULL);
                 break;
             }
-            const Item it = items[slot];
+            const Item it = items[qi % QSLOTS];
             if (it.job < 0) break;
-            for (int kp = 0; kp < it.np; ++kp, ++gp, ++nst) {
+            for (int kp = 0; kp < it.np; ++kp, ++gp) {
                 const int ps = gp % PST;
                 const bool got = mbar_wait(smem_u32(&pfull[ps]), (gp / PST) & 1, limit, bp.status);
                 if (!__all_sync(0xffffffffu, got)) {
@@ -305,8 +338,10 @@ k_ld_batch(const BatchParams bp) {
                     ok = false;
                     break;
                 }
-                const bool freed = nst == 0 || mbar_wait(smem_u32(&uempty[grp]), (nst - 1) & 1,
-                                                         limit, bp.status);
+                const int gu = gp * SUB + grp;
+                const int us = gu % UST;
+                const bool freed = gu < UST || mbar_wait(smem_u32(&uempty[us]),
+                                                         ((gu / UST) - 1) & 1, limit, bp.status);
                 if (!__all_sync(0xffffffffu, freed)) {
                     if (lane == 0) flag_error(bp.status, ST_TIMEOUT_MMA);
                     ok = false;
@@ -314,6 +349,8 @@ k_ld_batch(const BatchParams bp) {
                 }
                 const uint8_t *pa = smem + OFF_PA + ps * PA_BYTES;
                 const uint8_t *pb = smem + OFF_PB + ps * PB_BYTES;
+                uint8_t *ua = smem + OFF_UA + us * UA_BYTES;
+                uint8_t *ub = smem + OFF_UB + us * UB_BYTES;
                 uint4 w[TASKS][2];
 #pragma unroll
                 for (int j = 0; j < TASKS; ++j)
@@ -339,12 +376,12 @@ k_ld_batch(const BatchParams bp) {
                 fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) {
-                    mbar_arrive(smem_u32(&ufull[grp]));
+                    mbar_arrive_rank(smem_u32(&ufull[us]), 0);
                     mbar_arrive(smem_u32(&pempty[ps]));
                 }
             }
             __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&iempty[slot]));
+            if (lane == 0) release_item(qi);
         }
     } else {
         // ------------------------------------------------------- epilogue --
@@ -360,14 +397,12 @@ k_ld_batch(const BatchParams bp) {
         if (et == 0) *epi_fail = 0;
         named_bar_sync(1, EPI_THREADS);
         for (int qi = 0;; ++qi) {
-            const int slot = qi % QSLOTS;
-            const bool got_item =
-                mbar_wait(smem_u32(&ifull[slot]), (qi / QSLOTS) & 1, limit, bp.status);
+            const bool got_item = wait_item(qi);
             if (!__all_sync(0xffffffffu, got_item) && lane == 0) {
                 flag_error(bp.status, ST_TIMEOUT_FULL);
                 *epi_fail = 1;
             }
-            const Item it = items[slot];
+            const Item it = items[qi % QSLOTS];
             named_bar_sync(1, EPI_THREADS);
             if (*epi_fail || it.job < 0) break;
             const BatchJob &J = bp.jobs[it.job];
@@ -391,7 +426,7 @@ k_ld_batch(const BatchParams bp) {
             } else {
                 __syncwarp();
                 tc_fence_after();
-                const int a = it.ta * BM + q * 32 + lane;
+                const int a = it.ta * BM + (int)rank * HM + q * 32 + lane;
                 const bool a_ok = a < J.m;
                 const uint32_t ca = a_ok ? J.bcA[a] : 0u;
                 const epi::ARow ra = epi::make_arow<MODE>(ca, J.S);
@@ -421,28 +456,35 @@ k_ld_batch(const BatchParams bp) {
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(smem_u32(&accempty[ab]));
+                if (lane == 0) mbar_arrive_rank(smem_u32(&accempty[ab]), 0);
             }
             __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&iempty[slot]));
+            if (lane == 0) release_item(qi);
             named_bar_sync(1, EPI_THREADS);   // column factors may be rewritten
         }
     }
 
+    // Teardown: rank 0's last commit arrives on mma_done in both CTAs;
+    // neither CTA frees the pair's TMEM or exits while the other may still
+    // touch its shared memory.
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
         if (!mbar_wait(smem_u32(mma_done), 0, limit, nullptr))
             flag_error(bp.status, ST_TIMEOUT_MMA);
         __syncwarp();
+    }
+    tc_fence_before();
+    cluster_sync_all();
+    if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                      "r"(TMEM_COLS)
                      : "memory");
     }
 }
 
-int g_sm_count = 0;
+int g_max_pairs = 0;
 
 template <int MODE>
 cudaError_t launch_mode(const BatchParams &bp, int max_ctas, cudaStream_t st) {
@@ -450,23 +492,33 @@ cudaError_t launch_mode(const BatchParams &bp, int max_ctas, cudaStream_t st) {
     cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     if (e != cudaSuccess) return e;
-    if (g_sm_count == 0) {
-        int dev = 0;
+    if (g_max_pairs == 0) {
+        int dev = 0, sms = 0;
         if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-        if ((e = cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev)) !=
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) !=
             cudaSuccess)
             return e;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2 * (sms / 2), 1, 1);
+        cfg.blockDim = dim3(THREADS, 1, 1);
+        cfg.dynamicSmemBytes = SMEM_BYTES;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess || n <= 0) {
+            (void)cudaGetLastError();
+            n = sms / 2;
+        }
+        g_max_pairs = n;
     }
-    long long grid = bp.nitems < g_sm_count ? bp.nitems : g_sm_count;
-    if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
-    if (grid <= 0) return cudaSuccess;
-    kern<<<(int)grid, THREADS, SMEM_BYTES, st>>>(bp);
+    long long pairs = bp.nitems < g_max_pairs ? bp.nitems : g_max_pairs;
+    if (max_ctas > 0 && 2 * pairs > max_ctas) pairs = max_ctas / 2;
+    if (pairs <= 0) return cudaSuccess;
+    kern<<<(int)(2 * pairs), THREADS, SMEM_BYTES, st>>>(bp);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-const KernelShape kBatchShape = {BM, BN, PW, BM, BN, 64};
+const KernelShape kBatchShape = {BM, BN, PW, HM, HN, 64};
 const int kBatchMaxSamples = 1 << 24;
 
 cudaError_t launch_batch(const BatchParams &bp, int r2_mode, int max_ctas, cudaStream_t st) {

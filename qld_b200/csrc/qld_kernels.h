@@ -68,7 +68,7 @@ struct BatchParams {
     long long timeout_cycles;
 };
 
-extern const KernelShape kBatchShape;   // 128 x 240 tiles, the 4-bit path
+extern const KernelShape kBatchShape;   // 256 x 240 tiles on SM pairs, the 4-bit path
 extern const int kBatchMaxSamples;      // K * 64 limit of a batched task (2^24)
 
 // Persistent batched launch over all items of bp.jobs (max_ctas > 0 caps the grid).

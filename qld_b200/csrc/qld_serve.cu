@@ -240,7 +240,7 @@ int launch_slot(qld_server *s, int si) {
         const Query &q = sl.qs[i];
         const int m = q.q.a1 - q.q.a0, n = q.q.b1 - q.q.b0;
         const int sym = (q.q.a0 == q.q.b0 && q.q.a1 == q.q.b1);
-        tiles[i] = tc::TileList<128, 240>{(m + 127) / 128, 0, (n + 239) / 240, sym, 0}.count();
+        tiles[i] = tc::TileList<256, 240>{(m + 255) / 256, 0, (n + 239) / 240, sym, 0}.count();
         cost[i] = tiles[i] * (long long)tables[q.q.table].K;
         order[i] = i;
     }

@@ -158,6 +158,41 @@ __device__ __forceinline__ void mbar_arrive_rank(uint32_t bar, uint32_t rank) {
         : "memory");
 }
 
+// Hand a 16-byte record to CTA `rank`: store it at the same shared-memory
+// offset there, then arrive on that CTA's mbarrier `bar` with cluster-scope
+// release, so a waiter there that acquires at cluster scope sees the record.
+__device__ __forceinline__ void st_rank_and_arrive(uint32_t dst, int4 v, uint32_t bar,
+                                                   uint32_t rank) {
+    asm volatile(
+        "{\n\t.reg .b32 rd, rb;\n\t"
+        "mapa.shared::cluster.u32 rd, %0, %5;\n\t"
+        "mapa.shared::cluster.u32 rb, %6, %5;\n\t"
+        "st.shared::cluster.v4.u32 [rd], {%1, %2, %3, %4};\n\t"
+        "mbarrier.arrive.release.cluster.shared::cluster.b64 _, [rb];\n\t}"
+        ::"r"(dst), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "r"(rank), "r"(bar)
+        : "memory");
+}
+
+// mbar_wait with cluster-scope acquire (pairs with st_rank_and_arrive).
+__device__ __forceinline__ bool mbar_wait_acq_cluster(uint32_t bar, uint32_t parity,
+                                                      long long limit,
+                                                      const unsigned *status) {
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity), "r"(20000u)
+            : "memory");
+        if (ok) return true;
+        if (clock64() - t0 > limit) return false;
+        if (status && *((volatile const unsigned *)status) != 0u) return false;
+    }
+}
+
 __device__ __forceinline__ void tc_mma_mxf4_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
                                                  uint32_t idesc, uint32_t accumulate,
                                                  uint32_t sfa, uint32_t sfb) {
