@@ -49,7 +49,7 @@ constexpr int BM = 256, BN = 240;        // output tile of a pair
 constexpr int HM = 128, HN = 120;        // A and B rows held by each CTA
 constexpr int PW = 8;                    // packed words per row per packed stage
 constexpr int SUB = 2;                   // unpacked stages (256 samples) per packed stage
-constexpr int PST = 4;
+constexpr int PST = 5;                      // packed stages: ~2.8 us of MMA work in flight
 constexpr int UST = 4;
 constexpr int PA_BYTES = HM * PW * 8;    // 8 KB
 constexpr int PB_TX = HN * PW * 8;       // 7.5 KB delivered per stage
