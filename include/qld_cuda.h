@@ -337,6 +337,32 @@ int qld_cuda_measure_popc_peak(qld_ctx *ctx, double *bitops_per_s);
  * denominator of those kernels' roofline.  Runs ~10 ms. */
 int qld_cuda_measure_mma_peak(qld_ctx *ctx, int kernel, double *ops_per_s);
 
+/*
+ * Autotuner: measures every counts kernel that is exact for the shape
+ * (popcount; int8 MMA with 128- and 256-row tiles while K * 64 <= 131,071;
+ * 4-bit MMA on single SMs and on SM pairs while K * 64 <= 2^24) on a
+ * synthetic task of m x n SNPs (n = m when `symmetric`) and K words, and
+ * records the fastest for the task's shape class: floor(log2) of m, n and K
+ * and single versus two regions.  From then on QLD_KERNEL_AUTO uses the
+ * recorded kernel and tile option for tasks of that class (explicit
+ * QLD_OPT_MMA_TILE / QLD_OPT_SM_PAIR values still win; band tasks and
+ * untuned classes keep the built-in rule: the 4-bit kernel on SM pairs
+ * while exact, else popcount).  Sides above 16,384 are measured at 16,384.
+ * Outputs (each may be NULL): the kernel (QLD_KERNEL_*), its tile option
+ * (MMA tile rows, SMs per 4-bit tile, 0 for popcount) and the time of one
+ * launch in ms.  Uses the context's device buffers; synchronous.  No
+ * counterpart in the reference, which fixes its BLIS micro-kernel and
+ * blocking at build time (src/correlator/include/header.h:80-87).
+ */
+int qld_cuda_autotune(qld_ctx *ctx, int m, int n, int K, int symmetric, int *kernel,
+                      int *option, float *ms);
+/* The tuning table as text ("qld-tune 1", then one line per shape class:
+ * log2 m, log2 n, log2 K, single region (0/1), kernel, option, ms).  Loading
+ * adds to (and overrides entries of) the context's table; a malformed file
+ * changes nothing and returns QLD_ERR_INVALID. */
+int qld_cuda_tune_save(qld_ctx *ctx, const char *path);
+int qld_cuda_tune_load(qld_ctx *ctx, const char *path);
+
 #ifdef __cplusplus
 }
 #endif

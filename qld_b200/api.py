@@ -37,7 +37,7 @@ EXPORTED = (
     "qld_cuda_ld_band_device", "qld_cuda_sync",
     "qld_cuda_host_alloc",
     "qld_cuda_host_free", "qld_cuda_get_stats", "qld_cuda_measure_popc_peak",
-    "qld_cuda_measure_mma_peak",
+    "qld_cuda_measure_mma_peak", "qld_cuda_autotune", "qld_cuda_tune_save", "qld_cuda_tune_load",
     "qld_srv_create", "qld_srv_add_table", "qld_srv_submit", "qld_srv_poll", "qld_srv_fetch",
     "qld_srv_release", "qld_srv_destroy", "qld_srv_last_error",
 )
@@ -130,6 +130,10 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.qld_cuda_get_stats.argtypes = [vp, ct.POINTER(_Stats), i]
     lib.qld_cuda_measure_popc_peak.argtypes = [vp, ct.POINTER(ct.c_double)]
     lib.qld_cuda_measure_mma_peak.argtypes = [vp, i, ct.POINTER(ct.c_double)]
+    ip = ct.POINTER(ct.c_int)
+    lib.qld_cuda_autotune.argtypes = [vp, i, i, i, i, ip, ip, ct.POINTER(ct.c_float)]
+    lib.qld_cuda_tune_save.argtypes = [vp, ct.c_char_p]
+    lib.qld_cuda_tune_load.argtypes = [vp, ct.c_char_p]
     lib.qld_srv_create.argtypes = [i, ct.c_size_t, i, ct.POINTER(vp)]
     lib.qld_srv_add_table.argtypes = [vp, vp, vp, i, i, i, ct.POINTER(i)]
     lib.qld_srv_submit.argtypes = [vp, ct.POINTER(_Query), ct.POINTER(ll)]
@@ -202,6 +206,22 @@ class Context:
         v = ct.c_double()
         self._check(self.lib.qld_cuda_measure_popc_peak(self.h, ct.byref(v)))
         return v.value
+
+    def autotune(self, m: int, n: int, K: int, symmetric: bool = True):
+        """Time every exact counts kernel on a synthetic m x n x K task and make
+        the fastest the automatic choice for its shape class; returns
+        (kernel, option, ms per launch)."""
+        k, o, t = ct.c_int(), ct.c_int(), ct.c_float()
+        self._check(self.lib.qld_cuda_autotune(self.h, int(m), int(n), int(K),
+                                               int(bool(symmetric)), ct.byref(k), ct.byref(o),
+                                               ct.byref(t)))
+        return k.value, o.value, t.value
+
+    def tune_save(self, path: str):
+        self._check(self.lib.qld_cuda_tune_save(self.h, str(path).encode()))
+
+    def tune_load(self, path: str):
+        self._check(self.lib.qld_cuda_tune_load(self.h, str(path).encode()))
 
     def measure_mma_peak(self, kernel: int) -> float:
         """Measured dense tensor-pipe rate in ops/s (2 per multiply-accumulate)

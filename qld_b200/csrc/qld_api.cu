@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <utility>
 #include <vector>
 
@@ -34,6 +35,14 @@ struct HostBuf {   // pinned
     size_t bytes = 0;
 };
 
+// One autotuned choice of counts kernel: the variant, its tile option
+// (QLD_OPT_MMA_TILE rows for the int8 kernels, QLD_OPT_SM_PAIR SMs per tile
+// for the 4-bit kernel, 0 for popc) and the measured time per launch.
+struct TuneChoice {
+    int kernel, option;
+    float ms;
+};
+
 }  // namespace
 
 struct qld_ctx {
@@ -52,6 +61,7 @@ struct qld_ctx {
     int band_rows = 4096;
     int mma_tile = 0;                 // 0: per shape, else 128 or 256
     int sm_pair = 0;                  // 4-bit kernel: 0 per shape, 1 or 2 SMs per tile
+    std::map<long long, TuneChoice> tune;   // qld_cuda_autotune results by shape class
     long long timeout_cycles = 4000000000LL;  // ~2 s at boost clock
     DevBuf dA, dB, dbcA, dbcB, dOut[2], dCnt[2];
     DevBuf dJobs, dQueue;             // batched launches: job table, ticket counter
@@ -153,12 +163,43 @@ struct Task {
 bool mma_exact_for(const Task &t) { return (long long)t.K * 64 <= kMmaMaxSamples; }
 bool fp4_exact_for(const Task &t) { return (long long)t.K * 64 <= kMxf4MaxSamples; }
 
+// Shape class of a task for the autotuner's table: floor(log2) of m, n and
+// K, and the kind (two regions, single region, band).  Tasks in one class
+// differ in size by less than 2x on every side.
+int ilog2(long long x) {
+    int r = 0;
+    while (x > 1) { x >>= 1; ++r; }
+    return r;
+}
+long long tune_key(int m, int n, int K, int kind) {
+    return ((long long)ilog2(m) << 24) | ((long long)ilog2(n) << 16) |
+           ((long long)ilog2(K) << 8) | (long long)kind;
+}
+int task_kind(const Task &t) { return t.band > 0 ? 2 : (t.symmetric ? 1 : 0); }
+
+bool exact_for(int kernel, const Task &t);
+
+// The autotuned choice for the task's shape class, when the kernel option is
+// automatic, the class was tuned, and the tuned kernel is exact for the task.
+const TuneChoice *tuned_for(qld_ctx *c, const Task &t) {
+    if (c->kernel != QLD_KERNEL_AUTO || c->tune.empty()) return nullptr;
+    auto it = c->tune.find(tune_key(t.m, t.n, t.K, task_kind(t)));
+    if (it == c->tune.end() || !exact_for(it->second.kernel, t)) return nullptr;
+    return &it->second;
+}
+
 // Per-shape variant: the 4-bit tensor-core kernel wherever its F32
 // accumulators stay exact (K * 64 <= 2^24 samples: measured faster than the
 // i8 kernels on large and small tasks alike), the popcount kernel otherwise.
 int choose_kernel(qld_ctx *c, const Task &t) {
-    (void)c;
+    if (const TuneChoice *tc = tuned_for(c, t)) return tc->kernel;
     return fp4_exact_for(t) ? QLD_KERNEL_FP4 : QLD_KERNEL_POPC;
+}
+
+bool exact_for(int kernel, const Task &t) {
+    if (kernel == QLD_KERNEL_MMA) return mma_exact_for(t);
+    if (kernel == QLD_KERNEL_FP4) return fp4_exact_for(t);
+    return kernel == QLD_KERNEL_POPC;
 }
 
 long long tile_count(const Task &t, int bm, int bn, int b0, int b1) {
@@ -180,6 +221,8 @@ long long tile_count(const Task &t, int bm, int bn, int b0, int b1) {
 const KernelShape &mma_shape(qld_ctx *c, const Task &t, int b0, int b1) {
     if (c->mma_tile == 128) return kMmaShape;
     if (c->mma_tile == 256) return kMmaWideShape;
+    if (const TuneChoice *tc = tuned_for(c, t))
+        if (tc->kernel == QLD_KERNEL_MMA) return tc->option == 256 ? kMmaWideShape : kMmaShape;
     return tile_count(t, 256, 256, b0, b1) >= 4LL * c->sm_count ? kMmaWideShape : kMmaShape;
 }
 
@@ -189,7 +232,10 @@ const KernelShape &mma_shape(qld_ctx *c, const Task &t, int b0, int b1) {
 // faster one for every task size measured (a single region of 29,817 SNPs x
 // 16,622 samples: 2.63 ms against 3.33 ms).
 const KernelShape &fp4_shape(qld_ctx *c, const Task &t, int b0, int b1) {
-    (void)t; (void)b0; (void)b1;
+    (void)b0; (void)b1;
+    if (c->sm_pair == 0)
+        if (const TuneChoice *tc = tuned_for(c, t))
+            if (tc->kernel == QLD_KERNEL_FP4) return tc->option == 1 ? kMxf4Shape : kMxf4PairShape;
     return c->sm_pair == 1 ? kMxf4Shape : kMxf4PairShape;
 }
 
@@ -375,6 +421,52 @@ int stage_tables(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, cons
 }  // namespace
 
 // ================================================================== C ABI ==
+
+namespace {
+
+// Autotuner inputs: pseudo-random packed rows (splitmix64 of the word index,
+// zero past word K) and their bit counts, so the tuned kernels run on
+// consistent data.
+__global__ void k_tune_fill(uint64_t *T, long long rows, int K, long long ld, uint64_t seed) {
+    const long long n = rows * ld;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        uint64_t z = seed + (uint64_t)i * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        T[i] = (i % ld) < K ? (z ^ (z >> 31)) : 0ull;
+    }
+}
+
+__global__ void k_tune_bc(const uint64_t *T, long long rows, int K, long long ld, uint32_t *bc) {
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < rows;
+         r += (long long)gridDim.x * blockDim.x) {
+        uint32_t c = 0;
+        for (int w = 0; w < K; ++w) c += (uint32_t)__popcll(T[r * ld + w]);
+        bc[r] = c;
+    }
+}
+
+// Puts the context's kernel options and statistics back when the tuner
+// returns, on every path.
+struct OptionGuard {
+    qld_ctx *c;
+    int kernel, mma_tile, sm_pair;
+    qld_stats stats;
+    explicit OptionGuard(qld_ctx *ctx)
+        : c(ctx), kernel(ctx->kernel), mma_tile(ctx->mma_tile), sm_pair(ctx->sm_pair),
+          stats(ctx->stats) {}
+    ~OptionGuard() {
+        c->kernel = kernel;
+        c->mma_tile = mma_tile;
+        c->sm_pair = sm_pair;
+        c->stats = stats;
+    }
+};
+
+constexpr int kTuneMaxSide = 16384;   // the tuner measures at most 16,384 x 16,384
+
+}  // namespace
 
 extern "C" {
 
@@ -1056,7 +1148,7 @@ int qld_cuda_ld_batch(qld_ctx *c, const qld_ld_args *jobs, int njobs, void *stre
     if (e1) CUDA_TRY(c, cudaEventRecord(e1, st));
     c->stats.counts_launches++;
     c->stats.kernel_launches++;
-    c->stats.last_kernel = QLD_KERNEL_MMA;
+    c->stats.last_kernel = QLD_KERNEL_FP4;
     return QLD_OK;
 }
 
@@ -1064,6 +1156,126 @@ int qld_cuda_sync(qld_ctx *c, void *stream) {
     if (!c) return QLD_ERR_INVALID;
     CUDA_TRY(c, cudaSetDevice(c->device));
     return finish(c, stream ? static_cast<cudaStream_t>(stream) : c->stream);
+}
+
+int qld_cuda_autotune(qld_ctx *c, int m, int n, int K, int symmetric, int *kernel,
+                      int *option, float *ms) {
+    if (!c) return QLD_ERR_INVALID;
+    if (symmetric) n = m;
+    if (m < 1 || n < 1 || K < 1 || (long long)K * 64 > 0x7FFFFFFFLL)
+        return set_err(c, QLD_ERR_INVALID, "bad tuning shape m=%d n=%d K=%d", m, n, K);
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const int mt = m < kTuneMaxSide ? m : kTuneMaxSide;
+    const int nt = symmetric ? mt : (n < kTuneMaxSide ? n : kTuneMaxSide);
+    const long long Kp = K + (K & 1);
+    int rc;
+    if ((rc = ensure(c, c->dA, (size_t)mt * Kp * 8)) || (rc = ensure(c, c->dbcA, (size_t)mt * 4)) ||
+        (rc = ensure(c, c->dOut[0], (size_t)nt * mt * 4)))
+        return rc;
+    if (!symmetric && ((rc = ensure(c, c->dB, (size_t)nt * Kp * 8)) ||
+                       (rc = ensure(c, c->dbcB, (size_t)nt * 4))))
+        return rc;
+    uint64_t *dA = static_cast<uint64_t *>(c->dA.p);
+    uint64_t *dB = symmetric ? dA : static_cast<uint64_t *>(c->dB.p);
+    uint32_t *dbcA = static_cast<uint32_t *>(c->dbcA.p);
+    uint32_t *dbcB = symmetric ? dbcA : static_cast<uint32_t *>(c->dbcB.p);
+    k_tune_fill<<<1024, 256, 0, c->stream>>>(dA, mt, K, Kp, 0x5EEDull);
+    k_tune_bc<<<(mt + 255) / 256, 256, 0, c->stream>>>(dA, mt, K, Kp, dbcA);
+    if (!symmetric) {
+        k_tune_fill<<<1024, 256, 0, c->stream>>>(dB, nt, K, Kp, 0xB0B0ull);
+        k_tune_bc<<<(nt + 255) / 256, 256, 0, c->stream>>>(dB, nt, K, Kp, dbcB);
+    }
+    CUDA_TRY(c, cudaGetLastError());
+    const Task t{dA, dbcA, mt, Kp, dB, dbcB, nt, Kp, K, K * 64, symmetric, 0};
+    float *r2 = static_cast<float *>(c->dOut[0].p);
+
+    struct Cand { int kernel, option; };
+    std::vector<Cand> cands{{QLD_KERNEL_POPC, 0}};
+    if (mma_exact_for(t)) { cands.push_back({QLD_KERNEL_MMA, 128}); cands.push_back({QLD_KERNEL_MMA, 256}); }
+    if (fp4_exact_for(t)) { cands.push_back({QLD_KERNEL_FP4, 1}); cands.push_back({QLD_KERNEL_FP4, 2}); }
+
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CUDA_TRY(c, cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return set_err(c, QLD_ERR_CUDA, "cudaEventCreate failed");
+    }
+    TuneChoice best{0, 0, 0.f};
+    {
+        OptionGuard guard(c);
+        for (const Cand &cd : cands) {
+            c->kernel = cd.kernel;
+            c->mma_tile = cd.kernel == QLD_KERNEL_MMA ? cd.option : 0;
+            c->sm_pair = cd.kernel == QLD_KERNEL_FP4 ? cd.option : 0;
+            // one warm-up launch, then the mean of three
+            if ((rc = launch_counts(c, t, 0, nt, r2, mt, nullptr, 0, 0, c->stream)) ||
+                (rc = finish(c, c->stream)))
+                break;
+            cudaEventRecord(e0, c->stream);
+            for (int r = 0; r < 3 && !rc; ++r)
+                rc = launch_counts(c, t, 0, nt, r2, mt, nullptr, 0, 0, c->stream);
+            cudaEventRecord(e1, c->stream);
+            if (rc || (rc = finish(c, c->stream))) break;
+            float el = 0.f;
+            cudaEventElapsedTime(&el, e0, e1);
+            if (best.kernel == 0 || el / 3 < best.ms) best = TuneChoice{cd.kernel, cd.option, el / 3};
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    c->tune[tune_key(m, n, K, symmetric ? 1 : 0)] = best;
+    if (kernel) *kernel = best.kernel;
+    if (option) *option = best.option;
+    if (ms) *ms = best.ms;
+    return QLD_OK;
+}
+
+int qld_cuda_tune_save(qld_ctx *c, const char *path) {
+    if (!c || !path) return QLD_ERR_INVALID;
+    FILE *f = fopen(path, "w");
+    if (!f) return set_err(c, QLD_ERR_INVALID, "cannot write %s", path);
+    fprintf(f, "qld-tune 1\n");
+    for (const auto &kv : c->tune)
+        fprintf(f, "%d %d %d %d %d %d %.6f\n", (int)(kv.first >> 24), (int)((kv.first >> 16) & 255),
+                (int)((kv.first >> 8) & 255), (int)(kv.first & 255), kv.second.kernel,
+                kv.second.option, kv.second.ms);
+    const bool ok = fclose(f) == 0;
+    return ok ? QLD_OK : set_err(c, QLD_ERR_INVALID, "cannot write %s", path);
+}
+
+int qld_cuda_tune_load(qld_ctx *c, const char *path) {
+    if (!c || !path) return QLD_ERR_INVALID;
+    FILE *f = fopen(path, "r");
+    if (!f) return set_err(c, QLD_ERR_INVALID, "cannot read %s", path);
+    int version = 0;
+    if (fscanf(f, "qld-tune %d", &version) != 1 || version != 1) {
+        fclose(f);
+        return set_err(c, QLD_ERR_INVALID, "%s is not a qld tuning table", path);
+    }
+    std::map<long long, TuneChoice> table;
+    int ml, nl, kl, kind, kernel, option, line = 1;
+    float ms;
+    int got;
+    while ((got = fscanf(f, "%d %d %d %d %d %d %f", &ml, &nl, &kl, &kind, &kernel, &option, &ms)) == 7) {
+        ++line;
+        const bool opt_ok = kernel == QLD_KERNEL_POPC ? option == 0
+                            : kernel == QLD_KERNEL_MMA ? (option == 128 || option == 256)
+                            : kernel == QLD_KERNEL_FP4 ? (option == 1 || option == 2)
+                                                       : false;
+        if (ml < 0 || ml > 31 || nl < 0 || nl > 31 || kl < 0 || kl > 31 || kind < 0 || kind > 1 ||
+            !opt_ok || !(ms >= 0.f)) {
+            fclose(f);
+            return set_err(c, QLD_ERR_INVALID, "%s line %d: bad entry", path, line);
+        }
+        table[((long long)ml << 24) | ((long long)nl << 16) | ((long long)kl << 8) | kind] =
+            TuneChoice{kernel, option, ms};
+    }
+    const bool at_end = got == EOF;
+    fclose(f);
+    if (!at_end) return set_err(c, QLD_ERR_INVALID, "%s line %d: bad entry", path, line + 1);
+    for (const auto &kv : table) c->tune[kv.first] = kv.second;
+    return QLD_OK;
 }
 
 }  // extern "C"
