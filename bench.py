@@ -273,12 +273,26 @@ def reference_arm(args, rank, world):
 
 # -------------------------------------------------------------------- ours --
 
-def lower_tri_d2h_bytes(m, tile=128):
+def lower_tri_d2h_bytes(m, band=3840, block=512):
+    """Bytes qld_cuda_ld moves to the host for a single region of m SNPs:
+    B rows in bands (the default 4,096 rows rounded to whole 240-row tiles of
+    the 4-bit kernel), each band in 512-row 2-D blocks of columns [r0, m)."""
     total = 0
-    for r0 in range(0, m, tile):
-        rows = min(tile, m - r0)
-        total += rows * (m - r0) * 4
+    for b0 in range(0, m, band):
+        b1 = min(m, b0 + band)
+        for r0 in range(b0, b1, block):
+            total += (min(block, b1 - r0)) * (m - r0) * 4
     return total
+
+
+def max_over_ranks(value, world, device):
+    """The largest of the ranks' values; every rank calls it (a no-op at 1)."""
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def ours_arm(args, rank, world, local_rank):
@@ -353,10 +367,7 @@ def ours_arm(args, rank, world, local_rank):
     clocks = clk.summary()
 
     pairs = m * (m - 1) / 2
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms_max = float(t.item())
+    total_ms_max = max_over_ranks(total_ms, world, dev)
     value = pairs * args.steps * world / (total_ms_max * 1e-3)
 
     # roofline of the counts kernel
@@ -394,10 +405,8 @@ def ours_arm(args, rank, world, local_rank):
             t0 = time.perf_counter()
             ctx.ld(Th, bch, S=S, r2_out=outh)
             ts.append(time.perf_counter() - t0)
-        tt = torch.tensor([sum(ts)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        line["e2e"] = {"value": pairs * args.steps * world / float(tt.item()), "unit": "pairs/s",
+        e2e_s = max_over_ranks(sum(ts), world, dev)
+        line["e2e"] = {"value": pairs * args.steps * world / e2e_s, "unit": "pairs/s",
                        "h2d_bytes_per_step": m * K * 8 + m * 4,
                        "d2h_bytes_per_step": lower_tri_d2h_bytes(m),
                        "api": "qld_cuda_ld (pinned host buffers)"}
