@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma", "fp4"])
     ap.add_argument("--sm-pair", type=int, default=0, choices=[0, 1, 2],
                     help="4-bit kernel: SMs per output tile (0 = automatic)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="run qld_cuda_autotune on the workload's shape first (AUTO then uses it)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mma-tile", type=int, default=0, choices=[0, 128, 256],
@@ -336,6 +338,12 @@ def ours_arm(args, rank, world, local_rank):
     def step():
         ctx.ld_device(Tp, bc, m, lda, Tp, bc, m, lda, K, S, True, out, m, stream=st)
 
+    tuned = None
+    if args.autotune and kern == api.KERNEL_AUTO:
+        tk, topt, tms = ctx.autotune(m, m, K, True)
+        tuned = {"kernel": tk, "option": topt, "ms_per_launch_tuned": tms,
+                 "measured_at": f"{min(m, 16384)}x{min(m, 16384)}x{K} words"}
+
     for _ in range(args.warmup):
         flush.zero_()
         step()
@@ -376,7 +384,10 @@ def ours_arm(args, rank, world, local_rank):
     variant = stats.last_kernel
     roof = kernel_roofline(ctx, variant, bitops, kern_ms, dev)
     alg_bytes = m * K * 8 * 2 + pairs * 4
-    roof["traffic"] = measured_traffic(variant, cfg["workload"], args.sm_pair)
+    sm_pair = args.sm_pair
+    if tuned is not None and tuned["kernel"] == api.KERNEL_FP4 and sm_pair == 0:
+        sm_pair = tuned["option"]
+    roof["traffic"] = measured_traffic(variant, cfg["workload"], sm_pair)
     roof["algorithmic_bytes_per_launch"] = alg_bytes
     roof["kernel_ms"] = kern_ms
     roof["hbm_frac_of_measured"] = (alg_bytes / (kern_ms * 1e-3) / 1e9) / 6538.9
@@ -388,6 +399,8 @@ def ours_arm(args, rank, world, local_rank):
             "bitops_per_s": bitops * args.steps * world / (total_ms_max * 1e-3),
             "gpu_launches": stats.kernel_launches, "kernel_variant": variant,
             "roofline": roof, "clocks": clocks}
+    if tuned is not None:
+        line["autotune"] = tuned
 
     # ---- e2e through the host-buffer C-ABI call
     if not args.no_e2e:
@@ -488,10 +501,12 @@ def batched_arm(args, rank, world, local_rank):
         ctx.stats(reset=True)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push(f"qld_timed_{name}")
         e0.record(st)
         for _ in range(args.steps):
             fn()
         e1.record(st)
+        torch.cuda.nvtx.range_pop()
         ctx.sync(stream=st)
         torch.cuda.synchronize()
         res[name] = (e0.elapsed_time(e1) / args.steps, ctx.stats(reset=True))
