@@ -49,7 +49,6 @@ constexpr int BM = 256, BN = 240;        // output tile of a pair
 constexpr int HM = 128, HN = 120;        // A and B rows held by each CTA
 constexpr int PW = 8;                    // packed words per row per packed stage
 constexpr int SUB = 2;                   // unpacked stages (256 samples) per packed stage
-constexpr int PST = 5;                      // packed stages: ~2.8 us of MMA work in flight
 constexpr int UST = 4;
 constexpr int PA_BYTES = HM * PW * 8;    // 8 KB
 constexpr int PB_TX = HN * PW * 8;       // 7.5 KB delivered per stage
@@ -73,20 +72,29 @@ constexpr uint32_t IDESC_ODD = idesc_mxf4_sf(BM, BN, 2);    // k-steps 1, 3: sca
 constexpr int COLS_N = 256;              // epilogue column factors (BN used)
 constexpr uint16_t BOTH = 0x3;           // CTA mask of a commit to both ranks
 
-constexpr int OFF_UA = 0;
-constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
-constexpr int OFF_PA = OFF_UB + UST * UB_BYTES;
-constexpr int OFF_PB = OFF_PA + PST * PA_BYTES;
-constexpr int OFF_ROWS = OFF_PB + PST * PB_BYTES;
-constexpr int ROWS_BYTES = COLS_N * epi::COL_BYTES;
-constexpr int OFF_BAR = OFF_ROWS + ROWS_BYTES;
-constexpr int NBARS = 2 * PST + 2 * UST + 2 + 2 + 1;
-constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
-constexpr int SMEM_BYTES = OFF_TMEM + 16 + 1024;
-static_assert(SMEM_BYTES <= 232448, "shared memory budget");
-static_assert(OFF_UB % 1024 == 0 && UB_BYTES % 1024 == 0 && OFF_PA % 1024 == 0 &&
-                  OFF_PB % 1024 == 0 && PB_TX <= PB_BYTES,
-              "swizzled stages must start on 1024-byte boundaries");
+// Shared-memory layout per r^2 mode.  R2_EXACT needs 8 bytes of column
+// factors per column (epi::ColsF), R2_REFERENCE 24 (epi::Cols); the room
+// this saves holds a sixth packed stage (more TMA lookahead: 2.576 -> 2.562
+// ms on the single region).
+template <int MODE>
+struct Smem {
+    static constexpr int PST = MODE == R2_EXACT ? 6 : 5;   // packed stages in flight
+    static constexpr int OFF_UA = 0;
+    static constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
+    static constexpr int OFF_PA = OFF_UB + UST * UB_BYTES;
+    static constexpr int OFF_PB = OFF_PA + PST * PA_BYTES;
+    static constexpr int OFF_ROWS = OFF_PB + PST * PB_BYTES;
+    static constexpr int ROWS_BYTES = COLS_N * (MODE == R2_EXACT ? 8 : epi::COL_BYTES);
+    static constexpr int OFF_BAR = OFF_ROWS + ROWS_BYTES;
+    static constexpr int NBARS = 2 * PST + 2 * UST + 2 + 2 + 1;
+    static constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
+    static constexpr int BYTES = OFF_TMEM + 16 + 1024;
+    static_assert(BYTES <= 232448, "shared memory budget");
+    static_assert(OFF_UB % 1024 == 0 && UB_BYTES % 1024 == 0 && OFF_PA % 1024 == 0 &&
+                      OFF_PB % 1024 == 0 && PB_TX <= PB_BYTES,
+                  "swizzled stages must start on 1024-byte boundaries");
+};
+static_assert(sizeof(float2) == 8, "ColsF entry");
 static_assert(ACC_STRIDE + BN <= SF_COL && SF_COL + 16 <= TMEM_COLS, "TMEM map");
 static_assert(TASKS == 2 && SUB == 2 && UST % 2 == 0 && EPILOGUE == COLS_N, "work split");
 
@@ -137,18 +145,20 @@ template <int MODE>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
 k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                const LdParams p, const int tiles_b) {
+    using L = Smem<MODE>;
+    constexpr int PST = L::PST;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + OFF_BAR);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::OFF_BAR);
     uint64_t *pfull = bars, *pempty = bars + PST;
     uint64_t *ufull = bars + 2 * PST, *uempty = bars + 2 * PST + UST;
     uint64_t *accfull = bars + 2 * PST + 2 * UST;
     uint64_t *accempty = accfull + 2;
     uint64_t *mma_done = accempty + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + OFF_TMEM);
-    const epi::Cols cols(smem + OFF_ROWS, COLS_N);
-    const epi::ColsF colsf(smem + OFF_ROWS, COLS_N);   // R2_EXACT: FP32 factors
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L::OFF_TMEM);
+    const epi::Cols cols(smem + L::OFF_ROWS, COLS_N);
+    const epi::ColsF colsf(smem + L::OFF_ROWS, COLS_N);   // R2_EXACT: FP32 factors
 
     const uint32_t rank = cluster_rank();
     const int pair = (int)cluster_id_x(), npairs = (int)cluster_count_x();
@@ -219,8 +229,8 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                     }
                     const uint32_t fb = smem_u32(&pfull[s]);
                     mbar_arrive_expect_tx(fb, PA_BYTES + PB_TX);
-                    tma_load_2d(smem_u32(smem + OFF_PA + s * PA_BYTES), &tmA, kp * PW, ra, fb);
-                    tma_load_2d(smem_u32(smem + OFF_PB + s * PB_BYTES), &tmB, kp * PW, rb, fb);
+                    tma_load_2d(smem_u32(smem + L::OFF_PA + s * PA_BYTES), &tmA, kp * PW, ra, fb);
+                    tma_load_2d(smem_u32(smem + L::OFF_PB + s * PB_BYTES), &tmB, kp * PW, rb, fb);
                 }
             }
             for (int g = gp > PST ? gp - PST : 0; g < gp; ++g)
@@ -254,8 +264,8 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t a0 = smem_u32(smem + OFF_UA + s * UA_BYTES);
-                    const uint32_t b0 = smem_u32(smem + OFF_UB + s * UB_BYTES);
+                    const uint32_t a0 = smem_u32(smem + L::OFF_UA + s * UA_BYTES);
+                    const uint32_t b0 = smem_u32(smem + L::OFF_UB + s * UB_BYTES);
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk)
                         tc_mma_mxf4_pair(d, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32),
@@ -304,8 +314,8 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 if (lane == 0) flag_error(p.status, ST_TIMEOUT_MMA);
                 break;
             }
-            unpack_rows(task, smem + OFF_PA + ps * PA_BYTES, smem + OFF_PB + ps * PB_BYTES,
-                        smem + OFF_UA + us * UA_BYTES, smem + OFF_UB + us * UB_BYTES, grp);
+            unpack_rows(task, smem + L::OFF_PA + ps * PA_BYTES, smem + L::OFF_PB + ps * PB_BYTES,
+                        smem + L::OFF_UA + us * UA_BYTES, smem + L::OFF_UB + us * UB_BYTES, grp);
             fence_proxy_async_smem();
             __syncwarp();
             if (lane == 0) {
@@ -405,7 +415,7 @@ cudaError_t launch_mode(const CUtensorMap &tmA, const CUtensorMap &tmB, const Ld
                         int tiles_b, cudaStream_t st) {
     auto kern = k_ld_mxf4_pair<MODE>;
     cudaError_t e =
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Smem<MODE>::BYTES);
     if (e != cudaSuccess) return e;
     if (g_max_pairs == 0) {
         int dev = 0, sms = 0;
@@ -416,7 +426,7 @@ cudaError_t launch_mode(const CUtensorMap &tmA, const CUtensorMap &tmB, const Ld
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(2 * (sms / 2), 1, 1);
         cfg.blockDim = dim3(THREADS, 1, 1);
-        cfg.dynamicSmemBytes = SMEM_BYTES;
+        cfg.dynamicSmemBytes = Smem<MODE>::BYTES;
         int n = 0;
         if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess || n <= 0) {
             (void)cudaGetLastError();
@@ -428,7 +438,7 @@ cudaError_t launch_mode(const CUtensorMap &tmA, const CUtensorMap &tmB, const Ld
         TileList<BM, BN>{(p.m + BM - 1) / BM, p.tb0, tiles_b, p.symmetric, p.band}.count();
     if (ntiles == 0) return cudaSuccess;
     const int pairs = (int)(ntiles < g_max_pairs ? ntiles : g_max_pairs);
-    kern<<<2 * pairs, THREADS, SMEM_BYTES, st>>>(tmA, tmB, p, tiles_b);
+    kern<<<2 * pairs, THREADS, Smem<MODE>::BYTES, st>>>(tmA, tmB, p, tiles_b);
     return cudaGetLastError();
 }
 
