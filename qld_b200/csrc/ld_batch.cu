@@ -46,7 +46,6 @@ constexpr int BM = 256, BN = 240;           // work item: output tile of a pair
 constexpr int HM = 128, HN = 120;           // A and B rows held by each CTA
 constexpr int PW = 8;                       // packed words per row per packed stage
 constexpr int SUB = 2;                      // unpacked stages (256 samples) per packed stage
-constexpr int PST = 5;                      // packed stages: ~2.8 us of MMA work in flight
 constexpr int UST = 4;                      // two unpacked stages per unpack group
 constexpr int PA_BYTES = HM * PW * 8;       // 8 KB
 constexpr int PB_TX = HN * PW * 8;          // 7.5 KB delivered per stage
@@ -74,21 +73,28 @@ constexpr int QSLOTS = 4;                                    // item ring depth
 // unpack and epilogue warps; rank 1's TMA thread, unpack and epilogue warps
 constexpr int ITEM_USERS = 2 * (1 + UNPACK_WARPS + EPI_WARPS);
 
-constexpr int OFF_UA = 0;
-constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
-constexpr int OFF_PA = OFF_UB + UST * UB_BYTES;
-constexpr int OFF_PB = OFF_PA + PST * PA_BYTES;
-constexpr int OFF_ROWS = OFF_PB + PST * PB_BYTES;
-constexpr int ROWS_BYTES = COLS_N * epi::COL_BYTES;
-constexpr int OFF_ITEMS = OFF_ROWS + ROWS_BYTES;
-constexpr int OFF_BAR = OFF_ITEMS + QSLOTS * 16;
-constexpr int NBARS = 2 * PST + 2 * UST + 2 + 2 + 1 + 2 * QSLOTS;
-constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
-constexpr int SMEM_BYTES = OFF_TMEM + 16 + 1024;
-static_assert(SMEM_BYTES <= 232448, "shared memory budget");
-static_assert(OFF_UB % 1024 == 0 && UB_BYTES % 1024 == 0 && OFF_PA % 1024 == 0 &&
-                  OFF_PB % 1024 == 0 && PB_TX <= PB_BYTES && OFF_ITEMS % 16 == 0,
-              "swizzled stages must start on 1024-byte boundaries");
+// Shared-memory layout per r^2 mode: R2_EXACT needs 8 bytes of column
+// factors per column (epi::ColsF), R2_REFERENCE 24 (epi::Cols); the room this
+// saves holds a sixth packed stage (more TMA lookahead).
+template <int MODE>
+struct Smem {
+    static constexpr int PST = MODE == R2_EXACT ? 6 : 5;   // packed stages in flight
+    static constexpr int OFF_UA = 0;
+    static constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
+    static constexpr int OFF_PA = OFF_UB + UST * UB_BYTES;
+    static constexpr int OFF_PB = OFF_PA + PST * PA_BYTES;
+    static constexpr int OFF_ROWS = OFF_PB + PST * PB_BYTES;
+    static constexpr int ROWS_BYTES = COLS_N * (MODE == R2_EXACT ? 8 : epi::COL_BYTES);
+    static constexpr int OFF_ITEMS = OFF_ROWS + ROWS_BYTES;
+    static constexpr int OFF_BAR = OFF_ITEMS + QSLOTS * 16;
+    static constexpr int NBARS = 2 * PST + 2 * UST + 2 + 2 + 1 + 2 * QSLOTS;
+    static constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
+    static constexpr int BYTES = OFF_TMEM + 16 + 1024;
+    static_assert(BYTES <= 232448, "shared memory budget");
+    static_assert(OFF_UB % 1024 == 0 && UB_BYTES % 1024 == 0 && OFF_PA % 1024 == 0 &&
+                      OFF_PB % 1024 == 0 && PB_TX <= PB_BYTES && OFF_ITEMS % 16 == 0,
+                  "swizzled stages must start on 1024-byte boundaries");
+};
 static_assert(ACC_STRIDE + BN <= SF_COL && SF_COL + 16 <= TMEM_COLS, "TMEM map");
 static_assert(TASKS == 2 && SUB == 2 && UST % 2 == 0 && EPI_THREADS == COLS_N, "work split");
 
@@ -131,20 +137,22 @@ __device__ __forceinline__ Item decode_item(const BatchJob *jobs, int njobs, lon
 template <int MODE>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
 k_ld_batch(const BatchParams bp) {
+    using L = Smem<MODE>;
+    constexpr int PST = L::PST;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + OFF_BAR);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::OFF_BAR);
     uint64_t *pfull = bars, *pempty = bars + PST;
     uint64_t *ufull = bars + 2 * PST, *uempty = bars + 2 * PST + UST;
     uint64_t *accfull = bars + 2 * PST + 2 * UST;
     uint64_t *accempty = accfull + 2;
     uint64_t *mma_done = accempty + 2;
     uint64_t *ifull = mma_done + 1, *iempty = ifull + QSLOTS;
-    Item *items = reinterpret_cast<Item *>(smem + OFF_ITEMS);
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + OFF_TMEM);
-    const epi::Cols cols(smem + OFF_ROWS, COLS_N);
-    const epi::ColsF colsf(smem + OFF_ROWS, COLS_N);   // R2_EXACT: FP32 factors
+    Item *items = reinterpret_cast<Item *>(smem + L::OFF_ITEMS);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L::OFF_TMEM);
+    const epi::Cols cols(smem + L::OFF_ROWS, COLS_N);
+    const epi::ColsF colsf(smem + L::OFF_ROWS, COLS_N);   // R2_EXACT: FP32 factors
 
     const uint32_t rank = cluster_rank();
     const int tid = threadIdx.x;
@@ -243,8 +251,8 @@ k_ld_batch(const BatchParams bp) {
                     }
                     const uint32_t fb = smem_u32(&pfull[s]);
                     mbar_arrive_expect_tx(fb, PA_BYTES + PB_TX);
-                    tma_load_2d(smem_u32(smem + OFF_PA + s * PA_BYTES), &J.tmA, kp * PW, ra, fb);
-                    tma_load_2d(smem_u32(smem + OFF_PB + s * PB_BYTES), &J.tmB, kp * PW, rb, fb);
+                    tma_load_2d(smem_u32(smem + L::OFF_PA + s * PA_BYTES), &J.tmA, kp * PW, ra, fb);
+                    tma_load_2d(smem_u32(smem + L::OFF_PB + s * PB_BYTES), &J.tmB, kp * PW, rb, fb);
                 }
                 if (rank == 1) {
                     release_item(qi);
@@ -287,8 +295,8 @@ k_ld_batch(const BatchParams bp) {
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t a0 = smem_u32(smem + OFF_UA + s * UA_BYTES);
-                    const uint32_t b0 = smem_u32(smem + OFF_UB + s * UB_BYTES);
+                    const uint32_t a0 = smem_u32(smem + L::OFF_UA + s * UA_BYTES);
+                    const uint32_t b0 = smem_u32(smem + L::OFF_UB + s * UB_BYTES);
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk)
                         tc_mma_mxf4_pair(d, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32),
@@ -347,10 +355,10 @@ k_ld_batch(const BatchParams bp) {
                     ok = false;
                     break;
                 }
-                const uint8_t *pa = smem + OFF_PA + ps * PA_BYTES;
-                const uint8_t *pb = smem + OFF_PB + ps * PB_BYTES;
-                uint8_t *ua = smem + OFF_UA + us * UA_BYTES;
-                uint8_t *ub = smem + OFF_UB + us * UB_BYTES;
+                const uint8_t *pa = smem + L::OFF_PA + ps * PA_BYTES;
+                const uint8_t *pb = smem + L::OFF_PB + ps * PB_BYTES;
+                uint8_t *ua = smem + L::OFF_UA + us * UA_BYTES;
+                uint8_t *ub = smem + L::OFF_UB + us * UB_BYTES;
                 uint4 w[TASKS][2];
 #pragma unroll
                 for (int j = 0; j < TASKS; ++j)
@@ -389,7 +397,7 @@ k_ld_batch(const BatchParams bp) {
         // loop together: a failure is recorded in a shared flag that is only
         // read right after the first barrier of an item (every write to it
         // happens before that barrier or between the second and third).
-        volatile int *epi_fail = reinterpret_cast<volatile int *>(smem + OFF_TMEM + 8);
+        volatile int *epi_fail = reinterpret_cast<volatile int *>(smem + L::OFF_TMEM + 8);
         const int et = tid - FIRST_EPI_WARP * 32;
         const int ew = warp - FIRST_EPI_WARP;
         const int q = warp & 3;             // TMEM lane quarter
@@ -490,7 +498,7 @@ template <int MODE>
 cudaError_t launch_mode(const BatchParams &bp, int max_ctas, cudaStream_t st) {
     auto kern = k_ld_batch<MODE>;
     cudaError_t e =
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Smem<MODE>::BYTES);
     if (e != cudaSuccess) return e;
     if (g_max_pairs == 0) {
         int dev = 0, sms = 0;
@@ -501,7 +509,7 @@ cudaError_t launch_mode(const BatchParams &bp, int max_ctas, cudaStream_t st) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(2 * (sms / 2), 1, 1);
         cfg.blockDim = dim3(THREADS, 1, 1);
-        cfg.dynamicSmemBytes = SMEM_BYTES;
+        cfg.dynamicSmemBytes = Smem<MODE>::BYTES;
         int n = 0;
         if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess || n <= 0) {
             (void)cudaGetLastError();
@@ -512,7 +520,7 @@ cudaError_t launch_mode(const BatchParams &bp, int max_ctas, cudaStream_t st) {
     long long pairs = bp.nitems < g_max_pairs ? bp.nitems : g_max_pairs;
     if (max_ctas > 0 && 2 * pairs > max_ctas) pairs = max_ctas / 2;
     if (pairs <= 0) return cudaSuccess;
-    kern<<<(int)(2 * pairs), THREADS, SMEM_BYTES, st>>>(bp);
+    kern<<<(int)(2 * pairs), THREADS, Smem<MODE>::BYTES, st>>>(bp);
     return cudaGetLastError();
 }
 
