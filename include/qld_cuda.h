@@ -79,6 +79,12 @@ extern "C" {
 #define QLD_OPT_MMA_TILE  5  /* QLD_KERNEL_MMA output tile rows: 128, 256, 0 = per shape */
 #define QLD_OPT_SM_PAIR   6  /* QLD_KERNEL_FP4 SMs per output tile: 1, 2 (a cluster of two
                                 CTAs, tcgen05 cta_group::2), 0 = automatic (2) */
+#define QLD_OPT_WAIT_CYCLES 7 /* budget of every bounded wait inside the kernels' pipelines,
+                                in SM clock cycles (0 = the default 4e9, ~2 s; the environment
+                                variable QLD_TIMEOUT_CYCLES sets the initial value).  A wait
+                                that runs out records the cause and the kernel ends early:
+                                the call returns QLD_ERR_TIMEOUT and the context stays usable.
+                                Copies and MMAs in flight are always drained first. */
 
 typedef struct qld_ctx qld_ctx;
 

@@ -260,7 +260,7 @@ k_ld_batch(const BatchParams bp) {
                 }
             }
             for (int g = gp > PST ? gp - PST : 0; g < gp; ++g)
-                if (!mbar_wait(smem_u32(&pfull[g % PST]), (g / PST) & 1, limit, nullptr)) {
+                if (!mbar_wait(smem_u32(&pfull[g % PST]), (g / PST) & 1, kDrainCycles, nullptr)) {
                     flag_error(bp.status, ST_TIMEOUT_DRAIN);
                     break;
                 }
@@ -478,7 +478,7 @@ k_ld_batch(const BatchParams bp) {
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
-        if (!mbar_wait(smem_u32(mma_done), 0, limit, nullptr))
+        if (!mbar_wait(smem_u32(mma_done), 0, kDrainCycles, nullptr))
             flag_error(bp.status, ST_TIMEOUT_MMA);
         __syncwarp();
     }

@@ -159,7 +159,7 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
             }
             // Drain: this CTA's copies must land before it retires.
             for (int g = gp > PST ? gp - PST : 0; g < gp; ++g)
-                if (!mbar_wait(smem_u32(&pfull[g % PST]), (g / PST) & 1, p.timeout_cycles,
+                if (!mbar_wait(smem_u32(&pfull[g % PST]), (g / PST) & 1, kDrainCycles,
                                nullptr)) {
                     flag_error(p.status, ST_TIMEOUT_DRAIN);
                     break;
@@ -326,7 +326,7 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
     __syncthreads();
     if (warp == 1) {
         // Every MMA must be complete before TMEM is released.
-        if (!mbar_wait(smem_u32(mma_done), 0, p.timeout_cycles, nullptr))
+        if (!mbar_wait(smem_u32(mma_done), 0, kDrainCycles, nullptr))
             flag_error(p.status, ST_TIMEOUT_MMA);
         __syncwarp();
         tc_fence_after();

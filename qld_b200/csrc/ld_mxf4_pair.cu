@@ -234,7 +234,7 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 }
             }
             for (int g = gp > PST ? gp - PST : 0; g < gp; ++g)
-                if (!mbar_wait(smem_u32(&pfull[g % PST]), (g / PST) & 1, p.timeout_cycles,
+                if (!mbar_wait(smem_u32(&pfull[g % PST]), (g / PST) & 1, kDrainCycles,
                                nullptr)) {
                     flag_error(p.status, ST_TIMEOUT_DRAIN);
                     break;
@@ -394,7 +394,7 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
-        if (!mbar_wait(smem_u32(mma_done), 0, p.timeout_cycles, nullptr))
+        if (!mbar_wait(smem_u32(mma_done), 0, kDrainCycles, nullptr))
             flag_error(p.status, ST_TIMEOUT_MMA);
         __syncwarp();
     }

@@ -91,7 +91,7 @@ k_ld_popc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
             // these waits ignore other CTAs' errors.
             for (int kc = issued > STAGES ? issued - STAGES : 0; kc < issued; ++kc) {
                 if (!mbar_wait(smem_u32(&full[kc % STAGES]), (kc / STAGES) & 1,
-                               p.timeout_cycles, nullptr)) {
+                               kDrainCycles, nullptr)) {
                     flag_error(p.status, ST_TIMEOUT_DRAIN);
                     break;
                 }

@@ -586,6 +586,11 @@ int qld_cuda_set_option(qld_ctx *c, int option, long long value) {
             return set_err(c, QLD_ERR_INVALID, "SMs per 4-bit tile must be 0, 1 or 2");
         c->sm_pair = (int)value;
         return QLD_OK;
+    case QLD_OPT_WAIT_CYCLES:
+        if (value < 0)
+            return set_err(c, QLD_ERR_INVALID, "wait budget %lld out of range", value);
+        c->timeout_cycles = value ? value : 4000000000LL;
+        return QLD_OK;
     case QLD_OPT_BAND_ROWS:
         if (value < 256 || value > (1 << 24))
             return set_err(c, QLD_ERR_INVALID, "band rows %lld out of range", value);

@@ -94,6 +94,13 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long lo
     }
 }
 
+// Budget of the teardown waits: a kernel waits this long (~2 s at boost
+// clock) for its own TMA copies and MMAs still in flight before it releases
+// shared memory or TMEM, whatever budget its pipeline waits were given, so a
+// short pipeline budget (QLD_TIMEOUT_CYCLES) never retires a CTA with work
+// in flight.
+constexpr long long kDrainCycles = 4000000000LL;
+
 __device__ __forceinline__ bool grid_failed(const unsigned *status) {
     return status && *((volatile const unsigned *)status) != 0u;
 }
