@@ -85,6 +85,11 @@ extern "C" {
                                 that runs out records the cause and the kernel ends early:
                                 the call returns QLD_ERR_TIMEOUT and the context stays usable.
                                 Copies and MMAs in flight are always drained first. */
+#define QLD_OPT_MEM_CAP   8  /* cap, in bytes, on the device buffers the context allocates
+                                for its calls (0 = no cap).  A call that would grow them past
+                                it returns QLD_ERR_NOMEM before launching anything; the
+                                context stays usable.  Buffers already held count toward the
+                                cap and are kept (a lower cap applies as they grow). */
 
 typedef struct qld_ctx qld_ctx;
 

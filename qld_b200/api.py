@@ -28,7 +28,7 @@ ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NODEVICE, ERR_TIMEOUT, ERR_BUSY, ERR_UNSUP
 R2_EXACT, R2_REFERENCE = 0, 1
 KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA, KERNEL_FP4 = 0, 1, 2, 3
 OPT_KERNEL, OPT_R2_MODE, OPT_PROFILE, OPT_BAND_ROWS, OPT_MMA_TILE, OPT_SM_PAIR = 1, 2, 3, 4, 5, 6
-OPT_WAIT_CYCLES = 7
+OPT_WAIT_CYCLES, OPT_MEM_CAP = 7, 8
 
 EXPORTED = (
     "qld_cuda_init", "qld_cuda_release", "qld_cuda_last_error", "qld_cuda_set_option",

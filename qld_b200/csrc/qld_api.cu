@@ -63,6 +63,8 @@ struct qld_ctx {
     int sm_pair = 0;                  // 4-bit kernel: 0 per shape, 1 or 2 SMs per tile
     std::map<long long, TuneChoice> tune;   // qld_cuda_autotune results by shape class
     long long timeout_cycles = 4000000000LL;  // ~2 s at boost clock
+    size_t mem_cap = 0;               // QLD_OPT_MEM_CAP: 0 = no cap
+    size_t mem_held = 0;              // bytes of the buffers ensure() holds
     DevBuf dA, dB, dbcA, dbcB, dOut[2], dCnt[2];
     DevBuf dJobs, dQueue;             // batched launches: job table, ticket counter
     std::vector<BatchJob> hJobs;
@@ -102,10 +104,17 @@ int set_err(qld_ctx *c, int code, const char *fmt, ...) {
 
 int ensure(qld_ctx *c, DevBuf &b, size_t bytes) {
     if (bytes <= b.bytes) return QLD_OK;
+    const size_t others = c->mem_held - b.bytes;
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.bytes = 0;
+    c->mem_held = others;
+    if (c->mem_cap && others + bytes > c->mem_cap)
+        return set_err(c, QLD_ERR_NOMEM,
+                       "device memory cap: %zu bytes held + %zu needed > cap of %zu", others,
+                       bytes, c->mem_cap);
     size_t want = bytes + bytes / 8;  // headroom so nearby sizes reuse the buffer
+    if (c->mem_cap && others + want > c->mem_cap) want = bytes;
     if (cudaMalloc(&b.p, want) != cudaSuccess) {
         cudaGetLastError();
         if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
@@ -116,6 +125,7 @@ int ensure(qld_ctx *c, DevBuf &b, size_t bytes) {
         want = bytes;
     }
     b.bytes = want;
+    c->mem_held = others + want;
     return QLD_OK;
 }
 
@@ -585,6 +595,10 @@ int qld_cuda_set_option(qld_ctx *c, int option, long long value) {
         if (value < 0 || value > 2)
             return set_err(c, QLD_ERR_INVALID, "SMs per 4-bit tile must be 0, 1 or 2");
         c->sm_pair = (int)value;
+        return QLD_OK;
+    case QLD_OPT_MEM_CAP:
+        if (value < 0) return set_err(c, QLD_ERR_INVALID, "memory cap %lld out of range", value);
+        c->mem_cap = (size_t)value;
         return QLD_OK;
     case QLD_OPT_WAIT_CYCLES:
         if (value < 0)
