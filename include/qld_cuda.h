@@ -78,7 +78,9 @@ extern "C" {
                                 rounded down to whole tile rows of the kernel */
 #define QLD_OPT_MMA_TILE  5  /* QLD_KERNEL_MMA output tile rows: 128, 256, 0 = per shape */
 #define QLD_OPT_SM_PAIR   6  /* QLD_KERNEL_FP4 SMs per output tile: 1, 2 (a cluster of two
-                                CTAs, tcgen05 cta_group::2), 0 = automatic (2) */
+                                CTAs, tcgen05 cta_group::2), 0 = automatic (2 with
+                                QLD_R2_EXACT, 1 with QLD_R2_REFERENCE, whose FP64
+                                epilogue runs faster on the single-SM kernel's 16 warps) */
 #define QLD_OPT_WAIT_CYCLES 7 /* budget of every bounded wait inside the kernels' pipelines,
                                 in SM clock cycles (0 = the default 4e9, ~2 s; the environment
                                 variable QLD_TIMEOUT_CYCLES sets the initial value).  A wait
@@ -353,8 +355,9 @@ int qld_cuda_measure_mma_peak(qld_ctx *ctx, int kernel, double *ops_per_s);
  * (popcount; int8 MMA with 128- and 256-row tiles while K * 64 <= 131,071;
  * 4-bit MMA on single SMs and on SM pairs while K * 64 <= 2^24) on a
  * synthetic task of m x n SNPs (n = m when `symmetric`) and K words, and
- * records the fastest for the task's shape class: floor(log2) of m, n and K
- * and single versus two regions.  From then on QLD_KERNEL_AUTO uses the
+ * records the fastest for the task's shape class: floor(log2) of m, n and K,
+ * single versus two regions, and the context's r^2 mode (tune once per mode
+ * used).  From then on QLD_KERNEL_AUTO uses the
  * recorded kernel and tile option for tasks of that class (explicit
  * QLD_OPT_MMA_TILE / QLD_OPT_SM_PAIR values still win; band tasks and
  * untuned classes keep the built-in rule: the 4-bit kernel on SM pairs
@@ -368,7 +371,8 @@ int qld_cuda_measure_mma_peak(qld_ctx *ctx, int kernel, double *ops_per_s);
 int qld_cuda_autotune(qld_ctx *ctx, int m, int n, int K, int symmetric, int *kernel,
                       int *option, float *ms);
 /* The tuning table as text ("qld-tune 1", then one line per shape class:
- * log2 m, log2 n, log2 K, single region (0/1), kernel, option, ms).  Loading
+ * log2 m, log2 n, log2 K, kind (0 two regions, 1 single region, +4 in
+ * QLD_R2_REFERENCE mode), kernel, option, ms).  Loading
  * adds to (and overrides entries of) the context's table; a malformed file
  * changes nothing and returns QLD_ERR_INVALID. */
 int qld_cuda_tune_save(qld_ctx *ctx, const char *path);

@@ -174,8 +174,9 @@ bool mma_exact_for(const Task &t) { return (long long)t.K * 64 <= kMmaMaxSamples
 bool fp4_exact_for(const Task &t) { return (long long)t.K * 64 <= kMxf4MaxSamples; }
 
 // Shape class of a task for the autotuner's table: floor(log2) of m, n and
-// K, and the kind (two regions, single region, band).  Tasks in one class
-// differ in size by less than 2x on every side.
+// K, and the kind (0 two regions, 1 single region, 2 band; +4 in
+// R2_REFERENCE mode, whose epilogue changes which kernel is fastest).  Tasks
+// in one class differ in size by less than 2x on every side.
 int ilog2(long long x) {
     int r = 0;
     while (x > 1) { x >>= 1; ++r; }
@@ -185,7 +186,9 @@ long long tune_key(int m, int n, int K, int kind) {
     return ((long long)ilog2(m) << 24) | ((long long)ilog2(n) << 16) |
            ((long long)ilog2(K) << 8) | (long long)kind;
 }
-int task_kind(const Task &t) { return t.band > 0 ? 2 : (t.symmetric ? 1 : 0); }
+int task_kind(const Task &t, int r2_mode) {
+    return (t.band > 0 ? 2 : (t.symmetric ? 1 : 0)) + (r2_mode == QLD_R2_REFERENCE ? 4 : 0);
+}
 
 bool exact_for(int kernel, const Task &t);
 
@@ -193,7 +196,7 @@ bool exact_for(int kernel, const Task &t);
 // automatic, the class was tuned, and the tuned kernel is exact for the task.
 const TuneChoice *tuned_for(qld_ctx *c, const Task &t) {
     if (c->kernel != QLD_KERNEL_AUTO || c->tune.empty()) return nullptr;
-    auto it = c->tune.find(tune_key(t.m, t.n, t.K, task_kind(t)));
+    auto it = c->tune.find(tune_key(t.m, t.n, t.K, task_kind(t, c->r2_mode)));
     if (it == c->tune.end() || !exact_for(it->second.kernel, t)) return nullptr;
     return &it->second;
 }
@@ -236,16 +239,19 @@ const KernelShape &mma_shape(qld_ctx *c, const Task &t, int b0, int b1) {
     return tile_count(t, 256, 256, b0, b1) >= 4LL * c->sm_count ? kMmaWideShape : kMmaShape;
 }
 
-// The 4-bit kernel on SM pairs unless asked for single SMs (same 256 x 240
-// tiles).  The pair kernel overlaps each tile's epilogue with the next
-// tile's MMAs and finishes a tile on two SMs in half the time, so it is the
-// faster one for every task size measured (a single region of 29,817 SNPs x
-// 16,622 samples: 2.63 ms against 3.33 ms).
+// The 4-bit kernel on SM pairs or single SMs (same 256 x 240 tiles).  With
+// R2_EXACT the pair kernel overlaps each tile's epilogue with the next
+// tile's MMAs and finishes a tile on two SMs in half the time: the faster one
+// for every task size measured (a single region of 29,817 SNPs x 16,622
+// samples: 2.57 ms against 3.31 ms).  R2_REFERENCE's FP64 divisions make the
+// epilogue the bound, and the single-SM kernel runs it on 16 warps instead
+// of 8: 5.05 ms against 5.60 ms there.
 const KernelShape &fp4_shape(qld_ctx *c, const Task &t, int b0, int b1) {
     (void)b0; (void)b1;
     if (c->sm_pair == 0)
         if (const TuneChoice *tc = tuned_for(c, t))
             if (tc->kernel == QLD_KERNEL_FP4) return tc->option == 1 ? kMxf4Shape : kMxf4PairShape;
+    if (c->sm_pair == 0) return c->r2_mode == QLD_R2_REFERENCE ? kMxf4Shape : kMxf4PairShape;
     return c->sm_pair == 1 ? kMxf4Shape : kMxf4PairShape;
 }
 
@@ -1243,7 +1249,7 @@ int qld_cuda_autotune(qld_ctx *c, int m, int n, int K, int symmetric, int *kerne
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
-    c->tune[tune_key(m, n, K, symmetric ? 1 : 0)] = best;
+    c->tune[tune_key(m, n, K, (symmetric ? 1 : 0) + (c->r2_mode == QLD_R2_REFERENCE ? 4 : 0))] = best;
     if (kernel) *kernel = best.kernel;
     if (option) *option = best.option;
     if (ms) *ms = best.ms;
@@ -1282,7 +1288,8 @@ int qld_cuda_tune_load(qld_ctx *c, const char *path) {
                             : kernel == QLD_KERNEL_MMA ? (option == 128 || option == 256)
                             : kernel == QLD_KERNEL_FP4 ? (option == 1 || option == 2)
                                                        : false;
-        if (ml < 0 || ml > 31 || nl < 0 || nl > 31 || kl < 0 || kl > 31 || kind < 0 || kind > 1 ||
+        if (ml < 0 || ml > 31 || nl < 0 || nl > 31 || kl < 0 || kl > 31 ||
+            (kind != 0 && kind != 1 && kind != 4 && kind != 5) ||
             !opt_ok || !(ms >= 0.f)) {
             fclose(f);
             return set_err(c, QLD_ERR_INVALID, "%s line %d: bad entry", path, line);

@@ -88,3 +88,23 @@ def test_bad_table_is_rejected_and_changes_nothing(ctx, tmp_path):
     bad.write_text("not a table\n")
     with pytest.raises(api.QldError):
         ctx.tune_load(str(bad))
+
+
+def test_entries_are_per_r2_mode(ctx, tmp_path):
+    """An entry tuned in reference mode steers only reference-mode calls."""
+    path = tmp_path / "tune.txt"
+    path.write_text("qld-tune 1\n9 9 5 5 1 0 0.9\n")      # kind 1 + 4: reference mode
+    ctx.tune_load(str(path))
+    A, bc = _task(700, 2500, 7)
+    _check_auto(ctx, A, bc, 2500, api.KERNEL_FP4)         # exact mode: untuned
+    ctx.set_option(api.OPT_R2_MODE, api.R2_REFERENCE)
+    try:
+        r2, cnt = ctx.ld(A, bc, S=2500, counts=True)
+        assert ctx.stats().last_kernel == api.KERNEL_POPC
+        want = oracle.counts(A)
+        mask = lower_mask(*want.shape)
+        assert np.array_equal(cnt[mask], want[mask])
+        ref = oracle.r2_reference(bc, bc, want, 2500, fma_contract=False)
+        assert np.array_equal(r2[mask].view(np.uint32), ref[mask].view(np.uint32))
+    finally:
+        ctx.set_option(api.OPT_R2_MODE, api.R2_EXACT)
