@@ -66,6 +66,7 @@ struct qld_ctx {
     size_t mem_cap = 0;               // QLD_OPT_MEM_CAP: 0 = no cap
     size_t mem_held = 0;              // bytes of the buffers ensure() holds
     DevBuf dA, dB, dbcA, dbcB, dOut[2], dCnt[2];
+    DevBuf dStage;                    // host rows of odd K before padding (upload_rows)
     DevBuf dJobs, dQueue;             // batched launches: job table, ticket counter
     std::vector<BatchJob> hJobs;
     cudaEvent_t ev_band[2] = {nullptr, nullptr};
@@ -402,6 +403,38 @@ int launch_states_range(qld_ctx *c, const Task &t, int b0, int b1, uint8_t *out,
     return QLD_OK;
 }
 
+// Host rows of K words -> device rows of ldd words (ldd = K, or K + 1 to
+// keep rows 16-byte aligned).  A row-pitched 2-D copy moves rows of a few KB
+// at about a third of the link rate (19 vs 55 GB/s for 2,080-byte rows on a
+// B200) and slows device->host copies running beside it to a crawl, so the
+// rows go up as one 1-D copy: in place when ldd == K, else into `stage`
+// (rows * K words, reused by the next upload on the same stream) and a
+// kernel spreads them to the padded pitch.
+int upload_rows(qld_ctx *c, uint64_t *dst, long long ldd, const uint64_t *src, int K,
+                long long rows, uint64_t *stage, cudaStream_t st) {
+    if (rows <= 0) return QLD_OK;
+    const size_t bytes = (size_t)rows * K * 8;
+    if (ldd == K) {
+        CUDA_TRY(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        return QLD_OK;
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(stage, src, bytes, cudaMemcpyHostToDevice, st));
+    const cudaError_t e = launch_pad_rows(dst, ldd, stage, K, rows, st);
+    if (e != cudaSuccess)
+        return set_err(c, QLD_ERR_CUDA, "row padding launch failed: %s", cudaGetErrorString(e));
+    c->stats.kernel_launches++;
+    return QLD_OK;
+}
+
+// The staging buffer upload_rows needs for up to `rows` rows (none for even K).
+int ensure_stage(qld_ctx *c, int K, long long rows, uint64_t **stage) {
+    *stage = nullptr;
+    if (!(K & 1)) return QLD_OK;
+    if (int rc = ensure(c, c->dStage, (size_t)rows * K * 8)) return rc;
+    *stage = static_cast<uint64_t *>(c->dStage.p);
+    return QLD_OK;
+}
+
 // Copy host tables into the context's device buffers (rows padded to an even
 // word count, 16-byte aligned for TMA) on c->stream; *t describes them.
 // NULL bit counts are not copied (COUNTSTATES does not use them).
@@ -411,8 +444,10 @@ int stage_tables(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, cons
     int rc;
     if ((rc = ensure(c, c->dA, (size_t)m * Kp * 8)) || (rc = ensure(c, c->dbcA, (size_t)m * 4)))
         return rc;
-    CUDA_TRY(c, cudaMemcpy2DAsync(c->dA.p, Kp * 8, A, (size_t)K * 8, (size_t)K * 8, m,
-                                  cudaMemcpyHostToDevice, c->stream));
+    uint64_t *stage;
+    if ((rc = ensure_stage(c, K, symmetric || n < m ? m : n, &stage))) return rc;
+    if ((rc = upload_rows(c, static_cast<uint64_t *>(c->dA.p), Kp, A, K, m, stage, c->stream)))
+        return rc;
     if (bcA)
         CUDA_TRY(c, cudaMemcpyAsync(c->dbcA.p, bcA, (size_t)m * 4, cudaMemcpyHostToDevice,
                                     c->stream));
@@ -421,8 +456,9 @@ int stage_tables(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, cons
     if (!symmetric) {
         if ((rc = ensure(c, c->dB, (size_t)n * Kp * 8)) || (rc = ensure(c, c->dbcB, (size_t)n * 4)))
             return rc;
-        CUDA_TRY(c, cudaMemcpy2DAsync(c->dB.p, Kp * 8, B, (size_t)K * 8, (size_t)K * 8, n,
-                                      cudaMemcpyHostToDevice, c->stream));
+        if ((rc = upload_rows(c, static_cast<uint64_t *>(c->dB.p), Kp, B, K, n, stage,
+                              c->stream)))
+            return rc;
         if (bcB)
             CUDA_TRY(c, cudaMemcpyAsync(c->dbcB.p, bcB, (size_t)n * 4, cudaMemcpyHostToDevice,
                                         c->stream));
@@ -550,7 +586,8 @@ int qld_cuda_release(qld_ctx *c) {
                       &c->dMask[0], &c->dMask[1], &c->dHcnt[0], &c->dHcnt[1], &c->dHoff[0],
                       &c->dHoff[1], &c->dHval[0], &c->dHval[1], &c->vText,    &c->vSites,
                       &c->vValid,   &c->vSlash,   &c->vRoff,    &c->vRnd,     &c->vScratch,
-                      &c->vWords,   &c->vBc,      &c->vLen,     &c->vKeep,    &c->vErr};
+                      &c->vWords,   &c->vBc,      &c->vLen,     &c->vKeep,    &c->vErr,
+                      &c->dStage};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     HostBuf *hbufs[] = {&c->hMask[0], &c->hMask[1], &c->hOff[0], &c->hOff[1],
@@ -680,6 +717,8 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
         if ((rc = ensure(c, c->dOut[s], slot_rows * m * 4))) return rc;
         if (counts_out && (rc = ensure(c, c->dCnt[s], slot_rows * m * 4))) return rc;
     }
+    uint64_t *stage;
+    if ((rc = ensure_stage(c, K, !symmetric && m > band ? m : band, &stage))) return rc;
     // Tables go up in chunks of `band` rows on the h2d stream, an event after
     // each, so each band's kernel starts once the rows it reads are resident
     // and the host->device copies overlap the device->host results.  A single
@@ -694,15 +733,14 @@ int qld_cuda_ld(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, const
     CUDA_TRY(c, cudaMemcpyAsync(c->dbcA.p, bcA, (size_t)m * 4, cudaMemcpyHostToDevice, c->h2d));
     if (!symmetric) {
         CUDA_TRY(c, cudaMemcpyAsync(c->dbcB.p, bcB, (size_t)n * 4, cudaMemcpyHostToDevice, c->h2d));
-        CUDA_TRY(c, cudaMemcpy2DAsync(dA, Kp * 8, A, (size_t)K * 8, (size_t)K * 8, m,
-                                      cudaMemcpyHostToDevice, c->h2d));
+        if ((rc = upload_rows(c, dA, Kp, A, K, m, stage, c->h2d))) return rc;
     }
     for (int k = 0; k < nbands; ++k) {
         const int i = symmetric ? nbands - 1 - k : k;
         const int r0 = i * band, r1 = r0 + band < n ? r0 + band : n;
-        CUDA_TRY(c, cudaMemcpy2DAsync(dB + (size_t)r0 * Kp, Kp * 8, B + (size_t)r0 * K,
-                                      (size_t)K * 8, (size_t)K * 8, r1 - r0,
-                                      cudaMemcpyHostToDevice, c->h2d));
+        if ((rc = upload_rows(c, dB + (size_t)r0 * Kp, Kp, B + (size_t)r0 * K, K, r1 - r0, stage,
+                              c->h2d)))
+            return rc;
         CUDA_TRY(c, cudaEventRecord(c->h2d_ev[i], c->h2d));
     }
     for (int k = 0; k < nbands; ++k) {
@@ -1062,6 +1100,8 @@ int qld_cuda_ld_band(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, 
         if ((rc = ensure(c, c->dOut[s], (size_t)rows_blk * band * 4))) return rc;
         if (counts_band && (rc = ensure(c, c->dCnt[s], (size_t)rows_blk * band * 4))) return rc;
     }
+    uint64_t *stage;
+    if ((rc = ensure_stage(c, K, rows_blk, &stage))) return rc;
     // Host->device in row chunks on the h2d stream, an event after each.
     while ((int)c->h2d_ev.size() < nblk) {
         cudaEvent_t e;
@@ -1071,9 +1111,9 @@ int qld_cuda_ld_band(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, 
     CUDA_TRY(c, cudaMemcpyAsync(c->dbcA.p, bcA, (size_t)m * 4, cudaMemcpyHostToDevice, c->h2d));
     for (int i = 0; i < nblk; ++i) {
         const int r0 = i * rows_blk, r1 = r0 + rows_blk < m ? r0 + rows_blk : m;
-        CUDA_TRY(c, cudaMemcpy2DAsync(dA + (size_t)r0 * Kp, Kp * 8, A + (size_t)r0 * K,
-                                      (size_t)K * 8, (size_t)K * 8, r1 - r0,
-                                      cudaMemcpyHostToDevice, c->h2d));
+        if ((rc = upload_rows(c, dA + (size_t)r0 * Kp, Kp, A + (size_t)r0 * K, K, r1 - r0, stage,
+                              c->h2d)))
+            return rc;
         CUDA_TRY(c, cudaEventRecord(c->h2d_ev[i], c->h2d));
     }
     for (int bi = 0; bi < nblk; ++bi) {

@@ -120,4 +120,9 @@ cudaError_t launch_hits(const float *r2, long long ldr, int rows, int m, int row
                         float r2limit, uint32_t *mask, int W, long long *cnt, long long *off,
                         float *val, cudaStream_t st);
 
+// Rows of K words back to back (a staging copy of a host table) -> rows of
+// ldd >= K words, words past K zeroed (rows.cu).
+cudaError_t launch_pad_rows(uint64_t *dst, long long ldd, const uint64_t *src, int K,
+                            long long rows, cudaStream_t st);
+
 }  // namespace qld

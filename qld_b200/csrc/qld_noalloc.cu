@@ -144,13 +144,29 @@ extern "C" int qld_cuda_ld_noalloc(const uint64_t *A, const uint32_t *bcA, int m
     uint64_t *d_B = symmetric ? d_A : reinterpret_cast<uint64_t *>(scratch + o_B);
     float *d_band = reinterpret_cast<float *>(scratch + o_band);
 
+    // Each table goes up as one 1-D copy (row-pitched 2-D copies of a few KB
+    // per row run at about a third of the link rate): in place for even K,
+    // else through the r^2 band area (unused until the first kernel) and a
+    // padding kernel; row by row only when the band area cannot hold it.
+    auto upload = [&](uint64_t *dst, const uint64_t *src, int rows) -> int {
+        const size_t bytes = (size_t)rows * K * 8;
+        if (Kp == K) {
+            NA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        } else if (bytes <= kScratchBytes - o_band) {
+            uint64_t *stage = reinterpret_cast<uint64_t *>(scratch + o_band);
+            NA_TRY(cudaMemcpyAsync(stage, src, bytes, cudaMemcpyHostToDevice, st));
+            NA_TRY(launch_pad_rows(dst, Kp, stage, K, rows, st));
+        } else {
+            NA_TRY(cudaMemcpy2DAsync(dst, Kp * 8, src, (size_t)K * 8, (size_t)K * 8, rows,
+                                     cudaMemcpyHostToDevice, st));
+        }
+        return QLD_OK;
+    };
     NA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned), st));
-    NA_TRY(cudaMemcpy2DAsync(d_A, Kp * 8, A, (size_t)K * 8, (size_t)K * 8, m,
-                             cudaMemcpyHostToDevice, st));
+    if ((rc = upload(d_A, A, m))) return rc;
     NA_TRY(cudaMemcpyAsync(d_bcA, bcA, (size_t)m * 4, cudaMemcpyHostToDevice, st));
     if (!symmetric) {
-        NA_TRY(cudaMemcpy2DAsync(d_B, Kp * 8, B, (size_t)K * 8, (size_t)K * 8, n,
-                                 cudaMemcpyHostToDevice, st));
+        if ((rc = upload(d_B, B, n))) return rc;
         NA_TRY(cudaMemcpyAsync(d_bcB, bcB, (size_t)n * 4, cudaMemcpyHostToDevice, st));
     }
 
@@ -181,8 +197,8 @@ extern "C" int qld_cuda_ld_noalloc(const uint64_t *A, const uint32_t *bcA, int m
             NA_TRY(cudaMemcpyAsync(r2_out + (size_t)b0 * m, d_band, (size_t)(b1 - b0) * m * 4,
                                    cudaMemcpyDeviceToHost, st));
         } else {
-            for (int r0 = b0; r0 < b1; r0 += 128) {
-                const int r1 = r0 + 128 < b1 ? r0 + 128 : b1;
+            for (int r0 = b0; r0 < b1; r0 += 512) {
+                const int r1 = r0 + 512 < b1 ? r0 + 512 : b1;
                 NA_TRY(cudaMemcpy2DAsync(r2_out + (size_t)r0 * m + r0, (size_t)m * 4,
                                          d_band + (size_t)(r0 - b0) * m + r0, (size_t)m * 4,
                                          (size_t)(m - r0) * 4, r1 - r0, cudaMemcpyDeviceToHost,

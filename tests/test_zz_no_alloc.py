@@ -43,7 +43,8 @@ def _noalloc(lib, A, bcA, B, bcB, S, symmetric):
 @pytest.mark.parametrize("m,n,N,sym", [
     (2048, 2048, 4096, True),    # the all-pairs workload
     (3000, 3000, 4096, True),    # several output bands through the scratch
-    (700, 450, 9000, False),     # two regions
+    (700, 450, 9000, False),     # two regions (K = 141: rows padded on the device)
+    (1500, 1500, 2049, True),    # single region, K = 33
 ])
 def test_noalloc_matches_regular_entry_point_twice(m, n, N, sym):
     lib = _lib()
