@@ -482,9 +482,29 @@ int qld_srv_add_table(qld_server *s, const uint64_t *A, const uint32_t *bc, int 
         return srv_err(s, QLD_ERR_NOMEM, "table of %d x %d words does not fit", m, K);
     }
     // cudaMemcpyDefault: the table may come from host or from device memory.
-    if (cudaMemcpy2D(T.d, T.lda * 8, A, (size_t)K * 8, (size_t)K * 8, m, cudaMemcpyDefault) !=
-            cudaSuccess ||
-        cudaMemcpy(T.bc, bc, (size_t)m * 4, cudaMemcpyDefault) != cudaSuccess) {
+    // One 1-D copy, in place for even K, else into a staging buffer that a
+    // kernel re-pitches (row-pitched 2-D copies from the host run at about a
+    // third of the link rate); row by row only if the staging buffer does
+    // not fit.
+    const size_t bytes = (size_t)m * K * 8;
+    bool ok = cudaMemcpy(T.bc, bc, (size_t)m * 4, cudaMemcpyDefault) == cudaSuccess;
+    if (ok && T.lda == K) {
+        ok = cudaMemcpy(T.d, A, bytes, cudaMemcpyDefault) == cudaSuccess;
+    } else if (ok) {
+        void *stage = nullptr;
+        if (cudaMalloc(&stage, bytes) == cudaSuccess) {
+            ok = cudaMemcpy(stage, A, bytes, cudaMemcpyDefault) == cudaSuccess &&
+                 launch_pad_rows(T.d, T.lda, static_cast<const uint64_t *>(stage), K, m, 0) ==
+                     cudaSuccess &&
+                 cudaStreamSynchronize(0) == cudaSuccess;
+            cudaFree(stage);
+        } else {
+            cudaGetLastError();
+            ok = cudaMemcpy2D(T.d, T.lda * 8, A, (size_t)K * 8, (size_t)K * 8, m,
+                              cudaMemcpyDefault) == cudaSuccess;
+        }
+    }
+    if (!ok) {
         cudaGetLastError();
         cudaFree(T.d);
         cudaFree(T.bc);
