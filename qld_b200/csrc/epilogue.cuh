@@ -241,5 +241,41 @@ __device__ __forceinline__ void chunk_f32(uint32_t (&v)[32], uint32_t taddr, con
     }
 }
 
+// A warp's share of a task summary (BatchSummary): fold() takes the r^2
+// values chunk_f32 left in v (A row a against B rows b0 + t), flush() sums
+// the warp's lanes and adds them to the task's summary with three atomics.
+struct SumAcc {
+    double sum = 0.0;
+    unsigned long long cnt = 0;
+    float mx = 0.0f;
+    __device__ __forceinline__ void fold(const uint32_t (&v)[32], int b0, int a, bool a_ok,
+                                         int n, int symmetric, float threshold) {
+        if (!a_ok) return;
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+            const int b = b0 + t;
+            const float r = __uint_as_float(v[t]);
+            // a pair of the task, and not NaN or the 123.456 sentinel
+            if (b < n && (!symmetric || a > b) && r < 100.0f) {
+                sum += (double)r;
+                cnt += r >= threshold;
+                mx = fmaxf(mx, r);
+            }
+        }
+    }
+    __device__ __forceinline__ void flush(BatchSummary *out) {
+        for (int o = 16; o > 0; o >>= 1) {
+            sum += __shfl_down_sync(0xffffffffu, sum, o);
+            cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+            mx = fmaxf(mx, __shfl_down_sync(0xffffffffu, mx, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&out->sum, sum);
+            atomicAdd(&out->n_above, cnt);
+            atomicMax(&out->max_bits, __float_as_uint(mx));
+        }
+    }
+};
+
 }  // namespace epi
 }  // namespace qld

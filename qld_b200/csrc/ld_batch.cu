@@ -444,6 +444,7 @@ k_ld_batch(const BatchParams bp) {
                 // columns past the tile's 240 B rows are read but not written
                 const int n_tile = it.tb * BN + BN < J.n ? it.tb * BN + BN : J.n;
                 const int dlo = diag_lo(J.symmetric, 0), dhi = diag_hi(0);
+                epi::SumAcc acc;
 #pragma unroll 1
                 for (int c = colh; c < 8; c += 2) {
                     uint32_t v[32];
@@ -453,6 +454,9 @@ k_ld_batch(const BatchParams bp) {
                         epi::chunk_f32(v, tbase + (uint32_t)(c * 32), raf, colsf, c * 32,
                                        it.tb * BN + c * 32, a, a_ok, n_tile, dlo, dhi, J.r2,
                                        J.ldr, J.counts, J.ldc, 0, J.S);
+                        if (J.summary)
+                            acc.fold(v, it.tb * BN + c * 32, a, a_ok, J.n, J.symmetric,
+                                     J.threshold);
                     } else {
 #pragma unroll
                         for (int t = 0; t < 32; ++t)     // F32 accumulator -> count
@@ -465,6 +469,7 @@ k_ld_batch(const BatchParams bp) {
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive_rank(smem_u32(&accempty[ab]), 0);
+                if (MODE == R2_EXACT && J.summary) acc.flush(J.summary);
             }
             __syncwarp();
             if (lane == 0) release_item(qi);

@@ -38,6 +38,18 @@ struct LdParams {
     long long timeout_cycles;
 };
 
+// Per-task summary a batched launch folds into its epilogue (R2_EXACT):
+// over the task's pairs (a > b in a single region, all of them for two
+// regions), the r^2 values below 100 (NaN and the 123.456 sentinel left
+// out): their sum, how many reach the threshold, and the largest as float
+// bits (r^2 >= 0, so bit order is value order).  Zeroed before the launch.
+struct BatchSummary {
+    double sum;
+    unsigned long long n_above;
+    unsigned int max_bits;
+    unsigned int pad;
+};
+
 // ------------------------------------------------------------- PTX wrappers --
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {

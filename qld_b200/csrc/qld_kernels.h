@@ -57,6 +57,8 @@ struct BatchJob {
     long long ldr, ldc;
     long long item0;
     int m, n, K, S, symmetric;
+    float threshold;           // with summary: the n_above threshold
+    BatchSummary *summary;     // NULL: none
 };
 
 struct BatchParams {

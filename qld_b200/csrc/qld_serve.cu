@@ -5,9 +5,9 @@
 //              first-fit device pool while it has room (a query that does
 //              not fit waits; later ones wait behind it);
 //   batching   the admitted queries become the tasks of one persistent
-//              batched launch (launch_batch, ld_batch.cu) followed by a
-//              summary kernel, on the first free stream slot -- while the
-//              batches of earlier slots are still running;
+//              batched launch (launch_batch, ld_batch.cu), whose epilogue
+//              also folds each query's summary, on the first free stream
+//              slot -- while the batches of earlier slots are still running;
 //   completion a host function enqueued after each batch wakes the worker,
 //              which publishes results, copies summaries out and returns pool
 //              memory, so the next pending queries can be admitted.
@@ -36,65 +36,7 @@ namespace {
 
 constexpr int kMaxJobsPerBatch = 1024;
 
-struct Summary {
-    double sum;
-    unsigned long long n_above;
-    unsigned int max_bits;
-    unsigned int pad;
-};
-
-struct SumJob {
-    const float *r2;
-    long long ldr;
-    int n, m, symmetric;
-    float threshold;
-    Summary *out;
-};
-
-// Per query: the pairs a single region defines are a > b (the diagonal is
-// not a pair), all of them for two regions.
-__global__ void __launch_bounds__(256) k_summary(const SumJob *jobs) {
-    const SumJob J = jobs[blockIdx.y];
-    const long long total = (long long)J.n * J.m;
-    double sum = 0.0;
-    unsigned long long cnt = 0;
-    float mx = 0.0f;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(e / J.m), j = (int)(e % J.m);
-        if (J.symmetric && j <= i) continue;
-        const float v = J.r2[(long long)i * J.ldr + j];
-        if (!(v < 100.0f)) continue;   // NaN and the 123.456 sentinel
-        sum += v;
-        cnt += v >= J.threshold;
-        mx = fmaxf(mx, v);
-    }
-    __shared__ double s_sum[8];
-    __shared__ unsigned long long s_cnt[8];
-    __shared__ float s_max[8];
-    for (int o = 16; o > 0; o >>= 1) {
-        sum += __shfl_down_sync(0xffffffffu, sum, o);
-        cnt += __shfl_down_sync(0xffffffffu, cnt, o);
-        mx = fmaxf(mx, __shfl_down_sync(0xffffffffu, mx, o));
-    }
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
-        s_sum[w] = sum;
-        s_cnt[w] = cnt;
-        s_max[w] = mx;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
-            sum += s_sum[k];
-            cnt += s_cnt[k];
-            mx = fmaxf(mx, s_max[k]);
-        }
-        atomicAdd(&J.out->sum, sum);
-        atomicAdd(&J.out->n_above, cnt);
-        atomicMax(&J.out->max_bits, __float_as_uint(mx));   // r^2 >= 0: bit order = value order
-    }
-}
+using Summary = BatchSummary;   // per query, folded by the batch kernel's epilogue
 
 struct Table {
     uint64_t *d = nullptr;
@@ -118,7 +60,6 @@ struct Query {
 struct Slot {
     cudaStream_t st = nullptr;
     BatchJob *dJobs = nullptr, *hJobs = nullptr;
-    SumJob *dSumJobs = nullptr, *hSumJobs = nullptr;
     Summary *dSum = nullptr, *hSum = nullptr;
     unsigned long long *dQueue = nullptr;
     unsigned *dStatus = nullptr, *hStatus = nullptr;
@@ -265,16 +206,12 @@ int launch_slot(qld_server *s, int si) {
         J.ldr = m;
         J.item0 = items;
         J.m = m; J.n = n; J.K = T.K; J.S = T.S; J.symmetric = sym;
+        J.threshold = q.q.threshold;
+        J.summary = sl.dSum + i;
         items += tiles[i];
-        SumJob &Sj = sl.hSumJobs[k];
-        Sj.r2 = out; Sj.ldr = m; Sj.n = n; Sj.m = m; Sj.symmetric = sym;
-        Sj.threshold = q.q.threshold;
-        Sj.out = sl.dSum + i;
     }
     cudaStream_t st = sl.st;
     if (cudaMemcpyAsync(sl.dJobs, sl.hJobs, sizeof(BatchJob) * nj, cudaMemcpyHostToDevice, st) ||
-        cudaMemcpyAsync(sl.dSumJobs, sl.hSumJobs, sizeof(SumJob) * nj, cudaMemcpyHostToDevice,
-                        st) ||
         cudaMemsetAsync(sl.dQueue, 0, sizeof(unsigned long long), st) ||
         cudaMemsetAsync(sl.dStatus, 0, sizeof(unsigned), st) ||
         cudaMemsetAsync(sl.dSum, 0, sizeof(Summary) * nj, st))
@@ -287,8 +224,6 @@ int launch_slot(qld_server *s, int si) {
     bp.status = sl.dStatus;
     bp.timeout_cycles = 4000000000LL;
     if (items > 0 && launch_batch(bp, R2_EXACT, 0, st) != cudaSuccess) return QLD_ERR_CUDA;
-    k_summary<<<dim3(64, nj), 256, 0, st>>>(sl.dSumJobs);
-    if (cudaGetLastError() != cudaSuccess) return QLD_ERR_CUDA;
     for (int i = 0; i < nj; ++i) {
         const Query &q = sl.qs[i];
         if (q.q.host_r2)
@@ -397,9 +332,9 @@ void worker_main(qld_server *s) {
 
 void free_slot_buffers(Slot &sl) {
     if (sl.st) cudaStreamSynchronize(sl.st);
-    cudaFree(sl.dJobs); cudaFree(sl.dSumJobs); cudaFree(sl.dSum); cudaFree(sl.dQueue);
+    cudaFree(sl.dJobs); cudaFree(sl.dSum); cudaFree(sl.dQueue);
     cudaFree(sl.dStatus);
-    cudaFreeHost(sl.hJobs); cudaFreeHost(sl.hSumJobs); cudaFreeHost(sl.hSum);
+    cudaFreeHost(sl.hJobs); cudaFreeHost(sl.hSum);
     cudaFreeHost(sl.hStatus);
     if (sl.st) cudaStreamDestroy(sl.st);
 }
@@ -439,12 +374,10 @@ int qld_srv_create(int device, size_t pool_bytes, int max_inflight, qld_server *
         if (rc) break;
         if (cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) ||
             cudaMalloc(&sl.dJobs, sizeof(BatchJob) * kMaxJobsPerBatch) ||
-            cudaMalloc(&sl.dSumJobs, sizeof(SumJob) * kMaxJobsPerBatch) ||
             cudaMalloc(&sl.dSum, sizeof(Summary) * kMaxJobsPerBatch) ||
             cudaMalloc(&sl.dQueue, sizeof(unsigned long long)) ||
             cudaMalloc(&sl.dStatus, sizeof(unsigned)) ||
             cudaMallocHost(&sl.hJobs, sizeof(BatchJob) * kMaxJobsPerBatch) ||
-            cudaMallocHost(&sl.hSumJobs, sizeof(SumJob) * kMaxJobsPerBatch) ||
             cudaMallocHost(&sl.hSum, sizeof(Summary) * kMaxJobsPerBatch) ||
             cudaMallocHost(&sl.hStatus, sizeof(unsigned)))
             rc = QLD_ERR_NOMEM;
