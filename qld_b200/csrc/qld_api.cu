@@ -403,34 +403,44 @@ int launch_states_range(qld_ctx *c, const Task &t, int b0, int b1, uint8_t *out,
     return QLD_OK;
 }
 
+// Rows of odd K go through the staging buffer this many at a time, so it
+// stays small next to the tables themselves.
+constexpr long long kStageRows = 8192;
+
 // Host rows of K words -> device rows of ldd words (ldd = K, or K + 1 to
 // keep rows 16-byte aligned).  A row-pitched 2-D copy moves rows of a few KB
 // at about a third of the link rate (19 vs 55 GB/s for 2,080-byte rows on a
 // B200) and slows device->host copies running beside it to a crawl, so the
-// rows go up as one 1-D copy: in place when ldd == K, else into `stage`
-// (rows * K words, reused by the next upload on the same stream) and a
-// kernel spreads them to the padded pitch.
+// rows go up as 1-D copies: in place when ldd == K, else kStageRows at a
+// time into `stage` (reused in stream order) and a kernel spreads them to
+// the padded pitch.
 int upload_rows(qld_ctx *c, uint64_t *dst, long long ldd, const uint64_t *src, int K,
                 long long rows, uint64_t *stage, cudaStream_t st) {
     if (rows <= 0) return QLD_OK;
-    const size_t bytes = (size_t)rows * K * 8;
     if (ldd == K) {
-        CUDA_TRY(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(c, cudaMemcpyAsync(dst, src, (size_t)rows * K * 8, cudaMemcpyHostToDevice, st));
         return QLD_OK;
     }
-    CUDA_TRY(c, cudaMemcpyAsync(stage, src, bytes, cudaMemcpyHostToDevice, st));
-    const cudaError_t e = launch_pad_rows(dst, ldd, stage, K, rows, st);
-    if (e != cudaSuccess)
-        return set_err(c, QLD_ERR_CUDA, "row padding launch failed: %s", cudaGetErrorString(e));
-    c->stats.kernel_launches++;
+    for (long long r0 = 0; r0 < rows; r0 += kStageRows) {
+        const long long nr = rows - r0 < kStageRows ? rows - r0 : kStageRows;
+        CUDA_TRY(c, cudaMemcpyAsync(stage, src + r0 * K, (size_t)nr * K * 8,
+                                    cudaMemcpyHostToDevice, st));
+        const cudaError_t e = launch_pad_rows(dst + r0 * ldd, ldd, stage, K, nr, st);
+        if (e != cudaSuccess)
+            return set_err(c, QLD_ERR_CUDA, "row padding launch failed: %s",
+                           cudaGetErrorString(e));
+        c->stats.kernel_launches++;
+    }
     return QLD_OK;
 }
 
-// The staging buffer upload_rows needs for up to `rows` rows (none for even K).
+// The staging buffer upload_rows needs for tables of up to `rows` rows
+// (none for even K).
 int ensure_stage(qld_ctx *c, int K, long long rows, uint64_t **stage) {
     *stage = nullptr;
     if (!(K & 1)) return QLD_OK;
-    if (int rc = ensure(c, c->dStage, (size_t)rows * K * 8)) return rc;
+    const long long r = rows < kStageRows ? rows : kStageRows;
+    if (int rc = ensure(c, c->dStage, (size_t)r * K * 8)) return rc;
     *stage = static_cast<uint64_t *>(c->dStage.p);
     return QLD_OK;
 }
