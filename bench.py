@@ -160,6 +160,18 @@ class ClockSampler:
                 "window": "timed region" if inside else "whole run (no sample inside the region)"}
 
 
+def measured_peaks():
+    """HBM copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json
+    beside this file), else an earlier measurement on the same pool
+    (6.65 TB/s)."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return {"hbm_gbs": float(json.load(f)["hbm_gbs"]), "source": "MEASURED_PEAKS.json"}
+    except (OSError, ValueError, KeyError):
+        return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
 def kernel_roofline(ctx, variant, bitops, kern_ms, dev):
     """Roofline of the counts kernel against the measured rate of the pipe it
     runs on: the tensor pipe of its MMA kind (qld_cuda_measure_mma_peak,
@@ -390,7 +402,10 @@ def ours_arm(args, rank, world, local_rank):
     roof["traffic"] = measured_traffic(variant, cfg["workload"], sm_pair)
     roof["algorithmic_bytes_per_launch"] = alg_bytes
     roof["kernel_ms"] = kern_ms
-    roof["hbm_frac_of_measured"] = (alg_bytes / (kern_ms * 1e-3) / 1e9) / 6538.9
+    mp = measured_peaks()
+    roof["hbm_frac_of_measured"] = (alg_bytes / (kern_ms * 1e-3) / 1e9) / mp["hbm_gbs"]
+    roof["hbm_peak_gbs"] = mp["hbm_gbs"]
+    roof["hbm_peak_source"] = mp["source"]
 
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
