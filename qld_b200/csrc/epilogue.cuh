@@ -54,6 +54,7 @@ struct ARow {
     uint32_t c;
     double inv, cd;     // exact
     RowRef ref;         // reference
+    float Sf, rSf;      // reference: (float)S and its correctly rounded reciprocal
 };
 
 template <int MODE>
@@ -65,6 +66,8 @@ __device__ __forceinline__ ARow make_arow(uint32_t c, int S) {
         r.cd = (double)c;
     } else {
         r.ref = row_ref(c, S);
+        r.Sf = (float)S;
+        r.rSf = __frcp_rn(r.Sf);
     }
     return r;
 }
@@ -93,16 +96,141 @@ __device__ __forceinline__ float pair_r2(uint32_t cnt, const ARow &ra, const Col
     }
 }
 
+// ------------------------------------------- R2_REFERENCE without branches --
+//
+// The reference's operation sequence (r2_reference) rearranged so that a
+// chunk's 32 pairs run branch-free and with fewer conversions:
+//  * v3 = fl32(cab / S) by Markstein's FMA correction: q = RN(cab * y) with
+//    y = RN(1/S), then RN(q + (cab - q*S) * y), the residual exact in one
+//    FMA.  With y the correctly rounded reciprocal this is the correctly
+//    rounded quotient (P. Markstein, IBM J. Res. Dev. 34(1), 1990); cab and
+//    S are integers <= 2^24, exact in FP32.
+//  * fl32(RN64(x / den)), the reference's FP64 division rounded to float:
+//    Newton-Raphson reciprocal of den (three steps from the rcp.approx.ftz.f64
+//    seed, each squaring the relative error), q = x * y with one residual
+//    correction, then a rounding test in the manner of Ziv: if q lies more
+//    than 64 FP64 ulps from the nearest FP32 rounding midpoint, fl32(q) =
+//    fl32(RN64(x / den)).  Pairs failing it (about 3 in 10^7 at realistic S;
+//    ~10^-4 at S <= 100, whose simple fractions meet midpoints more often)
+//    or whose quotient would be an FP32 subnormal are flagged and
+//    recomputed with r2_reference.
+//  * (double)r > 1.0001 is r > 1 + 838 * 2^-23, the largest float not above
+//    1.0001.  x / 0 (a fixed SNP) is +inf, hence 123.456; 0 / 0 is the
+//    x86 default NaN the reference's build produces (0xFFC00000).
+// Moving the FP32<->FP64 conversions to integer bit-field arithmetic and
+// seeding the reciprocal from the bit pattern instead (four Newton steps)
+// measured slower: 5.16 / 5.42 ms against 4.85 / 4.95 ms on the single region.
+__device__ __forceinline__ double rcp_seed(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    return y;
+}
+
+__device__ __forceinline__ float r2_reference_fast(float cab, const RowRef &A, uint32_t cB,
+                                                   float vB, double omB, float Sf, float rSf,
+                                                   bool &redo) {
+    const float q0 = __fmul_rn(cab, rSf);
+    const float v3 = __fmaf_rn(__fmaf_rn(-q0, Sf, cab), rSf, q0);
+    const float p12 = __fmul_rn(A.v, vB);
+    const float d = __fsub_rn(v3, p12);
+    const float r = __fmul_rn(d, d);
+    const double den = __dmul_rn(__dmul_rn((double)p12, A.one_minus), omB);
+    const double x = (double)r;
+    double y = rcp_seed(den);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) y = __fma_rn(y, __fma_rn(-den, y, 1.0), y);
+    double q = __dmul_rn(x, y);
+    q = __fma_rn(__fma_rn(-q, den, x), y, q);
+    const long long mid = (long long)(__double_as_longlong(q) & 0x1FFFFFFFLL) - (1LL << 28);
+    const bool dz = den == 0.0;
+    const bool zero = A.c == 0u || cB == 0u;
+    redo = !zero && !dz &&
+           (!(den > 0x1p-1000 && den < 0x1p1000) || (q != 0.0 && q < 0x1p-126) ||
+            (mid >= -64 && mid <= 64));
+    float f = dz ? __uint_as_float(r == 0.0f ? 0xFFC00000u : 0x7F800000u) : __double2float_rn(q);
+    if (f > __uint_as_float(0x3F800000u + 838u)) f = 123.456f;
+    return zero ? 0.0f : f;
+}
+
+// The reference-mode chunk: every pair on the fast path, the flagged ones
+// (their counts kept in v, a bit in `redo`) redone with r2_reference.
+// FLOATCNT: v holds each count as F32 bits (the 4-bit kernels' accumulators),
+// else as an integer shifted left by SHIFT.
+template <int SHIFT, bool FLOATCNT>
+__device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARow &ra, const Cols &f,
+                                          int bl0, int b0, int a, bool a_ok, int n, int dlo,
+                                          int dhi, float *r2, long long ldr, uint32_t *counts,
+                                          long long ldc, int row0, int S) {
+    uint32_t *oc = (counts && a_ok) ? counts + (long long)(b0 - row0) * ldc + a : nullptr;
+    uint32_t redo = 0;
+    if (S <= (1 << 24)) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+            const float cf = FLOATCNT ? __uint_as_float(v[t]) : (float)(v[t] >> SHIFT);
+            const int b = b0 + t;
+            if (oc && b < n && a - b >= dlo && a - b <= dhi)
+                oc[(long long)t * ldc] = FLOATCNT ? (uint32_t)cf : v[t] >> SHIFT;
+            bool rd;
+            const float r = r2_reference_fast(cf, ra.ref, f.c[bl0 + t], f.v[bl0 + t],
+                                              f.d0[bl0 + t], ra.Sf, ra.rSf, rd);
+            if (rd) v[t] = FLOATCNT ? (uint32_t)cf : v[t] >> SHIFT;
+            else v[t] = __float_as_uint(r);
+            redo |= (uint32_t)rd << t;
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+            const uint32_t cnt = FLOATCNT ? (uint32_t)__uint_as_float(v[t]) : v[t] >> SHIFT;
+            const int b = b0 + t;
+            if (oc && b < n && a - b >= dlo && a - b <= dhi) oc[(long long)t * ldc] = cnt;
+            v[t] = cnt;
+        }
+        redo = 0xFFFFFFFFu;
+    }
+    if (!a_ok) redo = 0;
+    if (__any_sync(0xffffffffu, redo != 0)) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+            const bool rd = (redo >> t) & 1u;
+            if (__any_sync(0xffffffffu, rd) && rd) {
+                RowRef rb;
+                rb.c = f.c[bl0 + t];
+                rb.v = f.v[bl0 + t];
+                rb.one_minus = f.d0[bl0 + t];
+                v[t] = __float_as_uint(r2_reference(v[t], ra.ref, rb, S));
+            }
+        }
+    }
+    if (!a_ok) return;
+    float *o = r2 + (long long)(b0 - row0) * ldr + a;
+    const bool interior = (b0 + 31 < n) && (a - (b0 + 31) >= dlo) && (a - b0 <= dhi);
+    if (interior) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) o[(long long)t * ldr] = __uint_as_float(v[t]);
+    } else {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+            const int b = b0 + t;
+            if (b < n && a - b >= dlo && a - b <= dhi) o[(long long)t * ldr] = __uint_as_float(v[t]);
+        }
+    }
+}
+
 // One 32-column chunk: accumulators v[t] (holding count << shift) of A row a
 // against B rows b0 + t (local columns bl0 + t).  Output element (b, a) goes
 // to r2[(b - row0) * ldr + a] (and counts likewise).  Only entries inside the
 // task (b < n, a < m) and the diagonal window dlo <= a - b <= dhi are
 // written (a single region: a >= b; a band: 1 <= a - b <= W).
 template <int MODE, int SHIFT>
-__device__ __forceinline__ void chunk(const uint32_t (&v)[32], const ARow &ra, const Cols &f,
+__device__ __forceinline__ void chunk(uint32_t (&v)[32], const ARow &ra, const Cols &f,
                                       int bl0, int b0, int a, bool a_ok, int n, int dlo,
                                       int dhi, float *r2, long long ldr, uint32_t *counts,
                                       long long ldc, int row0, int S) {
+    if constexpr (MODE == R2_REFERENCE) {
+        chunk_ref<SHIFT, false>(v, ra, f, bl0, b0, a, a_ok, n, dlo, dhi, r2, ldr, counts, ldc,
+                                row0, S);
+        return;
+    }
     if (!a_ok) return;
     const double S_d = (double)S;
     float *o = r2 + (long long)(b0 - row0) * ldr + a;

@@ -458,10 +458,8 @@ k_ld_batch(const BatchParams bp) {
                             acc.fold(v, it.tb * BN + c * 32, a, a_ok, J.n, J.symmetric,
                                      J.threshold);
                     } else {
-#pragma unroll
-                        for (int t = 0; t < 32; ++t)     // F32 accumulator -> count
-                            v[t] = (uint32_t)__uint_as_float(v[t]);
-                        epi::chunk<MODE, 0>(v, ra, cols, c * 32, it.tb * BN + c * 32, a, a_ok,
+                        // the F32 accumulators hold the counts as floats
+                        epi::chunk_ref<0, true>(v, ra, cols, c * 32, it.tb * BN + c * 32, a, a_ok,
                                             n_tile, dlo, dhi, J.r2, J.ldr, J.counts, J.ldc, 0,
                                             J.S);
                     }

@@ -372,10 +372,8 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                                        tb * BN + c * 32, a, a_ok, n_tile,
                                        dlo, dhi, p.r2, p.ldr, p.counts, p.ldc, p.out_row0, p.S);
                     } else {
-#pragma unroll
-                        for (int t = 0; t < 32; ++t)     // F32 accumulator -> count
-                            v[t] = (uint32_t)__uint_as_float(v[t]);
-                        epi::chunk<MODE, 0>(v, ra, cols, c * 32, tb * BN + c * 32, a, a_ok,
+                        // the F32 accumulators hold the counts as floats
+                        epi::chunk_ref<0, true>(v, ra, cols, c * 32, tb * BN + c * 32, a, a_ok,
                                             n_tile, dlo, dhi, p.r2, p.ldr, p.counts, p.ldc,
                                             p.out_row0, p.S);
                     }

@@ -277,3 +277,47 @@ def test_threshold_with_inconsistent_bitcounts(gpu_ctx, kernel):
     d = np.diag(want)
     assert (d == 123.456).sum() == 4 and np.isnan(d).sum() == 1 and (d == 0).sum() == 1
     assert_r2_close(r2, want)
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_reference_mode_edge_pairs_bit_identical(gpu_ctx, kernel):
+    """Reference-mode r^2 bit for bit against the reference's operation
+    sequence on the pairs its special cases and the kernels' rounding tests
+    single out: the sentinel threshold, fixed SNPs (x/0 -> 123.456 and 0/0 ->
+    the reference build's NaN), monomorphic SNPs, and a small sample count
+    (S = 50) whose simple fractions often sit near FP32 rounding midpoints."""
+    S, K = 1000, 16
+    n = len(THRESHOLD_CASES)
+    bits = np.zeros((n, K * 64), np.uint8)
+    for i, (c, _, _) in enumerate(THRESHOLD_CASES):
+        bits[i, :c] = 1
+    rows = np.packbits(bits, axis=1).reshape(n, K, 8).view(">u8").reshape(n, K)
+    rows = rows.astype(np.uint64)
+    bcA = np.array([t[1] for t in THRESHOLD_CASES], np.uint32)
+    bcB = np.array([t[2] for t in THRESHOLD_CASES], np.uint32)
+    rng = np.random.default_rng(7)
+    S2 = 50
+    small = np.zeros((300, 64), np.uint8)
+    for i in range(300):
+        small[i, :S2] = rng.random(S2) < rng.uniform(0.0, 1.0)
+    small[0, :S2] = 1            # fixed SNP
+    small[1, :] = 0              # monomorphic
+    srows = np.packbits(small, axis=1).reshape(300, 1, 8).view(">u8").reshape(300, 1)
+    srows = srows.astype(np.uint64)
+    sbc = oracle.bitcounts(srows)
+    set_kernel(gpu_ctx, kernel)
+    gpu_ctx.set_option(api.OPT_R2_MODE, api.R2_REFERENCE)
+    try:
+        r2 = gpu_ctx.ld(rows, bcA, rows.copy(), bcB, S=S)
+        r2s = gpu_ctx.ld(srows, sbc, S=S2)
+    finally:
+        gpu_ctx.set_option(api.OPT_R2_MODE, api.R2_EXACT)
+        gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
+        gpu_ctx.set_option(api.OPT_SM_PAIR, 0)
+    want = oracle.r2_reference(bcA, bcB, oracle.counts(rows, rows), S, fma_contract=False)
+    assert np.isnan(np.diag(want)).sum() == 1
+    assert np.array_equal(r2.view(np.uint32), want.view(np.uint32))
+    wants = oracle.r2_reference(sbc, sbc, oracle.counts(srows), S2, fma_contract=False)
+    mask = lower_mask(300, 300)
+    assert np.isnan(wants[mask]).any()
+    assert np.array_equal(r2s[mask].view(np.uint32), wants[mask].view(np.uint32))
