@@ -10,7 +10,8 @@
 //                 r^2 = (D*D) * (1/varA * 1/varB) with one rounding to FP32.
 //                 No 64-bit integer arithmetic and one conversion per pair.
 //   R2_REFERENCE  the reference's float/double operation sequence
-//                 (qld_device.cuh: r2_reference), bit for bit.
+//                 (qld_device.cuh: r2_reference), bit for bit, evaluated
+//                 branch-free (r2_reference_fast) with a rare fallback.
 // Per-column factors live in shared memory (filled once per tile); the
 // per-row (A) factors in registers.
 #pragma once
@@ -77,23 +78,15 @@ __device__ __forceinline__ double u32_to_f64(uint32_t x) {
     return __hiloint2double(0x43300000, (int)x) - 4503599627370496.0;
 }
 
-template <int MODE>
-__device__ __forceinline__ float pair_r2(uint32_t cnt, const ARow &ra, const Cols &f, int bl,
-                                         double S_d, int S) {
-    if (MODE == R2_EXACT) {
-        const double cbd = f.d1[bl];
-        const double D = fma(S_d, u32_to_f64(cnt), -(ra.cd * cbd));
-        const double r = (D * D) * (ra.inv * f.d0[bl]);
-        if (ra.c == 0u || cbd == 0.0) return 0.0f;
-        if (r > 1.0001) return 123.456f;
-        return __double2float_rn(r);
-    } else {
-        RowRef rb;
-        rb.c = f.c[bl];
-        rb.v = f.v[bl];
-        rb.one_minus = f.d0[bl];
-        return r2_reference(cnt, ra.ref, rb, S);
-    }
+// R2_EXACT from an integer count, in FP64.
+__device__ __forceinline__ float pair_r2_exact(uint32_t cnt, const ARow &ra, const Cols &f,
+                                               int bl, double S_d) {
+    const double cbd = f.d1[bl];
+    const double D = fma(S_d, u32_to_f64(cnt), -(ra.cd * cbd));
+    const double r = (D * D) * (ra.inv * f.d0[bl]);
+    if (ra.c == 0u || cbd == 0.0) return 0.0f;
+    if (r > 1.0001) return 123.456f;
+    return __double2float_rn(r);
 }
 
 // ------------------------------------------- R2_REFERENCE without branches --
@@ -229,28 +222,28 @@ __device__ __forceinline__ void chunk(uint32_t (&v)[32], const ARow &ra, const C
     if constexpr (MODE == R2_REFERENCE) {
         chunk_ref<SHIFT, false>(v, ra, f, bl0, b0, a, a_ok, n, dlo, dhi, r2, ldr, counts, ldc,
                                 row0, S);
-        return;
-    }
-    if (!a_ok) return;
-    const double S_d = (double)S;
-    float *o = r2 + (long long)(b0 - row0) * ldr + a;
-    uint32_t *oc = counts ? counts + (long long)(b0 - row0) * ldc + a : nullptr;
-    const bool interior = (b0 + 31 < n) && (a - (b0 + 31) >= dlo) && (a - b0 <= dhi);
-    if (interior) {
-#pragma unroll
-        for (int t = 0; t < 32; ++t) {
-            const uint32_t cnt = v[t] >> SHIFT;
-            o[(long long)t * ldr] = pair_r2<MODE>(cnt, ra, f, bl0 + t, S_d, S);
-            if (oc) oc[(long long)t * ldc] = cnt;
-        }
     } else {
+        if (!a_ok) return;
+        const double S_d = (double)S;
+        float *o = r2 + (long long)(b0 - row0) * ldr + a;
+        uint32_t *oc = counts ? counts + (long long)(b0 - row0) * ldc + a : nullptr;
+        const bool interior = (b0 + 31 < n) && (a - (b0 + 31) >= dlo) && (a - b0 <= dhi);
+        if (interior) {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
-            const int b = b0 + t;
-            if (b < n && a - b >= dlo && a - b <= dhi) {
+            for (int t = 0; t < 32; ++t) {
                 const uint32_t cnt = v[t] >> SHIFT;
-                o[(long long)t * ldr] = pair_r2<MODE>(cnt, ra, f, bl0 + t, S_d, S);
+                o[(long long)t * ldr] = pair_r2_exact(cnt, ra, f, bl0 + t, S_d);
                 if (oc) oc[(long long)t * ldc] = cnt;
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < 32; ++t) {
+                const int b = b0 + t;
+                if (b < n && a - b >= dlo && a - b <= dhi) {
+                    const uint32_t cnt = v[t] >> SHIFT;
+                    o[(long long)t * ldr] = pair_r2_exact(cnt, ra, f, bl0 + t, S_d);
+                    if (oc) oc[(long long)t * ldc] = cnt;
+                }
             }
         }
     }
@@ -303,7 +296,7 @@ __device__ __forceinline__ float pair_r2_f32(float c, float S_f, const ARowF &ra
     return (ra.zero || col.x == 0.0f) ? 0.0f : r;
 }
 
-// The FP64 evaluation (pair_r2<R2_EXACT>) from the same exact inputs.
+// The FP64 evaluation (pair_r2_exact) from the same exact inputs.
 __device__ __forceinline__ float pair_r2_f64(float c, float ca, float cb, int S) {
     if (ca == 0.0f || cb == 0.0f) return 0.0f;
     const double Sd = (double)S, a = (double)ca, b = (double)cb;
