@@ -144,3 +144,32 @@ def test_bad_queries_rejected(table):
         with pytest.raises(api.QldError) as e:   # pageable host buffer
             srv.submit(tid, 0, 3, 0, 3, host_r2=np.empty((3, 3), np.float32))
         assert e.value.code == api.ERR_INVALID
+
+
+def test_device_table_same_as_host_table(table):
+    """A table added from device memory (odd K: it goes through the device
+    staging copy and the re-pitching kernel) gives the same r^2 blocks and
+    summaries as the same table added from host memory."""
+    A, bc = table
+    assert A.shape[1] % 2 == 1
+    dA = torch.from_numpy(A.view(np.int64).copy()).cuda()
+    dbc = torch.from_numpy(bc.view(np.int32).copy()).cuda()
+    ctx = api.Context(0)
+    qs = [(0, 1800, 0, 1800), (100, 2900, 2000, 3000)]
+    outs = {}
+    try:
+        for name, (tA, tbc) in {"host": (A, bc), "device": (dA, dbc)}.items():
+            with api.Server(0, pool_bytes=256 << 20, max_inflight=2) as srv:
+                tid = srv.add_table(tA, tbc, N)
+                bufs = [ctx.pinned_empty((b1 - b0, a1 - a0), np.float32) for (a0, a1, b0, b1) in qs]
+                ids = [srv.submit(tid, *q, host_r2=buf) for q, buf in zip(qs, bufs)]
+                got = _wait_all(srv, ids, release=True)
+                outs[name] = ([b.copy() for b in bufs],
+                              [(got[i].n_above, got[i].sum_r2, got[i].max_r2) for i in ids])
+    finally:
+        ctx.close()
+    for h, d in zip(outs["host"][0], outs["device"][0]):
+        assert np.array_equal(h.view(np.uint32), d.view(np.uint32))
+    assert outs["host"][1] == outs["device"][1] or all(
+        hn == dn and abs(hs - ds) <= 1e-9 * max(1.0, hs) and hm == dm
+        for (hn, hs, hm), (dn, ds, dm) in zip(outs["host"][1], outs["device"][1]))
