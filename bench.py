@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma", "fp4"])
     ap.add_argument("--sm-pair", type=int, default=0, choices=[0, 1, 2],
                     help="4-bit kernel: SMs per output tile (0 = automatic)")
+    ap.add_argument("--r2-mode", default="exact", choices=["exact", "reference"],
+                    help="r^2 evaluation: exact (FP64-accurate) or reference (bit-identical "
+                         "to qLD-compute's float/double sequence)")
     ap.add_argument("--autotune", action="store_true",
                     help="run qld_cuda_autotune on the workload's shape first (AUTO then uses it)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -207,9 +210,13 @@ def kernel_roofline(ctx, variant, bitops, kern_ms, dev):
             "peak_source": "measured: qld_cuda_measure_popc_peak (register-only AND+POPC)"}
 
 
-def measured_traffic(variant, workload, sm_pair=0):
+def measured_traffic(variant, workload, sm_pair=0, r2_mode="exact"):
     """DRAM bytes per launch of the counts kernel from the ncu capture
-    summarised under profiles/ (None when no capture covers this case)."""
+    summarised under profiles/ (None when no capture covers this case).
+    sm_pair 0 is the automatic choice: SM pairs for exact r^2, single SMs
+    for reference r^2."""
+    if sm_pair == 0:
+        sm_pair = 1 if r2_mode == "reference" else 2
     names = {2: "k_ld_mma_wide_traffic_16384.md",
              3: "k_ld_mxf4_traffic_16384.md" if sm_pair == 1 else "k_ld_mxf4_pair_traffic_16384.md"}
     if variant not in names or workload != "single_region_29817x16622_lower_triangle":
@@ -341,6 +348,10 @@ def ours_arm(args, rank, world, local_rank):
     ctx.set_option(api.OPT_KERNEL, kern)
     ctx.set_option(api.OPT_MMA_TILE, args.mma_tile)
     ctx.set_option(api.OPT_SM_PAIR, args.sm_pair)
+    ctx.set_option(api.OPT_R2_MODE,
+                   api.R2_REFERENCE if args.r2_mode == "reference" else api.R2_EXACT)
+    if args.r2_mode != "exact":
+        cfg["r2_mode"] = args.r2_mode
     ctx.set_option(api.OPT_PROFILE, 1)
     # A dedicated stream: torch's default stream is the legacy NULL stream,
     # which the C ABI reads as "the context's own stream".
@@ -399,7 +410,7 @@ def ours_arm(args, rank, world, local_rank):
     sm_pair = args.sm_pair
     if tuned is not None and tuned["kernel"] == api.KERNEL_FP4 and sm_pair == 0:
         sm_pair = tuned["option"]
-    roof["traffic"] = measured_traffic(variant, cfg["workload"], sm_pair)
+    roof["traffic"] = measured_traffic(variant, cfg["workload"], sm_pair, args.r2_mode)
     roof["algorithmic_bytes_per_launch"] = alg_bytes
     roof["kernel_ms"] = kern_ms
     mp = measured_peaks()
@@ -572,6 +583,8 @@ def windowed_arm(args, rank, world, local_rank):
     ctx.set_option(api.OPT_KERNEL, kern)
     ctx.set_option(api.OPT_MMA_TILE, args.mma_tile)
     ctx.set_option(api.OPT_SM_PAIR, args.sm_pair)
+    ctx.set_option(api.OPT_R2_MODE,
+                   api.R2_REFERENCE if args.r2_mode == "reference" else api.R2_EXACT)
     ctx.set_option(api.OPT_PROFILE, 1)
     st = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(st)
@@ -614,6 +627,8 @@ def windowed_arm(args, rank, world, local_rank):
             "roofline": dict(kernel_roofline(ctx, stats.last_kernel, bitops, kern_ms, dev),
                              kernel_ms=kern_ms),
             "clocks": clk.summary()}
+    if args.r2_mode != "exact":
+        line["config"]["r2_mode"] = args.r2_mode
     if not args.no_e2e:
         Th = ctx.pinned_empty((m, K), np.uint64)
         Th[:] = T.cpu().numpy().view(np.uint64)
