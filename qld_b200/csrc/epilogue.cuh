@@ -105,11 +105,12 @@ __device__ __forceinline__ float pair_r2_exact(uint32_t cnt, const ARow &ra, con
 //    than 64 FP64 ulps from the nearest FP32 rounding midpoint, fl32(q) =
 //    fl32(RN64(x / den)).  Pairs failing it (about 3 in 10^7 at realistic S;
 //    ~10^-4 at S <= 100, whose simple fractions meet midpoints more often)
-//    or whose quotient would be an FP32 subnormal are flagged and
-//    recomputed with r2_reference.
+//    or whose quotient would be an FP32 subnormal or negative are flagged
+//    and recomputed with r2_reference.
 //  * (double)r > 1.0001 is r > 1 + 838 * 2^-23, the largest float not above
-//    1.0001.  x / 0 (a fixed SNP) is +inf, hence 123.456; 0 / 0 is the
-//    x86 default NaN the reference's build produces (0xFFC00000).
+//    1.0001.  x / 0 (a fixed SNP) is +inf, hence 123.456 (-inf, kept, when
+//    a bit count above S makes den -0); 0 / 0 is the x86 default NaN the
+//    reference's build produces (0xFFC00000).
 // Moving the FP32<->FP64 conversions to integer bit-field arithmetic and
 // seeding the reciprocal from the bit pattern instead (four Newton steps)
 // measured slower: 5.16 / 5.42 ms against 4.85 / 4.95 ms on the single region.
@@ -137,16 +138,26 @@ __device__ __forceinline__ float r2_reference_fast(float cab, const RowRef &A, u
     const long long mid = (long long)(__double_as_longlong(q) & 0x1FFFFFFFLL) - (1LL << 28);
     const bool dz = den == 0.0;
     const bool zero = A.c == 0u || cB == 0u;
+    // den is 0 or in [2^-96, 1] for consistent counts; a negative den (bit
+    // counts above S) takes the plain sequence.  (Dropping the range test
+    // and testing the low word alone measured 4.89 / 4.82 ms against
+    // 4.78 / 4.95 ms: the single-SM kernel, the one used, runs this form
+    // faster.)
     redo = !zero && !dz &&
            (!(den > 0x1p-1000 && den < 0x1p1000) || (q != 0.0 && q < 0x1p-126) ||
             (mid >= -64 && mid <= 64));
-    float f = dz ? __uint_as_float(r == 0.0f ? 0xFFC00000u : 0x7F800000u) : __double2float_rn(q);
+    // x / 0 is an infinity of den's sign (-0 when a bit count exceeds S)
+    float f = dz ? __uint_as_float(r == 0.0f ? 0xFFC00000u
+                                             : 0x7F800000u | ((uint32_t)__double2hiint(den) &
+                                                              0x80000000u))
+                 : __double2float_rn(q);
     if (f > __uint_as_float(0x3F800000u + 838u)) f = 123.456f;
     return zero ? 0.0f : f;
 }
 
 // The reference-mode chunk: every pair on the fast path, the flagged ones
-// (their counts kept in v, a bit in `redo`) redone with r2_reference.
+// (their accumulator word kept in v, a bit in `redo`) redone with
+// r2_reference.
 // FLOATCNT: v holds each count as F32 bits (the 4-bit kernels' accumulators),
 // else as an integer shifted left by SHIFT.
 template <int SHIFT, bool FLOATCNT>
@@ -159,15 +170,15 @@ __device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARow &ra, con
     if (S <= (1 << 24)) {
 #pragma unroll
         for (int t = 0; t < 32; ++t) {
-            const float cf = FLOATCNT ? __uint_as_float(v[t]) : (float)(v[t] >> SHIFT);
+            const uint32_t raw = v[t];
+            const float cf = FLOATCNT ? __uint_as_float(raw) : (float)(raw >> SHIFT);
             const int b = b0 + t;
             if (oc && b < n && a - b >= dlo && a - b <= dhi)
-                oc[(long long)t * ldc] = FLOATCNT ? (uint32_t)cf : v[t] >> SHIFT;
+                oc[(long long)t * ldc] = FLOATCNT ? (uint32_t)cf : raw >> SHIFT;
             bool rd;
             const float r = r2_reference_fast(cf, ra.ref, f.c[bl0 + t], f.v[bl0 + t],
                                               f.d0[bl0 + t], ra.Sf, ra.rSf, rd);
-            if (rd) v[t] = FLOATCNT ? (uint32_t)cf : v[t] >> SHIFT;
-            else v[t] = __float_as_uint(r);
+            v[t] = rd ? raw : __float_as_uint(r);   // a flagged pair keeps its count
             redo |= (uint32_t)rd << t;
         }
     } else {
@@ -176,7 +187,6 @@ __device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARow &ra, con
             const uint32_t cnt = FLOATCNT ? (uint32_t)__uint_as_float(v[t]) : v[t] >> SHIFT;
             const int b = b0 + t;
             if (oc && b < n && a - b >= dlo && a - b <= dhi) oc[(long long)t * ldc] = cnt;
-            v[t] = cnt;
         }
         redo = 0xFFFFFFFFu;
     }
@@ -190,7 +200,8 @@ __device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARow &ra, con
                 rb.c = f.c[bl0 + t];
                 rb.v = f.v[bl0 + t];
                 rb.one_minus = f.d0[bl0 + t];
-                v[t] = __float_as_uint(r2_reference(v[t], ra.ref, rb, S));
+                const uint32_t cnt = FLOATCNT ? (uint32_t)__uint_as_float(v[t]) : v[t] >> SHIFT;
+                v[t] = __float_as_uint(r2_reference(cnt, ra.ref, rb, S));
             }
         }
     }

@@ -2,7 +2,7 @@
  * (qld_b200/csrc/epilogue.cuh: r2_reference_fast) against the reference's
  * operation sequence (qLD src/correlator/src/gemm_cpu.c:357-389), bit for
  * bit, over random pairs: small and large sample counts, fixed and
- * monomorphic SNPs, near-independence counts.  The same steps in C: the
+ * monomorphic SNPs, near-independence counts, bit counts above S.  The same steps in C: the
  * Markstein-corrected FP32 quotient cab/S, a Newton reciprocal of the FP64
  * denominator from a seed carrying an injected relative error up to 2^-8
  * (standing in for rcp.approx.ftz.f64), the residual-corrected quotient,
@@ -56,7 +56,9 @@ static float fast_r2(uint32_t cab, uint32_t ca, uint32_t cb, int S, double seed_
     const int redo = !zero && !dz &&
                      (!(den > 0x1p-1000 && den < 0x1p1000) || (q != 0.0 && q < 0x1p-126) ||
                       (mid >= -64 && mid <= 64));
-    float f = dz ? b2f(r == 0.0f ? 0xFFC00000u : 0x7F800000u) : (float)q;
+    float f = dz ? b2f(r == 0.0f ? 0xFFC00000u
+                                 : 0x7F800000u | ((uint32_t)(d2b(den) >> 32) & 0x80000000u))
+                 : (float)q;
     if (f > b2f(0x3F800000u + 838u)) f = 123.456f;
     if (zero) f = 0.0f;
     if (redo) { ++fallbacks; f = ref_r2(cab, ca, cb, S); }
@@ -73,6 +75,7 @@ int main(int argc, char **argv) {
         uint32_t ca = (uint32_t)(rnd() % (uint64_t)(S + 1)), cb = (uint32_t)(rnd() % (uint64_t)(S + 1));
         if (rnd() % 8 == 0) ca = (rnd() & 1) ? 1u : (uint32_t)S - 1;
         if (rnd() % 8 == 0) cb = (rnd() & 1) ? (uint32_t)S : 1u;
+        if (rnd() % 64 == 0) ca = (uint32_t)S + (uint32_t)(rnd() % 50);   /* counts above S */
         const uint32_t mx = ca < cb ? ca : cb;
         uint32_t cab = (uint32_t)(rnd() % (uint64_t)(mx + 1));
         if (rnd() % 4 == 0) {   /* near independence: cab ~ ca*cb/S */

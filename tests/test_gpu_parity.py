@@ -287,14 +287,16 @@ def test_reference_mode_edge_pairs_bit_identical(gpu_ctx, kernel):
     the reference build's NaN), monomorphic SNPs, and a small sample count
     (S = 50) whose simple fractions often sit near FP32 rounding midpoints."""
     S, K = 1000, 16
-    n = len(THRESHOLD_CASES)
+    # plus bit counts above S: den is -0 (x / -0 = -inf, kept) or negative
+    cases = THRESHOLD_CASES + [(250, 1010, 1000), (600, 1020, 990)]
+    n = len(cases)
     bits = np.zeros((n, K * 64), np.uint8)
-    for i, (c, _, _) in enumerate(THRESHOLD_CASES):
+    for i, (c, _, _) in enumerate(cases):
         bits[i, :c] = 1
     rows = np.packbits(bits, axis=1).reshape(n, K, 8).view(">u8").reshape(n, K)
     rows = rows.astype(np.uint64)
-    bcA = np.array([t[1] for t in THRESHOLD_CASES], np.uint32)
-    bcB = np.array([t[2] for t in THRESHOLD_CASES], np.uint32)
+    bcA = np.array([t[1] for t in cases], np.uint32)
+    bcB = np.array([t[2] for t in cases], np.uint32)
     rng = np.random.default_rng(7)
     S2 = 50
     small = np.zeros((300, 64), np.uint8)
@@ -315,7 +317,7 @@ def test_reference_mode_edge_pairs_bit_identical(gpu_ctx, kernel):
         gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
         gpu_ctx.set_option(api.OPT_SM_PAIR, 0)
     want = oracle.r2_reference(bcA, bcB, oracle.counts(rows, rows), S, fma_contract=False)
-    assert np.isnan(np.diag(want)).sum() == 1
+    assert np.isnan(np.diag(want)).sum() == 1 and np.isneginf(want).any()
     assert np.array_equal(r2.view(np.uint32), want.view(np.uint32))
     wants = oracle.r2_reference(sbc, sbc, oracle.counts(srows), S2, fma_contract=False)
     mask = lower_mask(300, 300)
