@@ -33,6 +33,7 @@
 // thread returns early: both CTAs meet at the cluster barriers at start and
 // end on every path.
 #include "epilogue.cuh"
+#include "mxf4_rows.cuh"
 #include "qld_kernels.h"
 #include "tcgen05.cuh"
 
@@ -102,19 +103,6 @@ struct Item {
     int job, ta, tb, np;   // job < 0: end of the queue
 };
 static_assert(sizeof(Item) == 16, "an item is one 16-byte record");
-
-// One unpack task: one packed row, both 16-byte halves of the 32 bytes a
-// 256-sample stage takes from it (ld_mxf4_pair.cu: RowTask).
-struct RowTask {
-    uint32_t src, xr, is_a, valid;
-    uint32_t off[8];     // destination: row base + swizzled offset of chunk 0..7
-};
-
-template <int T>
-__device__ __forceinline__ uint4 spread4(const uint4 &w) {
-    return make_uint4(spread_e2m1<T>(w.x), spread_e2m1<T>(w.y), spread_e2m1<T>(w.z),
-                      spread_e2m1<T>(w.w));
-}
 
 // (job, ta, tb) of global item g: binary search of the item prefix, then the
 // job's own B-tile-row-first tile list.
@@ -314,20 +302,10 @@ k_ld_batch(const BatchParams bp) {
         // group g takes sub-stage g of every packed stage
         const int grp = (warp - FIRST_UNPACK_WARP) / (UNPACK_WARPS / 2);
         const int wt = ((warp - FIRST_UNPACK_WARP) % (UNPACK_WARPS / 2)) * 32 + lane;
-        RowTask task[TASKS];
+        mxf4rows::RowTask task[TASKS];
 #pragma unroll
-        for (int j = 0; j < TASKS; ++j) {
-            const int row = wt + j * GROUP_THREADS;   // over 128 A + 120 B rows
-            const bool isA = row < HM;
-            const int r = isA ? row : row - HM;
-            task[j].valid = row < NROWS;
-            task[j].is_a = isA;
-            task[j].src = (uint32_t)(r * 64);
-            task[j].xr = (uint32_t)((r >> 1) & 3);
-#pragma unroll
-            for (int c = 0; c < 8; ++c)
-                task[j].off[c] = (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
-        }
+        for (int j = 0; j < TASKS; ++j)   // over 128 A + 120 B rows
+            task[j] = mxf4rows::make_task<HM>(wt + j * GROUP_THREADS, NROWS);
         int gp = 0;
         bool ok = true;
         for (int qi = 0; ok; ++qi) {
@@ -359,28 +337,7 @@ k_ld_batch(const BatchParams bp) {
                 const uint8_t *pb = smem + L::OFF_PB + ps * PB_BYTES;
                 uint8_t *ua = smem + L::OFF_UA + us * UA_BYTES;
                 uint8_t *ub = smem + L::OFF_UB + us * UB_BYTES;
-                uint4 w[TASKS][2];
-#pragma unroll
-                for (int j = 0; j < TASKS; ++j)
-                    if (task[j].valid) {
-                        const uint8_t *row = (task[j].is_a ? pa : pb) + task[j].src;
-#pragma unroll
-                        for (int h = 0; h < 2; ++h)
-                            w[j][h] = *reinterpret_cast<const uint4 *>(
-                                row + ((((uint32_t)grp * 2 + h) ^ task[j].xr) << 4));
-                    }
-#pragma unroll
-                for (int j = 0; j < TASKS; ++j) {
-                    if (!task[j].valid) continue;
-                    uint8_t *dst = task[j].is_a ? ua : ub;
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 0]) = spread4<0>(w[j][h]);
-                        *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 1]) = spread4<1>(w[j][h]);
-                        *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 2]) = spread4<2>(w[j][h]);
-                        *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 3]) = spread4<3>(w[j][h]);
-                    }
-                }
+                mxf4rows::unpack_rows(task, pa, pb, ua, ub, grp);
                 fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) {

@@ -36,6 +36,7 @@
 // cluster barriers at start and end on every path, including after a
 // timeout, and the TMEM is released only after the last MMA has completed.
 #include "epilogue.cuh"
+#include "mxf4_rows.cuh"
 #include "qld_kernels.h"
 #include "tcgen05.cuh"
 
@@ -97,49 +98,6 @@ struct Smem {
 static_assert(sizeof(float2) == 8, "ColsF entry");
 static_assert(ACC_STRIDE + BN <= SF_COL && SF_COL + 16 <= TMEM_COLS, "TMEM map");
 static_assert(TASKS == 2 && SUB == 2 && UST % 2 == 0 && EPILOGUE == COLS_N, "work split");
-
-// One unpack task: one packed row (A or B) of the CTA, both 16-byte halves of
-// the 32 bytes (256 samples) a sub-stage takes from each 64-byte packed row.
-// A quarter-warp then covers 8 consecutive rows, so its 16-byte loads from
-// the 64-byte-swizzled packed stage and its stores into the 128-byte-swizzled
-// unpacked stage both touch all 32 banks once.
-struct RowTask {
-    uint32_t src, xr, is_a, valid;
-    uint32_t off[8];     // destination: row base + swizzled offset of chunk 0..7
-};
-
-template <int T>
-__device__ __forceinline__ uint4 spread4(const uint4 &w) {
-    return make_uint4(spread_e2m1<T>(w.x), spread_e2m1<T>(w.y), spread_e2m1<T>(w.z),
-                      spread_e2m1<T>(w.w));
-}
-
-__device__ __forceinline__ void unpack_rows(const RowTask (&task)[TASKS], const uint8_t *pa,
-                                            const uint8_t *pb, uint8_t *ua, uint8_t *ub,
-                                            int sub) {
-    uint4 w[TASKS][2];
-#pragma unroll
-    for (int j = 0; j < TASKS; ++j)
-        if (task[j].valid) {
-            const uint8_t *row = (task[j].is_a ? pa : pb) + task[j].src;
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-                w[j][h] = *reinterpret_cast<const uint4 *>(
-                    row + ((((uint32_t)sub * 2 + h) ^ task[j].xr) << 4));
-        }
-#pragma unroll
-    for (int j = 0; j < TASKS; ++j) {
-        if (!task[j].valid) continue;
-        uint8_t *dst = task[j].is_a ? ua : ub;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 0]) = spread4<0>(w[j][h]);
-            *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 1]) = spread4<1>(w[j][h]);
-            *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 2]) = spread4<2>(w[j][h]);
-            *reinterpret_cast<uint4 *>(dst + task[j].off[h * 4 + 3]) = spread4<3>(w[j][h]);
-        }
-    }
-}
 
 template <int MODE>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
@@ -283,20 +241,10 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         // every packed stage
         const int grp = (warp - FIRST_UNPACK_WARP) / (UNPACK_WARPS / 2);
         const int wt = ((warp - FIRST_UNPACK_WARP) % (UNPACK_WARPS / 2)) * 32 + lane;
-        RowTask task[TASKS];
+        mxf4rows::RowTask task[TASKS];
 #pragma unroll
-        for (int j = 0; j < TASKS; ++j) {
-            const int row = wt + j * GROUP_THREADS;   // over 128 A + 120 B rows
-            const bool isA = row < HM;
-            const int r = isA ? row : row - HM;
-            task[j].valid = row < NTASK;
-            task[j].is_a = isA;
-            task[j].src = (uint32_t)(r * 64);
-            task[j].xr = (uint32_t)((r >> 1) & 3);
-#pragma unroll
-            for (int c = 0; c < 8; ++c)
-                task[j].off[c] = (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
-        }
+        for (int j = 0; j < TASKS; ++j)   // over 128 A + 120 B rows
+            task[j] = mxf4rows::make_task<HM>(wt + j * GROUP_THREADS, NTASK);
         const int total_u = my_tiles * nu;
         for (int gu = grp; gu < total_u; gu += 2) {
             const int gp = gu / SUB;
@@ -314,7 +262,7 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 if (lane == 0) flag_error(p.status, ST_TIMEOUT_MMA);
                 break;
             }
-            unpack_rows(task, smem + L::OFF_PA + ps * PA_BYTES, smem + L::OFF_PB + ps * PB_BYTES,
+            mxf4rows::unpack_rows(task, smem + L::OFF_PA + ps * PA_BYTES, smem + L::OFF_PB + ps * PB_BYTES,
                         smem + L::OFF_UA + us * UA_BYTES, smem + L::OFF_UB + us * UB_BYTES, grp);
             fence_proxy_async_smem();
             __syncwarp();
