@@ -176,11 +176,7 @@ k_ld_batch(const BatchParams bp) {
         fence_barrier_init();
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_u32(tmem_slot)),
-                     "r"(TMEM_COLS)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+        tmem_alloc<2>(smem_u32(tmem_slot), TMEM_COLS);
     }
     tc_fence_before();
     __syncthreads();
@@ -446,9 +442,7 @@ k_ld_batch(const BatchParams bp) {
     cluster_sync_all();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"(TMEM_COLS)
-                     : "memory");
+        tmem_dealloc<2>(tmem, TMEM_COLS);
     }
 }
 

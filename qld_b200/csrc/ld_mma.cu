@@ -122,11 +122,7 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
         fence_barrier_init();
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_u32(tmem_slot)),
-                     "r"(TMEM_COLS)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        tmem_alloc<1>(smem_u32(tmem_slot), TMEM_COLS);
     }
     tc_fence_before();
     __syncthreads();
@@ -330,9 +326,7 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
             flag_error(p.status, ST_TIMEOUT_MMA);
         __syncwarp();
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"(TMEM_COLS)
-                     : "memory");
+        tmem_dealloc<1>(tmem, TMEM_COLS);
     }
 }
 

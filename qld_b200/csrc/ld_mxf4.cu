@@ -157,11 +157,7 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
         fence_barrier_init();
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_u32(tmem_slot)),
-                     "r"(TMEM_COLS)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        tmem_alloc<1>(smem_u32(tmem_slot), TMEM_COLS);
     }
     tc_fence_before();
     __syncthreads();
@@ -373,9 +369,7 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
             flag_error(p.status, ST_TIMEOUT_MMA);
         __syncwarp();
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"(TMEM_COLS)
-                     : "memory");
+        tmem_dealloc<1>(tmem, TMEM_COLS);
     }
 }
 

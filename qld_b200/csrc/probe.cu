@@ -100,11 +100,7 @@ k_mma_peak(int iters, unsigned *status, long long timeout) {
     }
     fence_proxy_async_smem();
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_u32(slot)),
-                     "r"(512)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        tmem_alloc<1>(smem_u32(slot), 512);
     }
     tc_fence_before();
     __syncthreads();
@@ -135,8 +131,7 @@ k_mma_peak(int iters, unsigned *status, long long timeout) {
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512)
-                     : "memory");
+        tmem_dealloc<1>(tmem, 512);
     }
 }
 

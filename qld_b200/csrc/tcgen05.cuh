@@ -204,6 +204,35 @@ __device__ __forceinline__ void tc_mma_mxf4_pair(uint32_t d_tmem, uint64_t adesc
         : "memory");
 }
 
+// TMEM allocation by one warp (CG = 1: this CTA; 2: the CTA pair, issued by
+// one warp in each CTA), the column base written to shared memory at `slot`;
+// then the warp gives up its right to allocate again, so the CTAs waiting
+// for an SM's TMEM are not held back.
+template <int CG>
+__device__ __forceinline__ void tmem_alloc(uint32_t slot, uint32_t cols) {
+    if constexpr (CG == 2) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+                     "r"(cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    } else {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+                     "r"(cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+}
+
+template <int CG>
+__device__ __forceinline__ void tmem_dealloc(uint32_t tmem, uint32_t cols) {
+    if constexpr (CG == 2)
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols)
+                     : "memory");
+    else
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols)
+                     : "memory");
+}
+
 // Arrive once on the mbarrier at offset `bar` of every CTA in `mask` when the
 // pair MMAs issued so far have completed.
 __device__ __forceinline__ void tc_commit_pair(uint32_t bar, uint16_t mask) {
