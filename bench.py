@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--queries", type=int, default=10000, help="served workload: query count")
     ap.add_argument("--load", type=float, default=0.8,
                     help="served workload: offered load as a fraction of measured capacity")
+    ap.add_argument("--pool-gb", type=int, default=48, help="served workload: r^2 pool (GB)")
+    ap.add_argument("--inflight", type=int, default=3,
+                    help="served workload: batched launches in flight")
     ap.add_argument("--band", type=int, default=5000, help="windowed workload: band width")
     ap.add_argument("--jobs", type=int, default=4096, help="batched workload: number of tasks")
     ap.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma", "fp4"])
@@ -667,7 +670,7 @@ def served_arm(args, rank, world, local_rank):
     torch.cuda.set_device(dev)
     rng = np.random.default_rng(5 + rank)
     H = 20_000
-    srv = api.Server(local_rank, pool_bytes=48 << 30, max_inflight=3)
+    srv = api.Server(local_rank, pool_bytes=args.pool_gb << 30, max_inflight=args.inflight)
     sizes = []
     for c in range(22):
         m = int(rng.integers(50_000, 250_001))
@@ -737,7 +740,8 @@ def served_arm(args, rank, world, local_rank):
             "config": {"workload": f"served_{args.queries}_queries", "chromosomes": 22,
                        "snps_per_chromosome": "U(50000,250000)", "haplotypes": H,
                        "query_side_snps": "U(100,20000)", "arrivals": "Poisson",
-                       "offered_load": args.load, "pool_gb": 48, "max_inflight_batches": 3,
+                       "offered_load": args.load, "pool_gb": args.pool_gb,
+                       "max_inflight_batches": args.inflight,
                        "delivered": "per query: count of r2 >= 0.2 (< 100), sum, max; "
                                     "r2 blocks stay on the device until released"},
             "bitops_per_s": pairs * 64 * K / t,
