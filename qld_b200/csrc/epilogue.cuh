@@ -113,7 +113,7 @@ __device__ __forceinline__ float pair_r2_exact(uint32_t cnt, const ARow &ra, con
 //    reference's build produces (0xFFC00000).
 // Moving the FP32<->FP64 conversions to integer bit-field arithmetic and
 // seeding the reciprocal from the bit pattern instead (four Newton steps)
-// measured slower: 5.16 / 5.42 ms against 4.85 / 4.95 ms on the single region.
+// measured slower: 5.16 / 5.42 ms against 4.78 / 4.88 ms on the single region.
 __device__ __forceinline__ double rcp_seed(double x) {
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
@@ -130,9 +130,12 @@ __device__ __forceinline__ float r2_reference_fast(float cab, const RowRef &A, u
     const float r = __fmul_rn(d, d);
     const double den = __dmul_rn(__dmul_rn((double)p12, A.one_minus), omB);
     const double x = (double)r;
-    double y = rcp_seed(den);
+    double y = rcp_seed(den), e = 0.0;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) y = __fma_rn(y, __fma_rn(-den, y, 1.0), y);
+    for (int k = 0; k < 3; ++k) {
+        e = __fma_rn(-den, y, 1.0);
+        y = __fma_rn(y, e, y);
+    }
     double q = __dmul_rn(x, y);
     q = __fma_rn(__fma_rn(-q, den, x), y, q);
     const long long mid = (long long)(__double_as_longlong(q) & 0x1FFFFFFFLL) - (1LL << 28);
@@ -143,9 +146,11 @@ __device__ __forceinline__ float r2_reference_fast(float cab, const RowRef &A, u
     // and testing the low word alone measured 4.89 / 4.82 ms against
     // 4.78 / 4.95 ms: the single-SM kernel, the one used, runs this form
     // faster.)
+    // |e| <= 2^-20 before the last Newton step leaves y within ~2^-40 of
+    // 1/den whatever the seed's accuracy, which the 64-ulp margin needs
     redo = !zero && !dz &&
            (!(den > 0x1p-1000 && den < 0x1p1000) || (q != 0.0 && q < 0x1p-126) ||
-            (mid >= -64 && mid <= 64));
+            (mid >= -64 && mid <= 64) || !(fabs(e) <= 0x1p-20));
     // x / 0 is an infinity of den's sign (-0 when a bit count exceeds S)
     float f = dz ? __uint_as_float(r == 0.0f ? 0xFFC00000u
                                              : 0x7F800000u | ((uint32_t)__double2hiint(den) &

@@ -246,7 +246,7 @@ const KernelShape &mma_shape(qld_ctx *c, const Task &t, int b0, int b1) {
 // for every task size measured (a single region of 29,817 SNPs x 16,622
 // samples: 2.57 ms against 3.31 ms).  R2_REFERENCE's epilogue (the
 // reference's float/double sequence) is the bound, and the single-SM kernel
-// runs it on 16 warps instead of 8: 4.78 ms against 4.95 ms there.
+// runs it on 16 warps instead of 8: 4.78 ms against 5.19 ms there.
 const KernelShape &fp4_shape(qld_ctx *c, const Task &t, int b0, int b1) {
     (void)b0; (void)b1;
     if (c->sm_pair == 0)

@@ -47,15 +47,15 @@ static float fast_r2(uint32_t cab, uint32_t ca, uint32_t cb, int S, double seed_
     const float p = v1 * v2, d = v3 - p, r = d * d;
     const double den = ((double)p * (1.0 - (double)v1)) * (1.0 - (double)v2);
     const double x = (double)r;
-    double y = (1.0 / den) * (1.0 + seed_err);
-    for (int k = 0; k < 3; ++k) y = fma(y, fma(-den, y, 1.0), y);
+    double y = (1.0 / den) * (1.0 + seed_err), e = 0.0;
+    for (int k = 0; k < 3; ++k) { e = fma(-den, y, 1.0); y = fma(y, e, y); }
     double q = x * y;
     q = fma(fma(-q, den, x), y, q);
     const long long mid = (long long)(d2b(q) & 0x1FFFFFFFull) - (1ll << 28);
     const int dz = den == 0.0, zero = ca == 0 || cb == 0;
     const int redo = !zero && !dz &&
                      (!(den > 0x1p-1000 && den < 0x1p1000) || (q != 0.0 && q < 0x1p-126) ||
-                      (mid >= -64 && mid <= 64));
+                      (mid >= -64 && mid <= 64) || !(fabs(e) <= 0x1p-20));
     float f = dz ? b2f(r == 0.0f ? 0xFFC00000u
                                  : 0x7F800000u | ((uint32_t)(d2b(den) >> 32) & 0x80000000u))
                  : (float)q;
