@@ -1,0 +1,45 @@
+"""CPU tests of bench.py's bookkeeping: the measured peaks it divides by and
+the ncu capture it takes each kernel's DRAM traffic from."""
+import json
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+WORKLOAD = "single_region_29817x16622_lower_triangle"
+
+
+def test_measured_peaks_read_from_the_pool_file():
+    mp = bench.measured_peaks()
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            assert mp == {"hbm_gbs": float(json.load(f)["hbm_gbs"]),
+                          "source": "MEASURED_PEAKS.json"}
+    else:
+        assert mp == {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def _profile_value(name):
+    with open(os.path.join(ROOT, "profiles", name)) as f:
+        for line in f:
+            if line.startswith("traffic_bytes_per_launch_full:"):
+                return int(line.split(":")[1])
+    raise AssertionError(name)
+
+
+def test_traffic_follows_the_kernel_the_mode_runs():
+    pair = _profile_value("k_ld_mxf4_pair_traffic_16384.md")
+    single = _profile_value("k_ld_mxf4_traffic_16384.md")
+    fp4, mma = 3, 2
+    assert bench.measured_traffic(fp4, WORKLOAD, 0, "exact") == pair
+    assert bench.measured_traffic(fp4, WORKLOAD, 0, "reference") == single
+    assert bench.measured_traffic(fp4, WORKLOAD, 1, "exact") == single
+    assert bench.measured_traffic(fp4, WORKLOAD, 2, "reference") == pair
+    assert bench.measured_traffic(mma, WORKLOAD) == _profile_value(
+        "k_ld_mma_wide_traffic_16384.md")
+    assert bench.measured_traffic(fp4, "all_pairs_2048x4096_symmetric") is None
+    assert bench.measured_traffic(0, WORKLOAD) is None
