@@ -167,11 +167,11 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         if (lane == 0) {
             prefetch_tmap(&tmA);
             prefetch_tmap(&tmB);
-            int gp = 0;
+            int gp = 0, cur_t = 0, cur_base = 0;
             bool ok = true;
             for (int i = 0; i < my_tiles && ok; ++i) {
                 int ta, tb;
-                tl.decode(pair + i * npairs, ta, tb);
+                tl.decode_from(pair + i * npairs, ta, tb, cur_t, cur_base);
                 const int ra = ta * BM + (int)rank * HM, rb = tb * BN + (int)rank * HN;
                 for (int kp = 0; kp < np; ++kp, ++gp) {
                     const int s = gp % PST;
@@ -274,9 +274,10 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         const int q = warp & 3;                 // TMEM lane quarter
         const int colh = ew >> 2;               // chunks colh, colh + 2, colh + 4, colh + 6
         bool failed = false;
+        int cur_t = 0, cur_base = 0;
         for (int it = 0; it < my_tiles; ++it) {
             int ta, tb;
-            tl.decode(pair + it * npairs, ta, tb);
+            tl.decode_from(pair + it * npairs, ta, tb, cur_t, cur_base);
             const int ab = it & 1;
             {   // every column factor the chunks read; 0 past the tile and the task
                 const int b = tb * BN + et;

@@ -314,6 +314,25 @@ struct TileList {
         }
         return n;
     }
+    // decode() for a caller whose indices never decrease (a persistent CTA
+    // walking its tiles): the walk over B tiles resumes at (t, base), the B
+    // tile and the count of tiles before it where the previous call stopped,
+    // so a call costs the B tiles stepped over instead of all of them.
+    __host__ __device__ __forceinline__ void decode_from(int idx, int &ta, int &tb, int &t,
+                                                         int &base) const {
+        for (; t < tiles_b; ++t) {
+            const int lo = ta_lo(tb0 + t);
+            const int c = ta_hi(tb0 + t) - lo;
+            const int cc = c > 0 ? c : 0;
+            if (idx < base + cc) {
+                ta = lo + idx - base;
+                tb = tb0 + t;
+                return;
+            }
+            base += cc;
+        }
+        ta = tb = -1;
+    }
     __host__ __device__ __forceinline__ void decode(int idx, int &ta, int &tb) const {
         for (int t = 0; t < tiles_b; ++t) {
             const int lo = ta_lo(tb0 + t);
