@@ -136,9 +136,10 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
             prefetch_tmap(&tmB);
             int gp = 0;   // packed stages issued so far (ring position)
             bool ok = true;
+            int cur_t = 0, cur_base = 0;   // decode_from: tiles in increasing order
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 int ta, tb;
-                tl.decode(tile, ta, tb);
+                tl.decode_from(tile, ta, tb, cur_t, cur_base);
                 for (int kp = 0; kp < np; ++kp, ++gp) {
                     const int s = gp % PST;
                     if (gp >= PST && !mbar_wait(smem_u32(&pempty[s]), ((gp / PST) - 1) & 1,
@@ -272,9 +273,10 @@ k_ld_mma(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtens
         const int q = warp & 3;                  // TMEM lane quarter of this warp
         bool failed = false;
         int it = 0;
+        int cur_t = 0, cur_base = 0;   // decode_from: tiles in increasing order
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
             int ta, tb;
-            tl.decode(tile, ta, tb);
+            tl.decode_from(tile, ta, tb, cur_t, cur_base);
             const int ab = it & 1;
             // B-row factors of this tile: 2 per thread.
 #pragma unroll

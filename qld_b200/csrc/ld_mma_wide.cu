@@ -141,9 +141,10 @@ k_ld_mma_wide(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
             prefetch_tmap(&tmB);
             int gp = 0;
             bool ok = true;
+            int cur_t = 0, cur_base = 0;   // decode_from: tiles in increasing order
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 int ta, tb;
-                tl.decode(tile, ta, tb);
+                tl.decode_from(tile, ta, tb, cur_t, cur_base);
                 for (int kp = 0; kp < np; ++kp, ++gp) {
                     const int s = gp % PST;
                     if (gp >= PST && !mbar_wait(smem_u32(&pempty[s]), ((gp / PST) - 1) & 1,
@@ -269,9 +270,10 @@ k_ld_mma_wide(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ C
         const int acc_i = (wi >> 2) & 1;        // which accumulator (A row half)
         const int colh = wi >> 3;               // which 128-column half
         int it = 0;
+        int cur_t = 0, cur_base = 0;   // decode_from: tiles in increasing order
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
             int ta, tb;
-            tl.decode(tile, ta, tb);
+            tl.decode_from(tile, ta, tb, cur_t, cur_base);
             // this tile's stages, then the next tile's first UST stages
             const int lim = (it + 1) * nu + UST;
             produce_until(lim < total_u ? lim : total_u);

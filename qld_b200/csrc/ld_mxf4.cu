@@ -179,9 +179,10 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
             prefetch_tmap(&tmB);
             int gp = 0;
             bool ok = true;
+            int cur_t = 0, cur_base = 0;   // decode_from: tiles in increasing order
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 int ta, tb;
-                tl.decode(tile, ta, tb);
+                tl.decode_from(tile, ta, tb, cur_t, cur_base);
                 for (int kp = 0; kp < np; ++kp, ++gp) {
                     const int s = gp % PST;
                     if (gp >= PST && !mbar_wait(smem_u32(&pempty[s]), ((gp / PST) - 1) & 1,
@@ -305,9 +306,10 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
         const int acc_i = (wi >> 2) & 1;        // which accumulator (A row half)
         const int colh = wi >> 3;               // chunks colh, colh + 2, colh + 4, colh + 6
         int it = 0;
+        int cur_t = 0, cur_base = 0;   // decode_from: tiles in increasing order
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
             int ta, tb;
-            tl.decode(tile, ta, tb);
+            tl.decode_from(tile, ta, tb, cur_t, cur_base);
             const int lim = (it + 1) * nu + UST;
             produce_until(lim < total_u ? lim : total_u);
             if (wt < COLS_N) {   // every column factor the chunks read; 0 past the tile
