@@ -244,9 +244,9 @@ const KernelShape &mma_shape(qld_ctx *c, const Task &t, int b0, int b1) {
 // R2_EXACT the pair kernel overlaps each tile's epilogue with the next
 // tile's MMAs and finishes a tile on two SMs in half the time: the faster one
 // for every task size measured (a single region of 29,817 SNPs x 16,622
-// samples: 2.57 ms against 3.31 ms).  R2_REFERENCE's epilogue (the
+// samples: 2.49 ms against 3.16 ms).  R2_REFERENCE's epilogue (the
 // reference's float/double sequence) is the bound, and the single-SM kernel
-// runs it on 16 warps instead of 8: 4.78 ms against 5.19 ms there.
+// runs it on 16 warps instead of 8: 4.66 ms against 5.11 ms there.
 const KernelShape &fp4_shape(qld_ctx *c, const Task &t, int b0, int b1) {
     (void)b0; (void)b1;
     if (c->sm_pair == 0)
