@@ -1,13 +1,14 @@
 """Benchmark of the LD hot path (AND+popcount counts + fused r^2) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload single_region|all_pairs] [--kernel auto|popc|mma|fp4]
+                    [--workload single_region|all_pairs|windowed|batched|served]
+                    [--sections all_pairs,reference_mode,windowed,batched,served|none]
 
-Workload (default): the dataset-shaped single region -- 29,817 SNPs x 16,622
-haploid sequences (K = 260 words per SNP), allele frequencies Beta(0.1, 1)
-clipped to >= 1/16,622, haplotype-copying model (20 founders, recombination
-blocks of 50-500 SNPs, 1% per-site mutation), lower-triangular FP32 r^2.
-Seeded synthetic data of that shape stands in for the dataset.
+Headline workload (default): the dataset-shaped single region -- 29,817 SNPs x
+16,622 haploid sequences (K = 260 words per SNP), allele frequencies
+Beta(0.1, 1) clipped to >= 1/16,622, haplotype-copying model (20 founders,
+recombination blocks of 50-500 SNPs, 1% per-site mutation), lower-triangular
+FP32 r^2.  Seeded synthetic data of that shape stands in for the dataset.
 
 A step is one pass of the hot path over the region: counts + r^2 for all
 M(M-1)/2 SNP pairs (the kernel also fills the diagonal).  `value` is
@@ -15,13 +16,29 @@ SNP-pairs/s with the packed table resident in HBM (device-to-device call,
 output to HBM), timed per step with CUDA events on the launching stream after
 an L2 flush (a 512 MB write); `e2e` is the same metric through the host-buffer
 C-ABI call (qld_cuda_ld): pinned host table -> device, counts + r^2, lower
-triangle -> pinned host memory, all inside the timed region.
+triangle -> pinned host memory, all inside the timed region.  `parity` checks
+the timed output after the timed region: about two B rows from every 120-row
+block (so every output tile, including the last tiles each CTA pair walks) are
+compared with the CPU oracle -- counts bit-exact (from one more launch of the
+same kernel with the counts output on), r^2 within 1e-6 relative of FP64 --
+and reports the maximum and mean relative error.
+
+The same line carries one sub-object per other workload form (`--sections`),
+each with its own timing, clocks and sampled parity:
+  all_pairs       2,048 SNPs x 4,096 samples, iid, every row checked;
+  reference_mode  the headline region with r^2 bit-identical to qLD-compute
+                  (the drop-in's default mode);
+  windowed        200,000 SNPs x 100,000 haplotypes, 5,000-SNP band;
+  batched         4,096 tasks in one persistent launch vs per-task launches;
+  served          22 resident chromosomes, Poisson stream of 10,000 queries.
 
 With --gpus N (torchrun) every rank processes its own region of the same shape
-(no data-path collective; weak scaling); timing is the max over ranks.
-`--impl reference` times the reference's CPU path (its bin_gemm_2x2
-micro-kernel in a BLIS-style loop plus its get_pairwise_ld_score, built from
-the qLD sources into oracle/_ref) with all host threads on a bounded sample.
+(no data-path collective; weak scaling); timing is the max over ranks, and the
+sections run on rank 0's line only at N = 1.  `--impl reference` times the
+reference's stock fast CPU path -- qLD-compute -blis: BLIS 0.1.8 `binary_gemm`
+cblas_dsyrk with BLIS_IC_NT = physical cores, then get_pairwise_ld_score on
+one thread, built from the qLD sources into oracle/_ref -- on a bounded sample
+of the same region.
 """
 from __future__ import annotations
 
@@ -38,9 +55,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "r2 SNP-pairs/s (counts + fused r2 epilogue)"
+SECTIONS = ("all_pairs", "reference_mode", "windowed", "batched", "served")
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -48,6 +66,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="single_region",
                     choices=["single_region", "all_pairs", "batched", "windowed", "served"])
+    ap.add_argument("--sections", default=",".join(SECTIONS),
+                    help="sub-objects of the headline line (comma list, or 'none')")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the sampled oracle checks of the timed outputs")
     ap.add_argument("--queries", type=int, default=10000, help="served workload: query count")
     ap.add_argument("--load", type=float, default=0.8,
                     help="served workload: offered load as a fraction of measured capacity")
@@ -70,7 +92,7 @@ def parse():
                     help="tensor-core tile rows (0: per shape)")
     ap.add_argument("--snps", type=int, default=0,
                     help="use only the first N SNPs of the workload (profiling captures)")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def workload_config(name):
@@ -81,6 +103,19 @@ def workload_config(name):
     return dict(workload="all_pairs_2048x4096_symmetric", snps=2048, haplotypes=4096,
                 words_per_snp=64, model="iid Bernoulli", freq="Uniform(0.05,0.5)",
                 output="fp32 lower triangle")
+
+
+def arm_config(args, world):
+    """The `config` of the headline line; both arms print the same dict."""
+    cfg = workload_config(args.workload)
+    cfg["parallelism"] = f"replicas x{world} (independent regions, no collective)"
+    cfg["l2"] = "512 MB flush write between timed steps"
+    if args.snps:
+        cfg["snps"] = args.snps
+        cfg["workload"] += f"_first{args.snps}"
+    if args.r2_mode != "exact":
+        cfg["r2_mode"] = args.r2_mode
+    return cfg
 
 
 def make_table(name, device, seed_offset=0):
@@ -178,7 +213,7 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def kernel_roofline(ctx, variant, bitops, kern_ms, dev):
+def kernel_roofline(ctx, variant, bitops, kern_ms, dev, int8_context=True):
     """Roofline of the counts kernel against the measured rate of the pipe it
     runs on: the tensor pipe of its MMA kind (qld_cuda_measure_mma_peak,
     2 ops per bit-pair), or the popcount pipe (1 bit-op per bit-pair)."""
@@ -193,18 +228,19 @@ def kernel_roofline(ctx, variant, bitops, kern_ms, dev):
                 "peak_source": "measured: qld_cuda_measure_mma_peak, back-to-back 128x256 "
                                + ("kind::mxf4 MMAs (K=64)" if variant == api.KERNEL_FP4
                                   else "kind::i8 MMAs (K=32)") + ", one CTA per SM"}
-        # for context: the int8 rate a library GEMM reaches on this GPU
-        a = torch.randint(-2, 2, (8192, 8192), dtype=torch.int8, device=dev)
-        b = torch.randint(-2, 2, (8192, 8192), dtype=torch.int8, device=dev).t()
-        for _ in range(3):
-            torch._int_mm(a, b)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(10):
-            torch._int_mm(a, b)
-        e1.record()
-        torch.cuda.synchronize()
-        roof["int8_gemm_torch_tops"] = 2 * 8192 ** 3 * 10 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+        if int8_context:
+            # for context: the int8 rate a library GEMM reaches on this GPU
+            a = torch.randint(-2, 2, (8192, 8192), dtype=torch.int8, device=dev)
+            b = torch.randint(-2, 2, (8192, 8192), dtype=torch.int8, device=dev).t()
+            for _ in range(3):
+                torch._int_mm(a, b)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(10):
+                torch._int_mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            roof["int8_gemm_torch_tops"] = 2 * 8192 ** 3 * 10 / (e0.elapsed_time(e1) * 1e-3) / 1e12
         return roof
     popc_peak = ctx.measure_popc_peak() / 1e12
     achieved = bitops / (kern_ms * 1e-3) / 1e12
@@ -236,51 +272,148 @@ def measured_traffic(variant, workload, sm_pair=0, r2_mode="exact"):
 
 # ------------------------------------------------------------ reference CPU --
 
-def cpu_reference_rate(T_np, S, seconds_target=12.0, threads=None):
-    """Reference CPU path (bin_gemm_2x2 loop + get_pairwise_ld_score) on the
-    first Ms SNPs of the table, single region; Ms chosen so the timed sample
-    takes ~seconds_target.  Returns (pairs/s, cores, sample description)."""
+def host_cpu():
+    """(model name, physical cores, logical cpus) of this host."""
+    model, cores = "unknown", set()
+    phys = core = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            k, _, v = line.partition(":")
+            k, v = k.strip(), v.strip()
+            if k == "model name":
+                model = v
+            elif k == "physical id":
+                phys = v
+            elif k == "core id":
+                core = v
+            elif not k and phys is not None and core is not None:
+                cores.add((phys, core))
+                phys = core = None
+        if phys is not None and core is not None:
+            cores.add((phys, core))
+    except OSError:
+        pass
+    logical = os.cpu_count() or 1
+    return model, (len(cores) or logical), logical
+
+
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
-
     import oracle
-    threads = threads or os.cpu_count()
+    return oracle
 
-    def run(ms):
-        A = np.ascontiguousarray(T_np[:ms])
-        bc = oracle.bitcounts(A)
-        t0 = time.perf_counter()
-        C = oracle.ref_counts_ukr(A, None, lower_only=True, threads=threads)
-        oracle.ref_ld_score(bc, bc, C, S, threads=threads)
-        return time.perf_counter() - t0
 
-    m = T_np.shape[0]
+def _blis_threads(jc, ic):
+    os.environ["BLIS_JC_NT"] = str(jc)
+    os.environ["BLIS_IC_NT"] = str(ic)
+    os.environ["BLIS_JR_NT"] = "1"
+    os.environ["BLIS_IR_NT"] = "1"
+    os.environ["OMP_NUM_THREADS"] = str(jc * ic)
+
+
+def cpu_reference_sample(T_np, S, ms, factoring=None):
+    """One timed run of the reference's stock -blis path on the first `ms`
+    SNPs of the table (single region): BLIS cblas_dsyrk counts (BLIS threads
+    from `factoring` = (JC, IC) ways) + get_pairwise_ld_score on one thread,
+    as correlate() runs them.  Without the BLIS build, the reference
+    micro-kernel in a BLIS-style loop stands in (and says so).  Returns
+    (seconds, counts seconds, epilogue seconds, threads, kind of path)."""
+    import numpy as np
+    oracle = _oracle()
+    _, phys, logical = host_cpu()
+    blis = oracle.blis_available()
+    factoring = factoring or (1, phys)
+    A = np.ascontiguousarray(T_np[:ms])
+    bc = oracle.bitcounts(A)
+    if blis:
+        _blis_threads(*factoring)
+        _, _, tg, tl = oracle.ref_blis_counts_ld(A, bc, S)
+        kind = (f"qLD-compute -blis path: BLIS 0.1.8 binary_gemm cblas_dsyrk (BLIS_JC_NT="
+                f"{factoring[0]}, BLIS_IC_NT={factoring[1]}) + get_pairwise_ld_score (1 thread)")
+        return tg + tl, tg, tl, factoring[0] * factoring[1], kind
+    t0 = time.perf_counter()
+    C = oracle.ref_counts_ukr(A, None, lower_only=True, threads=logical)
+    t1 = time.perf_counter()
+    oracle.ref_ld_score(bc, bc, C, S, threads=1)
+    t2 = time.perf_counter()
+    kind = ("stand-in (BLIS not built): bin_gemm_2x2 in a BLIS-style loop + "
+            "get_pairwise_ld_score (1 thread)")
+    return t2 - t0, t1 - t0, t2 - t1, logical, kind
+
+
+def size_reference_sample(T_np, S, seconds_target, factoring=None):
+    """SNP count Ms whose single-region sample takes ~seconds_target, capped
+    so its C / results buffers (12 bytes per entry) fit in a quarter of the
+    host's free memory."""
+    try:
+        mem = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_AVPHYS_PAGES")
+    except (ValueError, OSError):
+        mem = 16 << 30
+    m = min(T_np.shape[0], int((mem / 4 / 12) ** 0.5))
     ms = min(m, 1024)
-    t = run(ms)
+    t = cpu_reference_sample(T_np, S, ms, factoring)[0]
     while t < seconds_target / 8 and ms < m:
         ms = min(m, ms * 2)
-        t = run(ms)
+        t = cpu_reference_sample(T_np, S, ms, factoring)[0]
     if t < seconds_target / 2 and ms < m:
         ms = min(m, int(ms * (seconds_target / max(t, 1e-3)) ** 0.5))
-        t = run(ms)
-    pairs = ms * (ms - 1) / 2
-    return pairs / t, threads, f"first {ms} SNPs of the region, all {ms*(ms-1)//2} pairs, {t:.2f} s"
+    return ms
+
+
+def cpu_reference_rate(T_np, S, seconds_target=8.0, factoring=None, ms=None):
+    """Pairs/s of the reference's stock CPU path on a bounded sample of the
+    region.  Returns (pairs/s, threads, sample description, path)."""
+    model, phys, _ = host_cpu()
+    ms = ms or size_reference_sample(T_np, S, seconds_target, factoring)
+    t, tg, tl, threads, kind = cpu_reference_sample(T_np, S, ms, factoring)
+    desc = (f"first {ms} SNPs of the region, all {ms * (ms - 1) // 2} pairs, {t:.2f} s "
+            f"(counts {tg:.2f} s, epilogue {tl:.2f} s); {model}, {phys} physical cores")
+    return ms * (ms - 1) / 2 / t, threads, desc, kind
+
+
+def best_blis_factoring(T_np, S):
+    """The fastest (JC, IC) split of the host's physical cores for the counts,
+    tried on a small sample (the reference's README leaves BLIS threading to
+    the BLIS_*_NT variables)."""
+    import numpy as np
+    oracle = _oracle()
+    _, phys, _ = host_cpu()
+    if not oracle.blis_available():
+        return None
+    cands = sorted({(1, phys), (2, max(1, phys // 2)), (phys, 1)})
+    ms = min(T_np.shape[0], 6144)
+    A = np.ascontiguousarray(T_np[:ms])
+    bc = oracle.bitcounts(A)
+    C = np.empty((ms, ms), np.uint64)
+    R = np.empty((ms, ms), np.float32)
+    best = None
+    for f in cands:
+        _blis_threads(*f)
+        oracle.ref_blis_counts_ld(A, bc, S, C=C, results=R)
+        _, _, tg, _ = oracle.ref_blis_counts_ld(A, bc, S, C=C, results=R)
+        if best is None or tg < best[0]:
+            best = (tg, f)
+    return best[1]
 
 
 def reference_arm(args, rank, world):
     import numpy as np
-    cfg = workload_config(args.workload)
+    cfg = arm_config(args, world)
     if rank != 0:
         return
     T, S = make_table(args.workload, "cpu")
     T_np = T.numpy().view(np.uint64)
+    if args.snps:
+        T_np = T_np[:args.snps]
+    fac = best_blis_factoring(T_np, S)
+    ms = size_reference_sample(T_np, S, 4.0, fac)
     for _ in range(args.warmup):
-        cpu_reference_rate(T_np, S, seconds_target=2.0)
+        cpu_reference_rate(T_np, S, factoring=fac, ms=max(1024, ms // 2))
     vals = []
-    desc = ""
+    desc = kind = ""
     cores = os.cpu_count()
     for _ in range(args.steps):
-        v, cores, desc = cpu_reference_rate(T_np, S, seconds_target=6.0)
+        v, cores, desc, kind = cpu_reference_rate(T_np, S, factoring=fac, ms=ms)
         vals.append(v)
     value = statistics.median(vals)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
@@ -289,13 +422,13 @@ def reference_arm(args, rank, world):
             "vs_baseline": None, "dtype": "u64 popcount / f32 r2", "data": "synthetic",
             "config": cfg,
             "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "reference",
-                             "sample": desc},
+                             "path": kind, "sample": desc},
             "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-# -------------------------------------------------------------------- ours --
+# ------------------------------------------------------------ shared timing --
 
 def lower_tri_d2h_bytes(m, band=3840, block=512):
     """Bytes qld_cuda_ld moves to the host for a single region of m SNPs:
@@ -319,43 +452,115 @@ def max_over_ranks(value, world, device):
     return float(t.item())
 
 
-def ours_arm(args, rank, world, local_rank):
-    import numpy as np
+def timed_steps(step, st, steps, warmup, flush, gpu, world=1):
+    """W warm-up steps, then K steps each after an L2-flushing write, timed
+    with CUDA events on the launching stream `st`, with nvidia-smi clock
+    samples over the timed region.  Returns (per-step ms, clocks)."""
     import torch
     import torch.distributed as dist
+    for _ in range(warmup):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(gpu) as clk:
+        clk.mark_start()
+        for i in range(steps):
+            flush.zero_()
+            ev[i][0].record(st)
+            step()
+            ev[i][1].record(st)
+        torch.cuda.synchronize()
+        clk.mark_end()
+    if world > 1:
+        dist.barrier()
+    return [a.elapsed_time(b) for a, b in ev], clk.summary()
 
-    from qld_b200 import api, synth
 
-    dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
-    cfg = workload_config(args.workload)
-    cfg["parallelism"] = f"replicas x{world} (independent regions, no collective)"
-    cfg["l2"] = "512 MB flush write between timed steps"
+def new_context(local_rank, args, kernel=None, r2_mode=None):
+    from qld_b200 import api
+    ctx = api.Context(local_rank)
+    kern = {"auto": api.KERNEL_AUTO, "popc": api.KERNEL_POPC, "mma": api.KERNEL_MMA,
+            "fp4": api.KERNEL_FP4}[kernel or args.kernel]
+    ctx.set_option(api.OPT_KERNEL, kern)
+    ctx.set_option(api.OPT_MMA_TILE, args.mma_tile)
+    ctx.set_option(api.OPT_SM_PAIR, args.sm_pair)
+    mode = r2_mode or args.r2_mode
+    ctx.set_option(api.OPT_R2_MODE, api.R2_REFERENCE if mode == "reference" else api.R2_EXACT)
+    ctx.set_option(api.OPT_PROFILE, 1)
+    return ctx
 
-    T, S = make_table(args.workload, dev, seed_offset=rank)
-    if args.snps:
-        T = T[:args.snps].contiguous()
-        cfg["snps"] = T.shape[0]
-        cfg["workload"] += f"_first{T.shape[0]}"
+
+def padded(T, dev):
+    """Device copy of a packed table with an even row pitch (16-byte rows)."""
+    import torch
     m, K = T.shape
     lda = K + (K & 1)
     Tp = torch.zeros(m, lda, dtype=torch.int64, device=dev)
     Tp[:, :K] = T
+    return Tp, lda
+
+
+# ------------------------------------------------------------------ parity --
+
+def region_parity(ctx, Tp, bc, m, lda, K, S, out, st, mode, seed=0, per_block=2, block=120):
+    """Sampled oracle check of a single-region output `out` (m x m, B-major,
+    entries j >= i defined) left by the timed launches: ~per_block B rows from
+    every `block` rows plus the first and last rows, against every A row.
+    Counts come from one more launch of the same call with the counts output
+    on, which must also reproduce the checked r^2 rows bit for bit."""
+    import numpy as np
+    import torch
+    oracle = _oracle()
+    rng = np.random.default_rng(seed)
+    rows = oracle.tile_row_samples(m, block, per_block, rng, extra=(0, m - 1))
+    idx = torch.as_tensor(rows, device=out.device)
+    got = out.index_select(0, idx).cpu().numpy()
+    cnt = torch.empty(m, m, dtype=torch.int32, device=out.device)
+    ctx.ld_device(Tp, bc, m, lda, Tp, bc, m, lda, K, S, True, out, m, counts=cnt, ldc=m,
+                  stream=st)
+    ctx.sync(stream=st)
+    again = out.index_select(0, idx).cpu().numpy()
+    got_c = cnt.index_select(0, idx).cpu().numpy().view(np.uint32)
+    del cnt
+    T_np = Tp[:, :K].contiguous().cpu().numpy().view(np.uint64)
+    bc_np = bc.cpu().numpy().astype(np.uint32)
+    valid = np.arange(m)[None, :] >= rows[:, None]
+    res = oracle.check_rows(T_np, bc_np, T_np[rows], bc_np[rows], S, got, valid,
+                            got_counts=got_c, mode=mode)
+    res["rerun_bit_identical"] = bool(np.array_equal(got[valid].view(np.uint32),
+                                                     again[valid].view(np.uint32)))
+    res["ok"] = res["ok"] and res["rerun_bit_identical"]
+    res["sample"] = f"{len(rows)} B rows (~{per_block} per {block}-row block) x all {m} A rows"
+    return res
+
+
+# -------------------------------------------------------------------- ours --
+
+def ours_arm(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    from qld_b200 import synth
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    cfg = arm_config(args, world)
+
+    T, S = make_table(args.workload, dev, seed_offset=rank)
+    if args.snps:
+        T = T[:args.snps].contiguous()
+    m, K = T.shape
+    Tp, lda = padded(T, dev)
     bc = synth.popcount_rows(T).to(torch.int32)
     out = torch.empty(m, m, dtype=torch.float32, device=dev)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
 
-    ctx = api.Context(local_rank)
-    kern = {"auto": api.KERNEL_AUTO, "popc": api.KERNEL_POPC, "mma": api.KERNEL_MMA,
-            "fp4": api.KERNEL_FP4}[args.kernel]
-    ctx.set_option(api.OPT_KERNEL, kern)
-    ctx.set_option(api.OPT_MMA_TILE, args.mma_tile)
-    ctx.set_option(api.OPT_SM_PAIR, args.sm_pair)
-    ctx.set_option(api.OPT_R2_MODE,
-                   api.R2_REFERENCE if args.r2_mode == "reference" else api.R2_EXACT)
-    if args.r2_mode != "exact":
-        cfg["r2_mode"] = args.r2_mode
-    ctx.set_option(api.OPT_PROFILE, 1)
+    ctx = new_context(local_rank, args)
     # A dedicated stream: torch's default stream is the legacy NULL stream,
     # which the C ABI reads as "the context's own stream".
     st = torch.cuda.Stream(device=dev)
@@ -365,7 +570,7 @@ def ours_arm(args, rank, world, local_rank):
         ctx.ld_device(Tp, bc, m, lda, Tp, bc, m, lda, K, S, True, out, m, stream=st)
 
     tuned = None
-    if args.autotune and kern == api.KERNEL_AUTO:
+    if args.autotune and args.kernel == "auto":
         tk, topt, tms = ctx.autotune(m, m, K, True)
         tuned = {"kernel": tk, "option": topt, "ms_per_launch_tuned": tms,
                  "measured_at": f"{min(m, 16384)}x{min(m, 16384)}x{K} words"}
@@ -375,30 +580,12 @@ def ours_arm(args, rank, world, local_rank):
         step()
     ctx.sync(stream=st)
     ctx.stats(reset=True)
-
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clk:
-        clk.mark_start()
-        torch.cuda.nvtx.range_push("qld_timed")
-        for i in range(args.steps):
-            flush.zero_()
-            ev[i][0].record(st)
-            step()
-            ev[i][1].record(st)
-        torch.cuda.nvtx.range_pop()
-        ctx.sync(stream=st)
-        torch.cuda.synchronize()
-        clk.mark_end()
-    if world > 1:
-        dist.barrier()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
+    torch.cuda.nvtx.range_push("qld_timed")
+    step_ms, clocks = timed_steps(step, st, args.steps, 0, flush, local_rank, world)
+    torch.cuda.nvtx.range_pop()
+    ctx.sync(stream=st)
     total_ms = sum(step_ms)
     stats = ctx.stats(reset=True)
-    clocks = clk.summary()
 
     pairs = m * (m - 1) / 2
     total_ms_max = max_over_ranks(total_ms, world, dev)
@@ -411,7 +598,7 @@ def ours_arm(args, rank, world, local_rank):
     roof = kernel_roofline(ctx, variant, bitops, kern_ms, dev)
     alg_bytes = m * K * 8 * 2 + pairs * 4
     sm_pair = args.sm_pair
-    if tuned is not None and tuned["kernel"] == api.KERNEL_FP4 and sm_pair == 0:
+    if tuned is not None and tuned["kernel"] == 3 and sm_pair == 0:
         sm_pair = tuned["option"]
     roof["traffic"] = measured_traffic(variant, cfg["workload"], sm_pair, args.r2_mode)
     roof["algorithmic_bytes_per_launch"] = alg_bytes
@@ -431,6 +618,11 @@ def ours_arm(args, rank, world, local_rank):
     if tuned is not None:
         line["autotune"] = tuned
 
+    # ---- sampled oracle check of the output the timed steps wrote
+    if not args.no_parity and rank == 0:
+        line["parity"] = region_parity(ctx, Tp, bc, m, lda, K, S, out, st, args.r2_mode,
+                                       seed=11)
+
     # ---- e2e through the host-buffer C-ABI call
     if not args.no_e2e:
         Th = ctx.pinned_empty((m, K), np.uint64)
@@ -441,6 +633,7 @@ def ours_arm(args, rank, world, local_rank):
         for _ in range(max(1, args.warmup)):
             ctx.ld(Th, bch, S=S, r2_out=outh)
         if world > 1:
+            import torch.distributed as dist
             dist.barrier()
         ts = []
         for _ in range(args.steps):
@@ -452,14 +645,203 @@ def ours_arm(args, rank, world, local_rank):
                        "h2d_bytes_per_step": m * K * 8 + m * 4,
                        "d2h_bytes_per_step": lower_tri_d2h_bytes(m),
                        "api": "qld_cuda_ld (pinned host buffers)"}
+        del Th, bch, outh
 
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, cores, desc = cpu_reference_rate(T.cpu().numpy().view(np.uint64), S)
+        T_np = T.cpu().numpy().view(np.uint64)
+        fac = best_blis_factoring(T_np, S)
+        v, cores, desc, kind = cpu_reference_rate(T_np, S, factoring=fac)
         line["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": cores, "kind": "reference",
-                                "sample": desc}
+                                "path": kind, "sample": desc}
+
+    sections = [] if args.sections in ("", "none") else args.sections.split(",")
+    if world == 1 and args.workload == "single_region" and not args.snps:
+        if "reference_mode" in sections:
+            line["reference_mode"] = section_reference_mode(args, Tp, bc, m, lda, K, S, out,
+                                                            flush, st, local_rank)
     ctx.close()
+    del out, Tp, T, bc
+    torch.cuda.empty_cache()
+    if world == 1 and args.workload == "single_region" and not args.snps:
+        for name, fn in (("all_pairs", section_all_pairs), ("windowed", section_windowed),
+                         ("batched", section_batched), ("served", section_served)):
+            if name in sections:
+                line[name] = fn(args, local_rank, flush)
+                torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- sections --
+
+def section_reference_mode(args, Tp, bc, m, lda, K, S, out, flush, st, local_rank):
+    """The headline region with r^2 in QLD_R2_REFERENCE mode (bit-identical to
+    qLD-compute's get_pairwise_ld_score; the drop-in's default), automatic
+    kernel choice."""
+    ctx = new_context(local_rank, args, r2_mode="reference")
+
+    def step():
+        ctx.ld_device(Tp, bc, m, lda, Tp, bc, m, lda, K, S, True, out, m, stream=st)
+    ctx.stats(reset=True)
+    step_ms, clocks = timed_steps(step, st, args.steps, args.warmup, flush, local_rank)
+    ctx.sync(stream=st)
+    stats = ctx.stats(reset=True)
+    pairs = m * (m - 1) / 2
+    ms = sum(step_ms) / len(step_ms)
+    kern_ms = stats.counts_kernel_ms / max(1, stats.counts_launches)
+    res = {"value": pairs / (ms * 1e-3), "unit": "pairs/s", "ms_per_step": ms,
+           "steps": args.steps, "kernel_variant": stats.last_kernel,
+           "gpu_launches": stats.kernel_launches // (args.steps + args.warmup),
+           "roofline": dict(kernel_roofline(ctx, stats.last_kernel, pairs * 64 * K, kern_ms,
+                                            None, int8_context=False), kernel_ms=kern_ms),
+           "clocks": clocks}
+    if not args.no_parity:
+        res["parity"] = region_parity(ctx, Tp, bc, m, lda, K, S, out, st, "reference", seed=12)
+    ctx.close()
+    return res
+
+
+def section_all_pairs(args, local_rank, flush):
+    """All-pairs r^2, one region: 2,048 SNPs x 4,096 samples (iid, Uniform(0.05,
+    0.5) frequencies), every B row checked against the oracle."""
+    import torch
+
+    from qld_b200 import synth
+    dev = torch.device("cuda", local_rank)
+    T, S = synth.all_pairs_workload(device=dev, seed=1)
+    m, K = T.shape
+    Tp, lda = padded(T, dev)
+    bc = synth.popcount_rows(T).to(torch.int32)
+    out = torch.empty(m, m, dtype=torch.float32, device=dev)
+    ctx = new_context(local_rank, args, r2_mode="exact")
+    st = torch.cuda.current_stream(dev)
+
+    def step():
+        ctx.ld_device(Tp, bc, m, lda, Tp, bc, m, lda, K, S, True, out, m, stream=st)
+    ctx.stats(reset=True)
+    step_ms, clocks = timed_steps(step, st, args.steps, args.warmup, flush, local_rank)
+    ctx.sync(stream=st)
+    stats = ctx.stats(reset=True)
+    pairs = m * (m - 1) / 2
+    ms = sum(step_ms) / len(step_ms)
+    kern_ms = stats.counts_kernel_ms / max(1, stats.counts_launches)
+    res = {"config": {"workload": "all_pairs_2048x4096_symmetric", "snps": m, "haplotypes": S,
+                      "words_per_snp": K, "model": "iid Bernoulli", "freq": "Uniform(0.05,0.5)",
+                      "l2": "512 MB flush write between timed steps"},
+           "value": pairs / (ms * 1e-3), "unit": "pairs/s", "ms_per_step": ms,
+           "steps": args.steps, "kernel_variant": stats.last_kernel, "kernel_ms": kern_ms,
+           "gpu_launches": stats.kernel_launches // (args.steps + args.warmup),
+           "clocks": clocks}
+    if not args.no_parity:
+        res["parity"] = region_parity(ctx, Tp, bc, m, lda, K, S, out, st, "exact", seed=13,
+                                      per_block=120)
+    ctx.close()
+    return res
+
+
+def band_pairs(m, W):
+    return sum(min(W, m - 1 - i) for i in range(m)) if m < 50_000 else \
+        W * (m - W) + W * (W - 1) // 2
+
+
+def band_parity(T_np, bc_np, S, out_rows, rows, W, mode="exact", counts_rows=None):
+    """Sampled oracle check of band rows: out_rows[k, d] = r^2(B row rows[k],
+    A row rows[k]+1+d) for the d that stay inside the table."""
+    import numpy as np
+    oracle = _oracle()
+    m = T_np.shape[0]
+    groups = []
+    for k, i in enumerate(rows):
+        w = min(W, m - 1 - int(i))
+        if w <= 0:
+            continue
+        groups.append(dict(A=T_np[i + 1:i + 1 + w], bcA=bc_np[i + 1:i + 1 + w],
+                           B=T_np[i:i + 1], bcB=bc_np[i:i + 1], S=S,
+                           got=out_rows[k:k + 1, :w], valid=np.ones((1, w), bool),
+                           counts=None if counts_rows is None else counts_rows[k:k + 1, :w]))
+    return oracle.check_groups(groups, mode=mode)
+
+
+def section_windowed(args, local_rank, flush, m_full=None):
+    """Windowed workload: 200,000 SNPs x 100,000 haplotypes (copying model,
+    100 founders), r^2 for pairs within `band` SNPs, FP32 band array."""
+    import numpy as np
+    import torch
+
+    from qld_b200 import api, synth
+    oracle = _oracle()
+    dev = torch.device("cuda", local_rank)
+    T, S = synth.windowed_workload(device=dev, m=m_full or args.snps or 200_000, seed=3)
+    m, K = T.shape
+    W = args.band
+    Tp, lda = padded(T, dev)
+    bc = synth.popcount_rows(T).to(torch.int32)
+    out = torch.empty(m, W, dtype=torch.float32, device=dev)
+    pairs = band_pairs(m, W)
+    ctx = new_context(local_rank, args)
+    st = torch.cuda.current_stream(dev)
+
+    def step():
+        ctx.ld_band_device(Tp, bc, m, lda, K, S, W, out, W, stream=st)
+    ctx.stats(reset=True)
+    step_ms, clocks = timed_steps(step, st, args.steps, args.warmup, flush, local_rank)
+    ctx.sync(stream=st)
+    stats = ctx.stats(reset=True)
+    ms = sum(step_ms) / len(step_ms)
+    kern_ms = stats.counts_kernel_ms / max(1, stats.counts_launches)
+    bitops = pairs * 64 * K
+    res = {"config": {"workload": f"windowed_{m}x{S}_band{W}", "snps": m, "haplotypes": S,
+                      "words_per_snp": K, "band": W, "model": "copying(100 founders)",
+                      "pairs_per_step": pairs, "l2": "inputs (2.5 GB) and outputs larger than L2"},
+           "value": pairs / (ms * 1e-3), "unit": "pairs/s", "ms_per_step": ms,
+           "steps": args.steps, "bitops_per_s": bitops / (ms * 1e-3),
+           "gpu_launches": stats.kernel_launches // (args.steps + args.warmup),
+           "kernel_variant": stats.last_kernel,
+           "roofline": dict(kernel_roofline(ctx, stats.last_kernel, bitops, kern_ms, dev,
+                                            int8_context=False), kernel_ms=kern_ms),
+           "clocks": clocks}
+    T_np = None
+    if not args.no_parity:
+        rng = np.random.default_rng(14)
+        rows = oracle.tile_row_samples(m, 240, 1, rng, extra=(0, m - W - 1, m - 2))
+        idx = torch.as_tensor(rows, device=dev)
+        got = out.index_select(0, idx).cpu().numpy()
+        cnt = torch.empty(m, W, dtype=torch.int32, device=dev)
+        ctx.ld_band_device(Tp, bc, m, lda, K, S, W, out, W, counts=cnt, ldc=W, stream=st)
+        ctx.sync(stream=st)
+        again = out.index_select(0, idx).cpu().numpy()
+        got_c = cnt.index_select(0, idx).cpu().numpy().view(np.uint32)
+        del cnt
+        T_np = T.cpu().numpy().view(np.uint64)
+        bc_np = bc.cpu().numpy().astype(np.uint32)
+        par = band_parity(T_np, bc_np, S, got, rows, W, counts_rows=got_c)
+        inside = np.arange(W)[None, :] < (m - 1 - rows)[:, None]
+        par["rerun_bit_identical"] = bool(np.array_equal(got[inside].view(np.uint32),
+                                                         again[inside].view(np.uint32)))
+        par["ok"] = par["ok"] and par["rerun_bit_identical"]
+        par["sample"] = f"{len(rows)} band rows (one per 240-row block) x their {W} pairs"
+        res["parity"] = par
+    if not args.no_e2e:
+        Th = ctx.pinned_empty((m, K), np.uint64)
+        Th[:] = T_np if T_np is not None else T.cpu().numpy().view(np.uint64)
+        bch = ctx.pinned_empty((m,), np.uint32)
+        bch[:] = bc.cpu().numpy().view(np.uint32)
+        outh = ctx.pinned_empty((m, W), np.float32)
+        ctx.set_option(api.OPT_BAND_ROWS, 8192)
+        for _ in range(max(1, args.warmup)):
+            ctx.ld_band(Th, bch, S=S, band=W, r2_out=outh)
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            ctx.ld_band(Th, bch, S=S, band=W, r2_out=outh)
+            ts.append(time.perf_counter() - t0)
+        res["e2e"] = {"value": pairs * len(ts) / sum(ts), "unit": "pairs/s",
+                      "h2d_bytes_per_step": m * K * 8 + m * 4,
+                      "d2h_bytes_per_step": m * W * 4,
+                      "api": "qld_cuda_ld_band (pinned host buffers, streamed)"}
+        del Th, bch, outh
+    ctx.close()
+    return res
 
 
 def make_batched_jobs(njobs, dev, seed=0):
@@ -485,9 +867,7 @@ def make_batched_jobs(njobs, dev, seed=0):
         f = torch.from_numpy(rng.beta(0.5, 0.5, rows).astype(np.float32))
         T = synth.iid_table(rows, S, f, seed * 100003 + j, device=dev, chunk=2048)
         K = T.shape[1]
-        lda = K + (K & 1)
-        Tp = torch.zeros(rows, lda, dtype=torch.int64, device=dev)
-        Tp[:, :K] = T
+        Tp, lda = padded(T, dev)
         del T
         bc = synth.popcount_rows(Tp).to(torch.int32)
         A, bcA = Tp[:m], bc[:m]
@@ -501,18 +881,57 @@ def make_batched_jobs(njobs, dev, seed=0):
     return jobs, pairs, bitops
 
 
-def batched_arm(args, rank, world, local_rank):
-    import numpy as np  # noqa: F401
+def batch_parity(jobs, rows_per_job=2, seed=0, chunk=256):
+    """Every job of a batched call, a few B rows each (one random row and the
+    last row, whose tile is among the last the queue hands out), checked
+    against the oracle over all of the job's A rows."""
+    import numpy as np
+    import torch
+    oracle = _oracle()
+    rng = np.random.default_rng(seed)
+    total = None
+    for c0 in range(0, len(jobs), chunk):
+        groups = []
+        for j in jobs[c0:c0 + chunk]:
+            m, n, K = j["m"], j["n"], j["K"]
+            rows = sorted({int(rng.integers(0, n)), n - 1} if rows_per_job >= 2
+                          else {n - 1})
+            idx = torch.as_tensor(rows, device=j["r2"].device)
+            got = j["r2"].index_select(0, idx).cpu().numpy()
+            A = j["A"][:, :K].contiguous().cpu().numpy().view(np.uint64)
+            B = j["B"].index_select(0, idx)[:, :K].contiguous().cpu().numpy().view(np.uint64)
+            bcA = j["bcA"].cpu().numpy().astype(np.uint32)
+            bcB = j["bcB"].index_select(0, idx).cpu().numpy().astype(np.uint32)
+            r = np.array(rows)
+            valid = (np.arange(m)[None, :] >= r[:, None]) if j["symmetric"] \
+                else np.ones((len(rows), m), bool)
+            groups.append(dict(A=A, bcA=bcA, B=B, bcB=bcB, S=j["S"], got=got, valid=valid))
+        res = oracle.check_groups(groups, mode="exact")
+        if total is None:
+            total = res
+        else:
+            for k in ("rows_checked", "pairs_checked"):
+                total[k] += res[k]
+            total["r2_mean_rel"] = max(total["r2_mean_rel"], res["r2_mean_rel"])
+            total["r2_max_rel"] = max(total["r2_max_rel"], res["r2_max_rel"])
+            total["r2_within_tol"] = total["r2_within_tol"] and res["r2_within_tol"]
+            total["ok"] = total["ok"] and res["ok"]
+    total["r2_mean_rel_note"] = "largest per-chunk mean over chunks of 256 jobs"
+    total["sample"] = f"all {len(jobs)} jobs x {rows_per_job} B rows x all A rows"
+    return total
+
+
+def section_batched(args, local_rank, flush):
+    """Batched workload: the same tasks as one persistent launch and as
+    per-task launches."""
     import torch
 
     from qld_b200 import api
     dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
-    jobs, pairs, bitops = make_batched_jobs(args.jobs, dev, seed=rank)
+    jobs, pairs, bitops = make_batched_jobs(args.jobs, dev, seed=0)
     ctx = api.Context(local_rank)
     ctx.set_option(api.OPT_PROFILE, 1)
-    st = torch.cuda.Stream(device=dev)
-    torch.cuda.set_stream(st)
+    st = torch.cuda.current_stream(dev)
 
     def batched():
         ctx.ld_batch(jobs, stream=st)
@@ -523,155 +942,56 @@ def batched_arm(args, rank, world, local_rank):
                           j["ldb"], j["K"], j["S"], j["symmetric"], j["r2"], j["ldr"], stream=st)
 
     res = {}
-    for name, fn in (("batched", batched), ("plain", plain)):
-        for _ in range(args.warmup):
-            fn()
-        ctx.sync(stream=st)
+    for name, fn in (("plain", plain), ("batched", batched)):
         ctx.stats(reset=True)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.nvtx.range_push(f"qld_timed_{name}")
-        e0.record(st)
-        for _ in range(args.steps):
-            fn()
-        e1.record(st)
+        step_ms, clocks = timed_steps(fn, st, args.steps, args.warmup, flush, local_rank)
         torch.cuda.nvtx.range_pop()
         ctx.sync(stream=st)
-        torch.cuda.synchronize()
-        res[name] = (e0.elapsed_time(e1) / args.steps, ctx.stats(reset=True))
-    ms_b, st_b = res["batched"]
-    ms_p, st_p = res["plain"]
-    line = {"metric": METRIC + ", batched tasks", "value": pairs / (ms_b * 1e-3),
-            "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_b, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64 popcount / f32 r2", "data": "synthetic",
-            "config": {"workload": f"batched_{args.jobs}_tasks", "snps_per_side": "logU(64,8192)",
-                       "samples": "logU(1000,50000)", "freq": "Beta(0.5,0.5)",
-                       "half": "single region (triangle) / two regions (rectangle)",
-                       "pairs_per_step": pairs, "bitops_per_step": bitops},
-            "bitops_per_s": bitops / (ms_b * 1e-3),
-            "gpu_launches": st_b.kernel_launches // max(1, args.steps),
-            "plain": {"value": pairs / (ms_p * 1e-3), "unit": "pairs/s", "ms_per_step": ms_p,
-                      "launches_per_step": st_p.kernel_launches // max(1, args.steps)},
-            "speedup_vs_plain": ms_p / ms_b}
+        res[name] = (sum(step_ms) / len(step_ms), ctx.stats(reset=True), clocks)
+    ms_b, st_b, clk_b = res["batched"]
+    ms_p, st_p, clk_p = res["plain"]
+    out = {"config": {"workload": f"batched_{args.jobs}_tasks", "snps_per_side": "logU(64,8192)",
+                      "samples": "logU(1000,50000)", "freq": "Beta(0.5,0.5)",
+                      "half": "single region (triangle) / two regions (rectangle)",
+                      "pairs_per_step": pairs, "bitops_per_step": bitops,
+                      "l2": "512 MB flush write between timed steps"},
+           "value": pairs / (ms_b * 1e-3), "unit": "pairs/s", "ms_per_step": ms_b,
+           "steps": args.steps, "bitops_per_s": bitops / (ms_b * 1e-3),
+           "gpu_launches": st_b.kernel_launches // (args.steps + args.warmup),
+           "clocks": clk_b,
+           "plain": {"value": pairs / (ms_p * 1e-3), "unit": "pairs/s", "ms_per_step": ms_p,
+                     "launches_per_step": st_p.kernel_launches // (args.steps + args.warmup),
+                     "clocks": clk_p},
+           "speedup_vs_plain": ms_p / ms_b}
+    if not args.no_parity:
+        # the batched call ran last: its outputs are what the jobs hold now
+        out["parity"] = batch_parity(jobs, seed=15)
     ctx.close()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    del jobs
+    return out
 
 
-def windowed_arm(args, rank, world, local_rank):
-    """Windowed workload: 200,000 SNPs x 100,000 haplotypes (copying model,
-    100 founders), r^2 for pairs within `band` SNPs, FP32 band array."""
-    import numpy as np
-    import torch
-
-    from qld_b200 import api, synth
-    dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
-    m_full = args.snps or 200_000
-    T, S = synth.windowed_workload(device=dev, m=m_full, seed=3 + rank)
-    m, K = T.shape
-    W = args.band
-    lda = K + (K & 1)
-    Tp = torch.zeros(m, lda, dtype=torch.int64, device=dev)
-    Tp[:, :K] = T
-    bc = synth.popcount_rows(T).to(torch.int32)
-    out = torch.empty(m, W, dtype=torch.float32, device=dev)
-    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
-    pairs = sum(min(W, m - 1 - i) for i in range(0, m)) if m < 50_000 else \
-        W * (m - W) + W * (W - 1) // 2
-    ctx = api.Context(local_rank)
-    kern = {"auto": api.KERNEL_AUTO, "popc": api.KERNEL_POPC, "mma": api.KERNEL_MMA,
-            "fp4": api.KERNEL_FP4}[args.kernel]
-    ctx.set_option(api.OPT_KERNEL, kern)
-    ctx.set_option(api.OPT_MMA_TILE, args.mma_tile)
-    ctx.set_option(api.OPT_SM_PAIR, args.sm_pair)
-    ctx.set_option(api.OPT_R2_MODE,
-                   api.R2_REFERENCE if args.r2_mode == "reference" else api.R2_EXACT)
-    ctx.set_option(api.OPT_PROFILE, 1)
-    st = torch.cuda.Stream(device=dev)
-    torch.cuda.set_stream(st)
-
-    def step():
-        ctx.ld_band_device(Tp, bc, m, lda, K, S, W, out, W, stream=st)
-
-    for _ in range(args.warmup):
-        flush.zero_()
-        step()
-    ctx.sync(stream=st)
-    ctx.stats(reset=True)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clk:
-        clk.mark_start()
-        for i in range(args.steps):
-            flush.zero_()
-            ev[i][0].record(st)
-            step()
-            ev[i][1].record(st)
-        ctx.sync(stream=st)
-        torch.cuda.synchronize()
-        clk.mark_end()
-    total_ms = sum(a.elapsed_time(b) for a, b in ev)
-    stats = ctx.stats(reset=True)
-    kern_ms = stats.counts_kernel_ms / max(1, stats.counts_launches)
-    bitops = pairs * 64 * K
-    line = {"metric": METRIC + ", windowed band", "value": pairs * args.steps / (total_ms * 1e-3),
-            "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64 popcount / f32 r2", "data": "synthetic",
-            "config": {"workload": f"windowed_{m}x{S}_band{W}", "snps": m, "haplotypes": S,
-                       "words_per_snp": K, "band": W, "model": "copying(100 founders)",
-                       "pairs_per_step": pairs, "l2": "512 MB flush write between timed steps"},
-            "bitops_per_s": bitops * args.steps / (total_ms * 1e-3),
-            "gpu_launches": stats.kernel_launches // max(1, args.steps),
-            "kernel_variant": stats.last_kernel,
-            "roofline": dict(kernel_roofline(ctx, stats.last_kernel, bitops, kern_ms, dev),
-                             kernel_ms=kern_ms),
-            "clocks": clk.summary()}
-    if args.r2_mode != "exact":
-        line["config"]["r2_mode"] = args.r2_mode
-    if not args.no_e2e:
-        Th = ctx.pinned_empty((m, K), np.uint64)
-        Th[:] = T.cpu().numpy().view(np.uint64)
-        bch = ctx.pinned_empty((m,), np.uint32)
-        bch[:] = bc.cpu().numpy().view(np.uint32)
-        outh = ctx.pinned_empty((m, W), np.float32)
-        ctx.set_option(api.OPT_BAND_ROWS, 8192)
-        for _ in range(max(1, args.warmup)):
-            ctx.ld_band(Th, bch, S=S, band=W, r2_out=outh)
-        ts = []
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            ctx.ld_band(Th, bch, S=S, band=W, r2_out=outh)
-            ts.append(time.perf_counter() - t0)
-        line["e2e"] = {"value": pairs * len(ts) / sum(ts), "unit": "pairs/s",
-                       "h2d_bytes_per_step": m * K * 8 + m * 4,
-                       "d2h_bytes_per_step": m * W * 4,
-                       "api": "qld_cuda_ld_band (pinned host buffers, streamed)"}
-    ctx.close()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-
-
-def served_arm(args, rank, world, local_rank):
+def section_served(args, local_rank, flush=None, check_queries=12):
     """Served workload: 22 resident chromosomes (50,000-250,000 SNPs x 20,000
     haplotypes, copying model), a Poisson stream of region-vs-region queries
     (each side 100-20,000 SNPs, uniform placement), admitted by output memory.
-    The arrival rate is `load` x the capacity measured by a saturated burst."""
+    The arrival rate is `load` x the capacity measured by a saturated burst.
+    Parity: `check_queries` more queries from the same distribution, their r^2
+    blocks fetched and three B rows each checked against the oracle, and the
+    device summary (count >= threshold, maximum) against the fetched block."""
     import threading
 
     import numpy as np
     import torch
 
     from qld_b200 import api, synth
+    oracle = _oracle()
     dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
-    rng = np.random.default_rng(5 + rank)
+    rng = np.random.default_rng(5)
     H = 20_000
     srv = api.Server(local_rank, pool_bytes=args.pool_gb << 30, max_inflight=args.inflight)
-    sizes = []
+    sizes, tables = [], []
     for c in range(22):
         m = int(rng.integers(50_000, 250_001))
         f = synth.beta_freqs(m, 0.1, 1.0, 100 + c, device=dev, clip_min=1.0 / H)
@@ -679,7 +999,7 @@ def served_arm(args, rank, world, local_rank):
         bc = synth.popcount_rows(T).to(torch.int32)
         srv.add_table(T, bc, H)
         sizes.append(m)
-        del T, bc
+        tables.append((T, bc))
     torch.cuda.synchronize()
 
     def draw(n):
@@ -692,9 +1012,10 @@ def served_arm(args, rank, world, local_rank):
             qs.append((c, a0, a0 + la, b0, b0 + lb))
         return qs
 
-    def run(qs, rate):
+    def run(qs, rate, keep=False):
         """Submit qs (Poisson arrivals at `rate` per second, all at once if
-        rate is None); return results and the wall time to the last one."""
+        rate is None); return results, the wall time to the last one, and the
+        query ids in submission order."""
         results = {}
         lock = threading.Lock()
         done_evt = threading.Event()
@@ -704,7 +1025,7 @@ def served_arm(args, rank, world, local_rank):
                 for r in srv.poll(wait_ms=50):
                     with lock:
                         results[r.id] = r
-                    if r.status == api.OK:
+                    if r.status == api.OK and not keep:
                         srv.release(r.id)
             done_evt.set()
 
@@ -713,45 +1034,105 @@ def served_arm(args, rank, world, local_rank):
         th.start()
         gaps = rng.exponential(1.0 / rate, len(qs)) if rate else np.zeros(len(qs))
         t_next = t0
+        ids = []
         for q, g in zip(qs, gaps):
             t_next += g
             d = t_next - time.perf_counter()
             if d > 0:
                 time.sleep(d)
-            srv.submit(q[0], q[1], q[2], q[3], q[4], threshold=0.2)
+            ids.append(srv.submit(q[0], q[1], q[2], q[3], q[4], threshold=0.2))
         done_evt.wait(timeout=3600)
-        return results, time.perf_counter() - t0
+        return results, time.perf_counter() - t0, ids
 
     warm = draw(max(8, args.warmup * 8))
     run(warm, None)
     calib = draw(min(400, max(50, args.queries // 10)))
-    res_c, t_c = run(calib, None)
+    res_c, t_c, _ = run(calib, None)
     pairs_c = sum(r.pairs for r in res_c.values())
     capacity_qps = len(calib) / t_c
     qs = draw(args.queries)
-    res, t = run(qs, args.load * capacity_qps)
+    with ClockSampler(local_rank) as clk:
+        clk.mark_start()
+        res, t, _ = run(qs, args.load * capacity_qps)
+        clk.mark_end()
     lat = np.array([r.latency_ms for r in res.values()])
     pairs = sum(r.pairs for r in res.values())
     K = (H + 63) // 64
-    line = {"metric": METRIC + ", served queries", "value": pairs / t, "unit": "pairs/s",
-            "n_gpus": world, "steps": 1, "warmup": args.warmup, "ms_per_step": t * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u64 popcount / f32 r2", "data": "synthetic",
-            "config": {"workload": f"served_{args.queries}_queries", "chromosomes": 22,
-                       "snps_per_chromosome": "U(50000,250000)", "haplotypes": H,
-                       "query_side_snps": "U(100,20000)", "arrivals": "Poisson",
-                       "offered_load": args.load, "pool_gb": args.pool_gb,
-                       "max_inflight_batches": args.inflight,
-                       "delivered": "per query: count of r2 >= 0.2 (< 100), sum, max; "
-                                    "r2 blocks stay on the device until released"},
-            "bitops_per_s": pairs * 64 * K / t,
-            "latency_ms": {"p50": float(np.percentile(lat, 50)),
-                           "p99": float(np.percentile(lat, 99)),
-                           "mean": float(lat.mean()), "max": float(lat.max())},
-            "arrival_qps": args.load * capacity_qps, "completed": len(res),
-            "failed": sum(1 for r in res.values() if r.status != api.OK),
-            "saturated_burst": {"queries": len(calib), "pairs_per_s": pairs_c / t_c}}
+    out = {"config": {"workload": f"served_{args.queries}_queries", "chromosomes": 22,
+                      "snps_per_chromosome": "U(50000,250000)", "haplotypes": H,
+                      "query_side_snps": "U(100,20000)", "arrivals": "Poisson",
+                      "offered_load": args.load, "pool_gb": args.pool_gb,
+                      "max_inflight_batches": args.inflight,
+                      "delivered": "per query: count of r2 >= 0.2 (< 100), sum, max; "
+                                   "r2 blocks stay on the device until released"},
+           "value": pairs / t, "unit": "pairs/s", "wall_s": t, "queries": len(qs),
+           "bitops_per_s": pairs * 64 * K / t,
+           "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                          "p99": float(np.percentile(lat, 99)),
+                          "mean": float(lat.mean()), "max": float(lat.max())},
+           "arrival_qps": args.load * capacity_qps, "completed": len(res),
+           "failed": sum(1 for r in res.values() if r.status != api.OK),
+           "saturated_burst": {"queries": len(calib), "pairs_per_s": pairs_c / t_c},
+           "clocks": clk.summary(),
+           "timing": "host wall clock from the first arrival to the last result"}
+    if not args.no_parity and check_queries:
+        cq = draw(check_queries)
+        got, _, ids = run(cq, None, keep=True)
+        groups, summary_ok = [], True
+        for q, qid in zip(cq, ids):
+            c, a0, a1, b0, b1 = q
+            r = got[qid]
+            if r.status != api.OK:
+                summary_ok = False
+                continue
+            blk = np.empty((b1 - b0, a1 - a0), np.float32)
+            srv.fetch(qid, blk)
+            srv.release(qid)
+            sym = (a0, a1) == (b0, b1)
+            full = (np.arange(a1 - a0)[None, :] > np.arange(b1 - b0)[:, None]) if sym \
+                else np.ones(blk.shape, bool)
+            v = blk[full]
+            v = v[v < 100]
+            summary_ok &= int((v >= 0.2).sum()) == r.n_above
+            summary_ok &= (float(v.max()) if v.size else 0.0) == r.max_r2
+            rows = sorted({0, b1 - b0 - 1, int(rng.integers(0, b1 - b0))})
+            T, bc = tables[c]
+            Kc = T.shape[1]
+            A = T[a0:a1].cpu().numpy().view(np.uint64)
+            bcA = bc[a0:a1].cpu().numpy().astype(np.uint32)
+            idx = torch.as_tensor([b0 + x for x in rows], device=dev)
+            B = T.index_select(0, idx)[:, :Kc].contiguous().cpu().numpy().view(np.uint64)
+            bcB = bc.index_select(0, idx).cpu().numpy().astype(np.uint32)
+            rr = np.array(rows)
+            valid = (np.arange(a1 - a0)[None, :] >= rr[:, None]) if sym \
+                else np.ones((len(rows), a1 - a0), bool)
+            groups.append(dict(A=A, bcA=bcA, B=B, bcB=bcB, S=H, got=blk[rows], valid=valid))
+        par = oracle.check_groups(groups, mode="exact") if groups else {"ok": False}
+        par["summaries_match_blocks"] = bool(summary_ok)
+        par["ok"] = par["ok"] and bool(summary_ok)
+        par["sample"] = (f"{check_queries} more queries from the same distribution: 3 B rows "
+                         "of each r2 block x all its A rows; device summaries vs the block")
+        out["parity"] = par
     srv.close()
+    del tables
+    return out
+
+
+def standalone(args, rank, world, local_rank):
+    """--workload windowed|batched|served: that section alone, as its own
+    line."""
+    import torch
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    fn = {"windowed": section_windowed, "batched": section_batched,
+          "served": section_served}[args.workload]
+    res = fn(args, local_rank, flush)
+    suffix = {"windowed": ", windowed band", "batched": ", batched tasks",
+              "served": ", served queries"}[args.workload]
+    line = {"metric": METRIC + suffix, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64 popcount / f32 r2", "data": "synthetic", **res}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -772,14 +1153,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        if args.workload == "batched":
-            batched_arm(args, rank, world, local_rank)
-        elif args.workload == "windowed":
-            windowed_arm(args, rank, world, local_rank)
-        elif args.workload == "served":
-            served_arm(args, rank, world, local_rank)
-        else:
+        if args.workload in ("single_region", "all_pairs"):
             ours_arm(args, rank, world, local_rank)
+        else:
+            standalone(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

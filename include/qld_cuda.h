@@ -332,6 +332,8 @@ int qld_cuda_get_stats(qld_ctx *ctx, qld_stats *out, int reset);
  * r^2 band (min(n, 256) rows x m x 4 bytes) must fit in the scratch; larger
  * tasks return QLD_ERR_TOO_LARGE.  Calls share the scratch, so calls that
  * overlap on the GPU (two streams or two threads) race: serialize them.
+ * On an error return nothing of the call is still running on the stream:
+ * a failure after work was queued waits for that work first.
  * No counterpart in the reference.
  */
 #define QLD_NOALLOC_SCRATCH_BYTES (16u << 20)

@@ -8,7 +8,8 @@
  * lands here.  With QLD_CUDA set in the environment the call goes to
  * correlate_cuda() (qld_b200/host/correlate_cuda.c, same arguments);
  * otherwise to the reference's correlate().  The real integration adds a
- * -cuda flag instead.
+ * -cuda flag to qLD-compute instead, which selects correlate_cuda() in the
+ * same place.
  */
 #include <stdlib.h>
 

@@ -38,9 +38,13 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 def build_oracle(with_reference: bool = True) -> None:
     """Compile the restatement, and the reference when its sources exist."""
     subprocess.run(["make", "-s", "-C", _HERE, "libqld_oracle.so"], check=True)
-    ref = os.environ.get("QLD_REFERENCE", "/root/reference")
-    if with_reference and os.path.isdir(os.path.join(ref, "src", "correlator")):
-        subprocess.run(["make", "-s", "-C", _HERE, f"REF={ref}", "ref"], check=True)
+    # The qLD source tree: $QLD_REFERENCE, else the Makefile's REF default.
+    ref = os.environ.get("QLD_REFERENCE") or subprocess.run(
+        ["make", "-s", "--no-print-directory", "-C", _HERE, "ref-dir"], check=True,
+        capture_output=True, text=True).stdout.strip()
+    if with_reference and ref and os.path.isdir(os.path.join(ref, "src", "correlator")):
+        subprocess.run(["make", "-s", f"-j{os.cpu_count() or 1}", "-C", _HERE, f"REF={ref}",
+                        "ref"], check=True)
 
 
 def _lib(name: str) -> ct.CDLL:
@@ -99,6 +103,12 @@ def _lib(name: str) -> ct.CDLL:
                 _u64p, _u32p, ct.POINTER(ct.c_char_p), _u32p, ct.c_int,
                 _u64p, _u32p, ct.POINTER(ct.c_char_p), _u32p, ct.c_int,
                 ct.c_int, ct.c_int, ct.c_int, ct.c_float]
+        elif name == "ref_blis":
+            lib = ct.CDLL(os.path.join(_HERE, "_ref", "libqldref_blis.so"))
+            lib.refb_counts_ld.argtypes = [ct.c_int, ct.c_int, ct.c_int, _u64p, _u64p, _u32p,
+                                           _u32p, ct.c_int, ct.c_int, _u64p, _f32p,
+                                           ct.c_void_p, ct.c_void_p]
+            lib.refb_counts_ld.restype = ct.c_int
         else:
             raise KeyError(name)
         _libs[name] = lib
@@ -266,6 +276,33 @@ def ref_ld_score(bcA, bcB, C64, S, threads=1) -> np.ndarray:
     return out
 
 
+def blis_available() -> bool:
+    return os.path.exists(os.path.join(_HERE, "_ref", "libqldref_blis.so"))
+
+
+def ref_blis_counts_ld(A, bc, S, B=None, bcB=None, C=None, results=None):
+    """The reference's stock -blis path on one task (ref_blis.c): BLIS
+    cblas_dsyrk (single region, lower triangle of C) or cblas_dgemm (two
+    regions), then get_pairwise_ld_score() on one thread.  BLIS threading
+    comes from BLIS_JC_NT / BLIS_IC_NT / ... in the environment.  Returns
+    (counts (n, m) uint64, results (n, m) float32, gemm seconds, ld seconds);
+    C / results may be preallocated (n, m) buffers."""
+    lib = _lib("ref_blis")
+    A = _c(A, np.uint64)
+    bc = _c(bc, np.uint32)
+    single = B is None
+    B = A if single else _c(B, np.uint64)
+    bcB = bc if single else _c(bcB, np.uint32)
+    m, K = A.shape
+    n = B.shape[0]
+    C = np.empty((n, m), np.uint64) if C is None else C
+    results = np.empty((n, m), np.float32) if results is None else results
+    tg, tl = ct.c_double(), ct.c_double()
+    lib.refb_counts_ld(m, n, K, A, B, bc, bcB, int(S), 0 if single else 1, C, results,
+                       ct.byref(tg), ct.byref(tl))
+    return C, results, tg.value, tl.value
+
+
 def ref_write_report(path, posA, idA, bcA, posB, idB, bcB, S, results, r2limit,
                      posWset2) -> None:
     posA, bcA = _c(posA, np.uint32), _c(bcA, np.uint32)
@@ -290,3 +327,112 @@ def ref_correlate(out_path, log_path, A, posA, idA, bcA, B, posB, idB, bcB, S,
         float(r2limit))
     if rc != 0:
         raise OSError("ref_correlate")
+
+
+# ------------------------------------------------- sampled checks of large --
+
+def r2_errors(got, want64):
+    """Compare FP32 r^2 with the FP64 oracle value by value.  Returns
+    (specials_ok, max_rel, mean_rel, compared): NaN, exact zeros and the
+    123.456 sentinel must match exactly; the relative error is taken over the
+    other values."""
+    got = np.asarray(got).astype(np.float64).ravel()
+    want = np.asarray(want64).astype(np.float64).ravel()
+    nan_w = np.isnan(want)
+    ok = bool(np.array_equal(nan_w, np.isnan(got)))
+    g, w = got[~nan_w], want[~nan_w]
+    sent = w == 123.456
+    ok &= bool(np.all(np.abs(g[sent] - 123.456) < 1e-4))
+    g, w = g[~sent], w[~sent]
+    zero = w == 0
+    ok &= bool(np.all(g[zero] == 0))
+    g, w = g[~zero], w[~zero]
+    if not g.size:
+        return ok, 0.0, 0.0, 0
+    rel = np.abs(g - w) / np.abs(w)
+    return ok, float(rel.max()), float(rel.mean()), int(rel.size)
+
+
+def _group_values(g, mode):
+    """Oracle values for one group: (counts, FP64 r^2, reference r^2 or None)."""
+    C = counts(g["A"], g["B"])
+    want64 = r2_exact(g["bcA"], g["bcB"], C, g["S"])
+    ref = r2_reference(g["bcA"], g["bcB"], C, g["S"], fma_contract=False) \
+        if mode == "reference" else None
+    return C, want64, ref
+
+
+def check_groups(groups, mode="exact", rtol=1e-6, workers=None):
+    """Check r^2 (and counts) of sampled outputs against the oracle.
+
+    Each group is a dict: A (w, K) and B (r, K) packed rows with their bit
+    counts bcA / bcB, S, `got` -- the library's (r, w) r^2 for those rows in
+    its B-major layout --, `valid` (r, w) marking the entries the task
+    defines, and optionally `counts` (r, w).  Groups are evaluated on a
+    thread pool (the C oracle releases the GIL).  Counts must be bit-exact.
+    In "exact" mode r^2 must be within `rtol` relative of the FP64 oracle
+    (NaN, zeros and the 123.456 sentinel exactly); in "reference" mode
+    bit-identical to the reference's float/double sequence.  The max and
+    mean relative error against FP64 are reported in both modes.
+    """
+    from concurrent.futures import ThreadPoolExecutor
+    workers = workers or min(32, os.cpu_count() or 1)
+    with ThreadPoolExecutor(workers) as ex:
+        vals = list(ex.map(lambda g: _group_values(g, mode), groups))
+    got, w64, ref, cnt_ok, rows, pairs = [], [], [], True, 0, 0
+    for g, (C, want64, r) in zip(groups, vals):
+        v = np.asarray(g["valid"], bool)
+        gg = np.asarray(g["got"], np.float32)
+        got.append(gg[v])
+        w64.append(want64[v])
+        if r is not None:
+            ref.append(r[v])
+        if g.get("counts") is not None:
+            cnt_ok &= bool(np.array_equal(np.asarray(g["counts"])[v].astype(np.uint32), C[v]))
+        rows += gg.shape[0]
+        pairs += int(v.sum())
+    got = np.concatenate(got) if got else np.zeros(0, np.float32)
+    w64 = np.concatenate(w64) if w64 else np.zeros(0)
+    specials, max_rel, mean_rel, _ = r2_errors(got, w64)
+    res = {"rows_checked": rows, "pairs_checked": pairs, "r2_max_rel": max_rel,
+           "r2_mean_rel": mean_rel, "r2_mode": mode}
+    has_counts = any(g.get("counts") is not None for g in groups)
+    if has_counts:
+        res["counts_exact"] = cnt_ok
+    if mode == "reference":
+        ref = np.concatenate(ref) if ref else np.zeros(0, np.float32)
+        res["r2_bit_identical"] = bool(np.array_equal(got.view(np.uint32), ref.view(np.uint32)))
+        res["ok"] = res["r2_bit_identical"]
+    else:
+        res["r2_within_tol"] = bool(specials and max_rel <= rtol)
+        res["rtol"] = rtol
+        res["ok"] = res["r2_within_tol"]
+    if has_counts:
+        res["ok"] = res["ok"] and cnt_ok
+    return res
+
+
+def check_rows(A, bcA, Brows, bcBrows, S, got_r2, valid, got_counts=None, mode="exact",
+               rtol=1e-6):
+    """check_groups() for sampled B rows against every row of A, the row set
+    split into groups so the thread pool shares the work."""
+    r = Brows.shape[0]
+    step = max(1, -(-r // 64))
+    groups = []
+    for k in range(0, r, step):
+        sl = slice(k, min(r, k + step))
+        groups.append(dict(A=A, bcA=bcA, B=Brows[sl], bcB=bcBrows[sl], S=S,
+                           got=np.asarray(got_r2)[sl], valid=np.asarray(valid)[sl],
+                           counts=None if got_counts is None else np.asarray(got_counts)[sl]))
+    return check_groups(groups, mode=mode, rtol=rtol)
+
+
+def tile_row_samples(n, block, per_block, rng, extra=()):
+    """Sorted distinct B rows: `per_block` random rows from every block of
+    `block` rows (so every output tile row is sampled), plus `extra`."""
+    rows = set(int(x) for x in extra if 0 <= x < n)
+    for b0 in range(0, n, block):
+        b1 = min(n, b0 + block)
+        k = min(per_block, b1 - b0)
+        rows.update(int(x) for x in rng.choice(np.arange(b0, b1), k, replace=False))
+    return np.array(sorted(rows), np.int64)

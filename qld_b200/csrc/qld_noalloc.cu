@@ -38,7 +38,6 @@ static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_lock;
 unsigned char *g_scratch_dev[kMaxDevices];                 // device address per device
-bool g_device_ok[kMaxDevices];
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -73,7 +72,6 @@ int setup(int dev, unsigned char **scratch) {
             g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
         }
         g_scratch_dev[dev] = static_cast<unsigned char *>(p);
-        g_device_ok[dev] = true;
     }
     *scratch = g_scratch_dev[dev];
     return QLD_OK;
@@ -97,6 +95,19 @@ bool make_map(CUtensorMap *tm, const void *base, int rows, int K, long long ld,
 #define NA_TRY(expr)                                  \
     do {                                              \
         if ((expr) != cudaSuccess) {                  \
+            cudaGetLastError();                       \
+            return QLD_ERR_CUDA;                      \
+        }                                             \
+    } while (0)
+
+// Once work is queued on the caller's stream, a failure first waits for it:
+// the copies still read the caller's host tables and write its r^2 buffer,
+// and the next call must not find the shared scratch still in use.
+#define NA_TRY_Q(expr)                                \
+    do {                                              \
+        if ((expr) != cudaSuccess) {                  \
+            cudaGetLastError();                       \
+            cudaStreamSynchronize(st);                \
             cudaGetLastError();                       \
             return QLD_ERR_CUDA;                      \
         }                                             \
@@ -151,23 +162,23 @@ extern "C" int qld_cuda_ld_noalloc(const uint64_t *A, const uint32_t *bcA, int m
     auto upload = [&](uint64_t *dst, const uint64_t *src, int rows) -> int {
         const size_t bytes = (size_t)rows * K * 8;
         if (Kp == K) {
-            NA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+            NA_TRY_Q(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
         } else if (bytes <= kScratchBytes - o_band) {
             uint64_t *stage = reinterpret_cast<uint64_t *>(scratch + o_band);
-            NA_TRY(cudaMemcpyAsync(stage, src, bytes, cudaMemcpyHostToDevice, st));
-            NA_TRY(launch_pad_rows(dst, Kp, stage, K, rows, st));
+            NA_TRY_Q(cudaMemcpyAsync(stage, src, bytes, cudaMemcpyHostToDevice, st));
+            NA_TRY_Q(launch_pad_rows(dst, Kp, stage, K, rows, st));
         } else {
-            NA_TRY(cudaMemcpy2DAsync(dst, Kp * 8, src, (size_t)K * 8, (size_t)K * 8, rows,
+            NA_TRY_Q(cudaMemcpy2DAsync(dst, Kp * 8, src, (size_t)K * 8, (size_t)K * 8, rows,
                                      cudaMemcpyHostToDevice, st));
         }
         return QLD_OK;
     };
-    NA_TRY(cudaMemsetAsync(status, 0, sizeof(unsigned), st));
+    NA_TRY_Q(cudaMemsetAsync(status, 0, sizeof(unsigned), st));
     if ((rc = upload(d_A, A, m))) return rc;
-    NA_TRY(cudaMemcpyAsync(d_bcA, bcA, (size_t)m * 4, cudaMemcpyHostToDevice, st));
+    NA_TRY_Q(cudaMemcpyAsync(d_bcA, bcA, (size_t)m * 4, cudaMemcpyHostToDevice, st));
     if (!symmetric) {
         if ((rc = upload(d_B, B, n))) return rc;
-        NA_TRY(cudaMemcpyAsync(d_bcB, bcB, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+        NA_TRY_Q(cudaMemcpyAsync(d_bcB, bcB, (size_t)n * 4, cudaMemcpyHostToDevice, st));
     }
 
     // The 128 x 256 tensor-core kernel where its accumulators are exact,
@@ -175,8 +186,11 @@ extern "C" int qld_cuda_ld_noalloc(const uint64_t *A, const uint32_t *bcA, int m
     const bool mma = (long long)K * 64 <= kMmaMaxSamples;
     const KernelShape &ks = mma ? kMmaShape : kPopcShape;
     CUtensorMap tmA, tmB;
-    if (!make_map(&tmA, d_A, m, K, Kp, ks, true) || !make_map(&tmB, d_B, n, K, Kp, ks, false))
+    if (!make_map(&tmA, d_A, m, K, Kp, ks, true) || !make_map(&tmB, d_B, n, K, Kp, ks, false)) {
+        cudaStreamSynchronize(st);
+        cudaGetLastError();
         return QLD_ERR_CUDA;
+    }
 
     for (int b0 = 0; b0 < n; b0 += band) {
         const int b1 = b0 + band < n ? b0 + band : n;
@@ -190,16 +204,16 @@ extern "C" int qld_cuda_ld_noalloc(const uint64_t *A, const uint32_t *bcA, int m
         p.status = status;
         p.timeout_cycles = 4000000000LL;
         const int tiles_b = (b1 - b0 + ks.bn - 1) / ks.bn;
-        NA_TRY(mma ? launch_mma(tmA, tmB, p, tiles_b, R2_EXACT, st)
+        NA_TRY_Q(mma ? launch_mma(tmA, tmB, p, tiles_b, R2_EXACT, st)
                    : launch_popc(tmA, tmB, p, tiles_b, R2_EXACT, st));
         // Stream order keeps the next band's kernel behind this copy.
         if (!symmetric) {
-            NA_TRY(cudaMemcpyAsync(r2_out + (size_t)b0 * m, d_band, (size_t)(b1 - b0) * m * 4,
+            NA_TRY_Q(cudaMemcpyAsync(r2_out + (size_t)b0 * m, d_band, (size_t)(b1 - b0) * m * 4,
                                    cudaMemcpyDeviceToHost, st));
         } else {
             for (int r0 = b0; r0 < b1; r0 += 512) {
                 const int r1 = r0 + 512 < b1 ? r0 + 512 : b1;
-                NA_TRY(cudaMemcpy2DAsync(r2_out + (size_t)r0 * m + r0, (size_t)m * 4,
+                NA_TRY_Q(cudaMemcpy2DAsync(r2_out + (size_t)r0 * m + r0, (size_t)m * 4,
                                          d_band + (size_t)(r0 - b0) * m + r0, (size_t)m * 4,
                                          (size_t)(m - r0) * 4, r1 - r0, cudaMemcpyDeviceToHost,
                                          st));
@@ -207,7 +221,7 @@ extern "C" int qld_cuda_ld_noalloc(const uint64_t *A, const uint32_t *bcA, int m
         }
     }
     unsigned h_status = 0;
-    NA_TRY(cudaMemcpyAsync(&h_status, status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    NA_TRY(cudaStreamSynchronize(st));
+    NA_TRY_Q(cudaMemcpyAsync(&h_status, status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    NA_TRY_Q(cudaStreamSynchronize(st));
     return h_status ? QLD_ERR_TIMEOUT : QLD_OK;
 }

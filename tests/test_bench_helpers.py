@@ -43,3 +43,22 @@ def test_traffic_follows_the_kernel_the_mode_runs():
         "k_ld_mma_wide_traffic_16384.md")
     assert bench.measured_traffic(fp4, "all_pairs_2048x4096_symmetric") is None
     assert bench.measured_traffic(0, WORKLOAD) is None
+
+
+def test_both_arms_print_the_same_config():
+    args = bench.parse(["--impl", "reference"])
+    ours = bench.parse([])
+    assert bench.arm_config(args, 2) == bench.arm_config(ours, 2)
+    cfg = bench.arm_config(ours, 1)
+    assert cfg["workload"] == WORKLOAD and "parallelism" in cfg and "l2" in cfg
+
+
+def test_band_pair_count():
+    assert bench.band_pairs(10, 3) == sum(min(3, 9 - i) for i in range(10))
+    m, W = 200_000, 5000
+    assert bench.band_pairs(m, W) == sum(min(W, m - 1 - i) for i in range(0, m))
+
+
+def test_host_cpu_reports_cores():
+    model, phys, logical = bench.host_cpu()
+    assert 1 <= phys <= logical and isinstance(model, str)

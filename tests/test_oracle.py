@@ -143,3 +143,32 @@ def test_count_states_small_python_restatement():
 
     want = np.array([[states(A[j], B[i]) for j in range(6)] for i in range(4)], np.uint8)
     assert np.array_equal(oracle.count_states(A, B), want)
+
+
+@pytest.mark.skipif(not oracle.blis_available(), reason="BLIS build of the reference absent")
+@pytest.mark.parametrize("m,n,N", [(700, None, 4096), (513, 300, 1000), (257, None, 130)])
+def test_stock_blis_path_matches_the_oracle(m, n, N):
+    """The reference's -blis path (BLIS dsyrk / dgemm with bin_gemm_2x2, then
+    get_pairwise_ld_score) as the CPU baseline times it: counts equal the
+    restatement's (SYRK fills the lower triangle only), r^2 bit-identical to
+    the reference-semantics restatement."""
+    rng = np.random.default_rng(m)
+    K = (N + 63) // 64
+    A = rng.integers(0, 2 ** 63, (m, K), dtype=np.uint64)
+    A[:, -1] &= np.uint64(((1 << 64) - 1) ^ ((1 << (K * 64 - N)) - 1))
+    bcA = oracle.bitcounts(A)
+    if n is None:
+        C, R, _, _ = oracle.ref_blis_counts_ld(A, bcA, N)
+        want = oracle.counts(A)
+        low = np.arange(m)[None, :] >= np.arange(m)[:, None]
+        assert np.array_equal(C[low].astype(np.uint32), want[low])
+        ref = oracle.r2_reference(bcA, bcA, want, N, fma_contract=False)
+        assert np.array_equal(R[low].view(np.uint32), ref[low].view(np.uint32))
+    else:
+        B = rng.integers(0, 2 ** 63, (n, K), dtype=np.uint64)
+        bcB = oracle.bitcounts(B)
+        C, R, _, _ = oracle.ref_blis_counts_ld(A, bcA, N, B=B, bcB=bcB)
+        want = oracle.counts(A, B)
+        assert np.array_equal(C.astype(np.uint32), want)
+        ref = oracle.r2_reference(bcA, bcB, want, N, fma_contract=False)
+        assert np.array_equal(R.view(np.uint32), ref.view(np.uint32))

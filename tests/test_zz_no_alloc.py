@@ -1,11 +1,16 @@
 """GPU test of qld_cuda_ld_noalloc(), the entry point for callers that cannot
 allocate device memory (their GPU memory is owned by another component).
 
-It is checked through the C ABI against the regular entry point,
-qld_cuda_ld(), on the same inputs: r^2 within the suite's tolerance (1e-6
-relative; special values exact), on two calls in a row, because every call
-reuses the same static scratch array and must not see the previous call's
-contents.  The file is named to be collected last.
+It is checked through the C ABI against the oracle (counts from
+oracle.counts, r^2 from oracle.r2_exact: within the suite's tolerance of
+1e-6 relative, special values exact) and against the regular entry point,
+qld_cuda_ld(), on the same inputs.  Every call reuses the same static
+scratch array, so each task is run twice with a call on a different task
+(other m, K and S, odd K so the r^2 band area serves as the staging area)
+in between: the second call must not depend on what the previous call left
+there.  The cases cover several output bands for one and two regions, and
+an odd-K table too large for the band area, which goes up row by row.  The
+file is named to be collected last.
 """
 import ctypes as ct
 
@@ -19,6 +24,7 @@ from qld_b200 import api, synth
 pytestmark = pytest.mark.gpu
 
 ERR_TOO_LARGE = -8
+SCRATCH = 16 << 20
 
 
 def _lib():
@@ -29,39 +35,77 @@ def _lib():
     return lib
 
 
-def _noalloc(lib, A, bcA, B, bcB, S, symmetric):
-    m, K = A.shape
-    n = m if symmetric else B.shape[0]
-    out = np.full((n, m), np.nan, np.float32)
-    rc = lib.qld_cuda_ld_noalloc(A.ctypes.data, bcA.ctypes.data, m,
-                                 None if symmetric else B.ctypes.data,
-                                 None if symmetric else bcB.ctypes.data, n, K, int(S),
-                                 int(symmetric), out.ctypes.data, None)
+def _task(m, n, N, sym, seed):
+    t, _ = synth.all_pairs_workload(m=m + (0 if sym else n), n=N, seed=seed)
+    T = t.numpy().view(np.uint64)
+    A = np.ascontiguousarray(T[:m])
+    B = A if sym else np.ascontiguousarray(T[m:])
+    bcA = oracle.bitcounts(A)
+    bcB = bcA if sym else oracle.bitcounts(B)
+    want = oracle.r2_exact(bcA, bcB, oracle.counts(A, None if sym else B), N)
+    return dict(A=A, B=B, bcA=bcA, bcB=bcB, m=m, n=n, N=N, sym=sym, want=want,
+                mask=lower_mask(n, m) if sym else None)
+
+
+def _noalloc(lib, t):
+    m, K = t["A"].shape
+    out = np.full((t["n"], m), np.nan, np.float32)
+    rc = lib.qld_cuda_ld_noalloc(t["A"].ctypes.data, t["bcA"].ctypes.data, m,
+                                 None if t["sym"] else t["B"].ctypes.data,
+                                 None if t["sym"] else t["bcB"].ctypes.data, t["n"], K,
+                                 int(t["N"]), int(t["sym"]), out.ctypes.data, None)
     return rc, out
+
+
+def _bands(m, n, N, sym):
+    """Output bands the entry point uses for this task (its scratch layout)."""
+    K = (N + 63) // 64
+    Kp = K + (K & 1)
+    a = lambda x: (x + 255) & ~255  # noqa: E731
+    off = a(256 + m * 4)
+    if not sym:
+        off = a(off + n * 4)
+    off = a(off + m * Kp * 8)
+    if not sym:
+        off = a(off + n * Kp * 8)
+    fit = (SCRATCH - off) // (m * 4)
+    band = n if fit >= n else fit // 256 * 256
+    return -(-n // band), SCRATCH - off
 
 
 @pytest.mark.parametrize("m,n,N,sym", [
     (2048, 2048, 4096, True),    # the all-pairs workload
-    (3000, 3000, 4096, True),    # several output bands through the scratch
-    (700, 450, 9000, False),     # two regions (K = 141: rows padded on the device)
-    (1500, 1500, 2049, True),    # single region, K = 33
+    (3000, 3000, 4096, True),    # single region, several output bands
+    (3000, 2000, 4096, False),   # two regions, several output bands
+    (700, 450, 9000, False),     # two regions, K = 141: rows padded on the device
+    (4000, 4000, 16_800, True),  # K = 263: table larger than the band area
 ])
-def test_noalloc_matches_regular_entry_point_twice(m, n, N, sym):
+def test_noalloc_matches_oracle_and_regular_entry_point(m, n, N, sym):
     lib = _lib()
-    t, _ = synth.all_pairs_workload(m=m + (0 if sym else n), n=N, seed=m + 3 * n)
-    T = t.numpy().view(np.uint64)
-    A = np.ascontiguousarray(T[:m])
-    B = None if sym else np.ascontiguousarray(T[m:])
-    bcA = oracle.bitcounts(A)
-    bcB = bcA if sym else oracle.bitcounts(B)
+    t = _task(m, n, N, sym, seed=m + 3 * n + N)
+    other = _task(900, 900, 2049, True, seed=7)        # K = 33, staged through the band area
     with api.Context(0) as ctx:
         ctx.set_option(api.OPT_R2_MODE, api.R2_EXACT)
-        want = ctx.ld(A, bcA, B, bcB, S=N, symmetric=sym)
-    mask = lower_mask(n, m) if sym else None
+        regular = ctx.ld(t["A"], t["bcA"], None if sym else t["B"], None if sym else t["bcB"],
+                         S=N, symmetric=sym)
+    assert_r2_close(regular, t["want"], mask=t["mask"])
     for _ in range(2):
-        rc, got = _noalloc(lib, A, bcA, B, bcB, N, sym)
+        rc, got = _noalloc(lib, t)
         assert rc == api.OK
-        assert_r2_close(got, want.astype(np.float64), mask=mask)
+        assert_r2_close(got, t["want"], mask=t["mask"])
+        assert_r2_close(got, regular, mask=t["mask"])
+        rc, got_other = _noalloc(lib, other)
+        assert rc == api.OK
+        assert_r2_close(got_other, other["want"], mask=other["mask"])
+
+
+def test_case_shapes_reach_the_paths_they_name():
+    """The parameters above reach what their comments say (scratch layout
+    restated): several bands, and a table past the band area."""
+    assert _bands(3000, 3000, 4096, True)[0] > 1
+    assert _bands(3000, 2000, 4096, False)[0] > 1
+    bands, area = _bands(4000, 4000, 16_800, True)
+    assert bands > 1 and 4000 * 263 * 8 > area
 
 
 def test_noalloc_rejects_tasks_beyond_its_scratch():
