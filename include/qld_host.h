@@ -52,6 +52,15 @@ typedef struct qld_table {
 int qld_mdf_read_header(const char *dir, qld_mdf_header *h);
 
 /*
+ * How many of the sample names on the dataset's #CHROM line appear in
+ * `names` (all of them when nnames is 0): makeValidList() + sample_isValid()
+ * (correlate_IO.c:60-76,262-290) for a -sampleList read by getFilter()
+ * (correlate_IO.c:35-58).  qLD-compute multiplies the result by the ploidy
+ * to get the valid sample count that sizes K (correlate_function.c:112-122).
+ */
+int qld_mdf_listed_samples(const char *dir, const char *const *names, int nnames, int *listed);
+
+/*
  * Rows with pos_min <= POS <= pos_max of every part of the dataset, in file
  * order, K words per row (K = ceil(valid samples / 64)); words past K on a
  * line are ignored, as qLD-compute ignores them (qLD-parse-2MDF's diploid

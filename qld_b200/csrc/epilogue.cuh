@@ -11,7 +11,8 @@
 //                 No 64-bit integer arithmetic and one conversion per pair.
 //   R2_REFERENCE  the reference's float/double operation sequence
 //                 (qld_device.cuh: r2_reference), bit for bit, evaluated
-//                 branch-free (r2_reference_fast) with a rare fallback.
+//                 branch-free in FP32 (r2_reference_ff) with a rare
+//                 fallback to the literal sequence.
 // Per-column factors live in shared memory (filled once per tile); the
 // per-row (A) factors in registers.
 #pragma once
@@ -21,32 +22,69 @@
 namespace qld {
 namespace epi {
 
-// Shared-memory column factors of one tile: BN entries each of
-// d0 (exact: 1/(c(S-c)); reference: 1 - c/S), d1 (exact: c as double),
-// c (bit count), v (reference: c/S as float).  24 bytes per column.
+// ------------------------------------------- R2_REFERENCE column factors --
+//
+// One float4 per column (and per A row, in registers): x = v = fl32(c/S) as
+// the reference computes it; y + z = 1/(v(1-v)) as an unevaluated pair of
+// floats (y = RN32 of the FP64 value, z = RN32 of the remainder: ~2^-48
+// relative); w = RN32(1/v).  A zero row (c = 0) is all zeros, so every pair
+// with it evaluates to 0 -- the reference's rule for an empty SNP -- without
+// a test.  A row with v >= 1 (c = S, or a bit count above S) carries a NaN
+// in y, which sends every pair with it to the literal sequence.
+struct ColsR {
+    float4 *f;
+    __device__ __forceinline__ ColsR(uint8_t *base, int) : f(reinterpret_cast<float4 *>(base)) {}
+};
+constexpr int COLR_BYTES = 16;
+
+__device__ __forceinline__ float4 ref_factors(uint32_t c, int S) {
+    if (c == 0u) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float v = __fdiv_rn((float)c, (float)S);
+    if (!(v < 1.0f)) return make_float4(v, __uint_as_float(0x7FC00000u), 0.0f, 1.0f);
+    const double om = __dsub_rn(1.0, (double)v);
+    const double i = __ddiv_rn(1.0, __dmul_rn((double)v, om));
+    const float hi = __double2float_rn(i);
+    return make_float4(v, hi, __double2float_rn(__dsub_rn(i, (double)hi)), __frcp_rn(v));
+}
+
+__device__ __forceinline__ void store_col_ref(const ColsR &f, int bl, uint32_t c, int S) {
+    f.f[bl] = ref_factors(c, S);
+}
+
+// Per-thread A-row factors of the reference mode.
+struct ARowR {
+    float4 k;           // ref_factors of the row
+    uint32_t c;
+    float Sf, rSf;      // (float)S and its correctly rounded reciprocal
+};
+
+__device__ __forceinline__ ARowR make_arow_ref(uint32_t c, int S) {
+    ARowR r;
+    r.k = ref_factors(c, S);
+    r.c = c;
+    r.Sf = (float)S;
+    r.rSf = __frcp_rn(r.Sf);
+    return r;
+}
+
+// Shared-memory column factors of one tile for the integer-count kernels:
+// BN entries each of d0 = 1/(c(S-c)) and d1 = c as double (R2_EXACT), or one
+// ColsR float4 at the same address (R2_REFERENCE).  24 bytes per column.
 struct Cols {
+    uint8_t *base;
     double *d0, *d1;
-    uint32_t *c;
-    float *v;
-    __device__ __forceinline__ Cols(uint8_t *base, int bn)
-        : d0(reinterpret_cast<double *>(base)),
-          d1(reinterpret_cast<double *>(base) + bn),
-          c(reinterpret_cast<uint32_t *>(reinterpret_cast<double *>(base) + 2 * bn)),
-          v(reinterpret_cast<float *>(reinterpret_cast<uint32_t *>(
-                reinterpret_cast<double *>(base) + 2 * bn) + bn)) {}
+    __device__ __forceinline__ Cols(uint8_t *b, int bn)
+        : base(b), d0(reinterpret_cast<double *>(b)), d1(reinterpret_cast<double *>(b) + bn) {}
 };
 constexpr int COL_BYTES = 24;
 
 template <int MODE>
 __device__ __forceinline__ void store_col(const Cols &f, int bl, uint32_t c, int S) {
-    f.c[bl] = c;
     if (MODE == R2_EXACT) {
         f.d0[bl] = row_exact(c, S).inv_var;
         f.d1[bl] = (double)c;
     } else {
-        const RowRef r = row_ref(c, S);
-        f.v[bl] = r.v;
-        f.d0[bl] = r.one_minus;
+        store_col_ref(ColsR(f.base, 0), bl, c, S);
     }
 }
 
@@ -54,8 +92,7 @@ __device__ __forceinline__ void store_col(const Cols &f, int bl, uint32_t c, int
 struct ARow {
     uint32_t c;
     double inv, cd;     // exact
-    RowRef ref;         // reference
-    float Sf, rSf;      // reference: (float)S and its correctly rounded reciprocal
+    ARowR rr;           // reference
 };
 
 template <int MODE>
@@ -66,9 +103,7 @@ __device__ __forceinline__ ARow make_arow(uint32_t c, int S) {
         r.inv = row_exact(c, S).inv_var;
         r.cd = (double)c;
     } else {
-        r.ref = row_ref(c, S);
-        r.Sf = (float)S;
-        r.rSf = __frcp_rn(r.Sf);
+        r.rr = make_arow_ref(c, S);
     }
     return r;
 }
@@ -91,73 +126,59 @@ __device__ __forceinline__ float pair_r2_exact(uint32_t cnt, const ARow &ra, con
 
 // ------------------------------------------- R2_REFERENCE without branches --
 //
-// The reference's operation sequence (r2_reference) rearranged so that a
-// chunk's 32 pairs run branch-free and with fewer conversions:
-//  * v3 = fl32(cab / S) by Markstein's FMA correction: q = RN(cab * y) with
-//    y = RN(1/S), then RN(q + (cab - q*S) * y), the residual exact in one
-//    FMA.  With y the correctly rounded reciprocal this is the correctly
-//    rounded quotient (P. Markstein, IBM J. Res. Dev. 34(1), 1990); cab and
-//    S are integers <= 2^24, exact in FP32.
-//  * fl32(RN64(x / den)), the reference's FP64 division rounded to float:
-//    Newton-Raphson reciprocal of den (three steps from the rcp.approx.ftz.f64
-//    seed, each squaring the relative error), q = x * y with one residual
-//    correction, then a rounding test in the manner of Ziv: if q lies more
-//    than 64 FP64 ulps from the nearest FP32 rounding midpoint, fl32(q) =
-//    fl32(RN64(x / den)).  Pairs failing it (about 3 in 10^7 at realistic S;
-//    ~10^-4 at S <= 100, whose simple fractions meet midpoints more often)
-//    or whose quotient would be an FP32 subnormal or negative are flagged
-//    and recomputed with r2_reference.
+// The reference's operation sequence (r2_reference) gives, per pair,
+// fl32(RN64(x / den)) with x = fl32(d*d), d = fl32(v3 - p12),
+// v3 = fl32(cab/S), p12 = fl32(vA*vB) and den = RN64(RN64(p12*(1-vA))*(1-vB)).
+// r2_reference_ff evaluates it in FP32 alone (no FP64 instruction, no
+// conversion, no MUFU), branch-free:
+//  * v3 by Markstein's FMA correction: q = RN(cab * y) with y = RN(1/S),
+//    then RN(q + (cab - q*S) * y), the residual exact in one FMA; with y the
+//    correctly rounded reciprocal this is the correctly rounded quotient
+//    (P. Markstein, IBM J. Res. Dev. 34(1), 1990); cab and S are integers
+//    <= 2^24, exact in FP32.  p12, d and x as in the reference (__f*_rn: no
+//    contraction).
+//  * 1/den to ~2^-45: with e = vA*vB - p12 exact (the FMA TwoProduct),
+//    p12*(1-vA)*(1-vB) = vA(1-vA) * vB(1-vB) * (1 - e/(vA vB)), so
+//    1/den = IA * IB * (1 + t) up to 2^-48, where IA = 1/(vA(1-vA)) and IB
+//    are the rows' float pairs (y + z) and t = e * (1/vA) * (1/vB); the
+//    reference's two FP64 roundings of den move it by at most 2^-52.
+//    q = x * IA * IB * (1 + t) is formed as an unevaluated float pair
+//    (qh, ql) with FMA products (Dekker / Ogita-Rump-Oishi style error-free
+//    transformations).
+//  * The rounding test: RN32(qh + ql +- 2^-40 qh) are equal when no FP32
+//    rounding midpoint lies within 2^-40 of the quotient, far beyond the
+//    evaluation error, and then RN32(qh + ql) = fl32(RN64(x / den)).
+//    Pairs failing it (~1e-5 at realistic S; more at S <= 100, whose simple
+//    fractions meet midpoints more often), with a row whose v >= 1 (NaN
+//    factors), or with 0 < x < 2^-100 (a subnormal-range quotient) are
+//    flagged and recomputed with r2_reference.
 //  * (double)r > 1.0001 is r > 1 + 838 * 2^-23, the largest float not above
-//    1.0001.  x / 0 (a fixed SNP) is +inf, hence 123.456 (-inf, kept, when
-//    a bit count above S makes den -0); 0 / 0 is the x86 default NaN the
-//    reference's build produces (0xFFC00000).
-// Moving the FP32<->FP64 conversions to integer bit-field arithmetic and
-// seeding the reciprocal from the bit pattern instead (four Newton steps)
-// measured slower: 5.16 / 5.42 ms against 4.78 / 4.88 ms on the single region.
-__device__ __forceinline__ double rcp_seed(double x) {
-    double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    return y;
-}
-
-__device__ __forceinline__ float r2_reference_fast(float cab, const RowRef &A, uint32_t cB,
-                                                   float vB, double omB, float Sf, float rSf,
-                                                   bool &redo) {
-    const float q0 = __fmul_rn(cab, rSf);
-    const float v3 = __fmaf_rn(__fmaf_rn(-q0, Sf, cab), rSf, q0);
-    const float p12 = __fmul_rn(A.v, vB);
+//    1.0001.
+// Exact zeros need no test: a zero row's factors are 0, so q = 0.
+// The earlier FP64 form (Newton reciprocal of den from rcp.approx.f64 with a
+// rounding test in FP64) spent its time in FP64 conversions and the MUFU.
+__device__ __forceinline__ float r2_reference_ff(float cab, const ARowR &A, float4 B,
+                                                 bool &redo) {
+    const float q0 = __fmul_rn(cab, A.rSf);
+    const float v3 = __fmaf_rn(__fmaf_rn(-q0, A.Sf, cab), A.rSf, q0);
+    const float p12 = __fmul_rn(A.k.x, B.x);
+    const float e = __fmaf_rn(A.k.x, B.x, -p12);
     const float d = __fsub_rn(v3, p12);
-    const float r = __fmul_rn(d, d);
-    const double den = __dmul_rn(__dmul_rn((double)p12, A.one_minus), omB);
-    const double x = (double)r;
-    double y = rcp_seed(den), e = 0.0;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        e = __fma_rn(-den, y, 1.0);
-        y = __fma_rn(y, e, y);
-    }
-    double q = __dmul_rn(x, y);
-    q = __fma_rn(__fma_rn(-q, den, x), y, q);
-    const long long mid = (long long)(__double_as_longlong(q) & 0x1FFFFFFFLL) - (1LL << 28);
-    const bool dz = den == 0.0;
-    const bool zero = A.c == 0u || cB == 0u;
-    // den is 0 or in [2^-96, 1] for consistent counts; a negative den (bit
-    // counts above S) takes the plain sequence.  (Dropping the range test
-    // and testing the low word alone measured 4.89 / 4.82 ms against
-    // 4.78 / 4.95 ms: the single-SM kernel, the one used, runs this form
-    // faster.)
-    // |e| <= 2^-20 before the last Newton step leaves y within ~2^-40 of
-    // 1/den whatever the seed's accuracy, which the 64-ulp margin needs
-    redo = !zero && !dz &&
-           (!(den > 0x1p-1000 && den < 0x1p1000) || (q != 0.0 && q < 0x1p-126) ||
-            (mid >= -64 && mid <= 64) || !(fabs(e) <= 0x1p-20));
-    // x / 0 is an infinity of den's sign (-0 when a bit count exceeds S)
-    float f = dz ? __uint_as_float(r == 0.0f ? 0xFFC00000u
-                                             : 0x7F800000u | ((uint32_t)__double2hiint(den) &
-                                                              0x80000000u))
-                 : __double2float_rn(q);
-    if (f > __uint_as_float(0x3F800000u + 838u)) f = 123.456f;
-    return zero ? 0.0f : f;
+    const float x = __fmul_rn(d, d);
+    const float Ph = __fmul_rn(A.k.y, B.y);
+    float Pl = __fmaf_rn(A.k.y, B.y, -Ph);
+    Pl = __fmaf_rn(A.k.y, B.z, Pl);
+    Pl = __fmaf_rn(A.k.z, B.y, Pl);
+    const float t = __fmul_rn(e, __fmul_rn(A.k.w, B.w));
+    const float qh = __fmul_rn(x, Ph);
+    float ql = __fmaf_rn(x, Ph, -qh);
+    ql = __fmaf_rn(x, Pl, ql);
+    ql = __fmaf_rn(qh, t, ql);
+    const float rh = __fadd_rn(qh, __fmaf_rn(qh, 0x1p-40f, ql));
+    const float rl = __fadd_rn(qh, __fmaf_rn(qh, -0x1p-40f, ql));
+    const bool tiny = __float_as_uint(x) - 1u < __float_as_uint(0x1p-100f) - 1u;
+    redo = !(rh == rl) || tiny;
+    return rh > __uint_as_float(0x3F800000u + 838u) ? 123.456f : rh;
 }
 
 // The reference-mode chunk: every pair on the fast path, the flagged ones
@@ -166,7 +187,7 @@ __device__ __forceinline__ float r2_reference_fast(float cab, const RowRef &A, u
 // FLOATCNT: v holds each count as F32 bits (the 4-bit kernels' accumulators),
 // else as an integer shifted left by SHIFT.
 template <int SHIFT, bool FLOATCNT>
-__device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARow &ra, const Cols &f,
+__device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARowR &ra, const ColsR &f,
                                           int bl0, int b0, int a, bool a_ok, int n, int dlo,
                                           int dhi, float *r2, long long ldr, uint32_t *counts,
                                           long long ldc, int row0, int S) {
@@ -181,8 +202,7 @@ __device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARow &ra, con
             if (oc && b < n && a - b >= dlo && a - b <= dhi)
                 oc[(long long)t * ldc] = FLOATCNT ? (uint32_t)cf : raw >> SHIFT;
             bool rd;
-            const float r = r2_reference_fast(cf, ra.ref, f.c[bl0 + t], f.v[bl0 + t],
-                                              f.d0[bl0 + t], ra.Sf, ra.rSf, rd);
+            const float r = r2_reference_ff(cf, ra, f.f[bl0 + t], rd);
             v[t] = rd ? raw : __float_as_uint(r);   // a flagged pair keeps its count
             redo |= (uint32_t)rd << t;
         }
@@ -197,16 +217,21 @@ __device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARow &ra, con
     }
     if (!a_ok) redo = 0;
     if (__any_sync(0xffffffffu, redo != 0)) {
+        RowRef rA;
+        rA.c = ra.c;
+        rA.v = ra.k.x;
+        rA.one_minus = __dsub_rn(1.0, (double)ra.k.x);
 #pragma unroll
         for (int t = 0; t < 32; ++t) {
             const bool rd = (redo >> t) & 1u;
             if (__any_sync(0xffffffffu, rd) && rd) {
+                const float4 cb = f.f[bl0 + t];
                 RowRef rb;
-                rb.c = f.c[bl0 + t];
-                rb.v = f.v[bl0 + t];
-                rb.one_minus = f.d0[bl0 + t];
+                rb.c = cb.x != 0.0f;        // only the zero rule reads it
+                rb.v = cb.x;
+                rb.one_minus = __dsub_rn(1.0, (double)cb.x);
                 const uint32_t cnt = FLOATCNT ? (uint32_t)__uint_as_float(v[t]) : v[t] >> SHIFT;
-                v[t] = __float_as_uint(r2_reference(cnt, ra.ref, rb, S));
+                v[t] = __float_as_uint(r2_reference(cnt, rA, rb, S));
             }
         }
     }
@@ -236,8 +261,8 @@ __device__ __forceinline__ void chunk(uint32_t (&v)[32], const ARow &ra, const C
                                       int dhi, float *r2, long long ldr, uint32_t *counts,
                                       long long ldc, int row0, int S) {
     if constexpr (MODE == R2_REFERENCE) {
-        chunk_ref<SHIFT, false>(v, ra, f, bl0, b0, a, a_ok, n, dlo, dhi, r2, ldr, counts, ldc,
-                                row0, S);
+        chunk_ref<SHIFT, false>(v, ra.rr, ColsR(f.base, 0), bl0, b0, a, a_ok, n, dlo, dhi, r2,
+                                ldr, counts, ldc, row0, S);
     } else {
         if (!a_ok) return;
         const double S_d = (double)S;

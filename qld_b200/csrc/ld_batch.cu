@@ -75,17 +75,17 @@ constexpr int QSLOTS = 4;                                    // item ring depth
 constexpr int ITEM_USERS = 2 * (1 + UNPACK_WARPS + EPI_WARPS);
 
 // Shared-memory layout per r^2 mode: R2_EXACT needs 8 bytes of column
-// factors per column (epi::ColsF), R2_REFERENCE 24 (epi::Cols); the room this
-// saves holds a sixth packed stage (more TMA lookahead).
+// factors per column (epi::ColsF), R2_REFERENCE 16 (epi::ColsR); both leave
+// room for six packed stages (more TMA lookahead than five).
 template <int MODE>
 struct Smem {
-    static constexpr int PST = MODE == R2_EXACT ? 6 : 5;   // packed stages in flight
+    static constexpr int PST = 6;                          // packed stages in flight
     static constexpr int OFF_UA = 0;
     static constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
     static constexpr int OFF_PA = OFF_UB + UST * UB_BYTES;
     static constexpr int OFF_PB = OFF_PA + PST * PA_BYTES;
     static constexpr int OFF_ROWS = OFF_PB + PST * PB_BYTES;
-    static constexpr int ROWS_BYTES = COLS_N * (MODE == R2_EXACT ? 8 : epi::COL_BYTES);
+    static constexpr int ROWS_BYTES = COLS_N * (MODE == R2_EXACT ? 8 : epi::COLR_BYTES);
     static constexpr int OFF_ITEMS = OFF_ROWS + ROWS_BYTES;
     static constexpr int OFF_BAR = OFF_ITEMS + QSLOTS * 16;
     static constexpr int NBARS = 2 * PST + 2 * UST + 2 + 2 + 1 + 2 * QSLOTS;
@@ -139,7 +139,7 @@ k_ld_batch(const BatchParams bp) {
     uint64_t *ifull = mma_done + 1, *iempty = ifull + QSLOTS;
     Item *items = reinterpret_cast<Item *>(smem + L::OFF_ITEMS);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L::OFF_TMEM);
-    const epi::Cols cols(smem + L::OFF_ROWS, COLS_N);
+    const epi::ColsR colsr(smem + L::OFF_ROWS, COLS_N);   // R2_REFERENCE factors
     const epi::ColsF colsf(smem + L::OFF_ROWS, COLS_N);   // R2_EXACT: FP32 factors
 
     const uint32_t rank = cluster_rank();
@@ -374,7 +374,7 @@ k_ld_batch(const BatchParams bp) {
                 if constexpr (MODE == R2_EXACT)
                     epi::store_col_f32(colsf, et, cb, J.S);
                 else
-                    epi::store_col<MODE>(cols, et, cb, J.S);
+                    epi::store_col_ref(colsr, et, cb, J.S);
             }
             named_bar_sync(1, EPI_THREADS);
             bool ready = mbar_wait(smem_u32(&accfull[ab]), (qi >> 1) & 1, limit, bp.status);
@@ -390,7 +390,7 @@ k_ld_batch(const BatchParams bp) {
                 const int a = it.ta * BM + (int)rank * HM + q * 32 + lane;
                 const bool a_ok = a < J.m;
                 const uint32_t ca = a_ok ? J.bcA[a] : 0u;
-                const epi::ARow ra = epi::make_arow<MODE>(ca, J.S);
+                const epi::ARowR ra = epi::make_arow_ref(ca, J.S);
                 const epi::ARowF raf = epi::make_arow_f32(ca, J.S);
                 const uint32_t tbase =
                     tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)ab * ACC_STRIDE;
@@ -412,7 +412,7 @@ k_ld_batch(const BatchParams bp) {
                                      J.threshold);
                     } else {
                         // the F32 accumulators hold the counts as floats
-                        epi::chunk_ref<0, true>(v, ra, cols, c * 32, it.tb * BN + c * 32, a, a_ok,
+                        epi::chunk_ref<0, true>(v, ra, colsr, c * 32, it.tb * BN + c * 32, a, a_ok,
                                             n_tile, dlo, dhi, J.r2, J.ldr, J.counts, J.ldc, 0,
                                             J.S);
                     }

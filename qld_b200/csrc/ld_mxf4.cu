@@ -67,7 +67,7 @@ constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
 constexpr int OFF_PA = OFF_UB + UST * UB_BYTES;
 constexpr int OFF_PB = OFF_PA + PST * PA_BYTES;
 constexpr int OFF_ROWS = OFF_PB + PST * PB_BYTES;
-constexpr int ROWS_BYTES = COLS_N * epi::COL_BYTES;
+constexpr int ROWS_BYTES = COLS_N * epi::COLR_BYTES;   // R2_EXACT uses 8 of the 16
 constexpr int OFF_BAR = OFF_ROWS + ROWS_BYTES;
 constexpr int NBARS = 2 * PST + 2 * UST + 2 + 1;
 constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
@@ -128,7 +128,7 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
     uint64_t *accempty = accfull + 1;
     uint64_t *mma_done = accempty + 1;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + OFF_TMEM);
-    const epi::Cols cols(smem + OFF_ROWS, COLS_N);
+    const epi::ColsR colsr(smem + OFF_ROWS, COLS_N);   // R2_REFERENCE factors
     const epi::ColsF colsf(smem + OFF_ROWS, COLS_N);   // R2_EXACT: FP32 factors
 
     if (grid_failed(p.status)) return;
@@ -318,7 +318,7 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
                 if constexpr (MODE == R2_EXACT)
                     epi::store_col_f32(colsf, wt, cb, p.S);
                 else
-                    epi::store_col<MODE>(cols, wt, cb, p.S);
+                    epi::store_col_ref(colsr, wt, cb, p.S);
             }
             named_bar_sync(1, WORKERS);
             bool ready = ok && !failed && mbar_wait(smem_u32(accfull), it & 1, p.timeout_cycles,
@@ -334,7 +334,7 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
                 const int a = ta * BM + acc_i * HM + q * 32 + lane;
                 const bool a_ok = a < p.m;
                 const uint32_t ca = a_ok ? p.bcA[a] : 0u;
-                const epi::ARow ra = epi::make_arow<MODE>(ca, p.S);
+                const epi::ARowR ra = epi::make_arow_ref(ca, p.S);
                 const epi::ARowF raf = epi::make_arow_f32(ca, p.S);
                 const uint32_t tbase =
                     tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)acc_i * ACC1;
@@ -351,7 +351,7 @@ k_ld_mxf4(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUten
                                        dlo, dhi, p.r2, p.ldr, p.counts, p.ldc, p.out_row0, p.S);
                     } else {
                         // the F32 accumulators hold the counts as floats
-                        epi::chunk_ref<0, true>(v, ra, cols, c * 32, tb * BN + c * 32, a, a_ok,
+                        epi::chunk_ref<0, true>(v, ra, colsr, c * 32, tb * BN + c * 32, a, a_ok,
                                             n_tile, dlo, dhi, p.r2, p.ldr, p.counts, p.ldc,
                                             p.out_row0, p.S);
                     }

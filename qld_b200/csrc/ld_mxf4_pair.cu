@@ -74,18 +74,18 @@ constexpr int COLS_N = 256;              // epilogue column factors (BN used)
 constexpr uint16_t BOTH = 0x3;           // CTA mask of a commit to both ranks
 
 // Shared-memory layout per r^2 mode.  R2_EXACT needs 8 bytes of column
-// factors per column (epi::ColsF), R2_REFERENCE 24 (epi::Cols); the room
-// this saves holds a sixth packed stage (more TMA lookahead: 2.576 -> 2.562
+// factors per column (epi::ColsF), R2_REFERENCE 16 (epi::ColsR); both leave
+// room for six packed stages (more TMA lookahead than five: 2.576 -> 2.562
 // ms on the single region).
 template <int MODE>
 struct Smem {
-    static constexpr int PST = MODE == R2_EXACT ? 6 : 5;   // packed stages in flight
+    static constexpr int PST = 6;                          // packed stages in flight
     static constexpr int OFF_UA = 0;
     static constexpr int OFF_UB = OFF_UA + UST * UA_BYTES;
     static constexpr int OFF_PA = OFF_UB + UST * UB_BYTES;
     static constexpr int OFF_PB = OFF_PA + PST * PA_BYTES;
     static constexpr int OFF_ROWS = OFF_PB + PST * PB_BYTES;
-    static constexpr int ROWS_BYTES = COLS_N * (MODE == R2_EXACT ? 8 : epi::COL_BYTES);
+    static constexpr int ROWS_BYTES = COLS_N * (MODE == R2_EXACT ? 8 : epi::COLR_BYTES);
     static constexpr int OFF_BAR = OFF_ROWS + ROWS_BYTES;
     static constexpr int NBARS = 2 * PST + 2 * UST + 2 + 2 + 1;
     static constexpr int OFF_TMEM = OFF_BAR + NBARS * 8;
@@ -115,7 +115,7 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     uint64_t *accempty = accfull + 2;
     uint64_t *mma_done = accempty + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + L::OFF_TMEM);
-    const epi::Cols cols(smem + L::OFF_ROWS, COLS_N);
+    const epi::ColsR colsr(smem + L::OFF_ROWS, COLS_N);   // R2_REFERENCE factors
     const epi::ColsF colsf(smem + L::OFF_ROWS, COLS_N);   // R2_EXACT: FP32 factors
 
     const uint32_t rank = cluster_rank();
@@ -285,7 +285,7 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 if constexpr (MODE == R2_EXACT)
                     epi::store_col_f32(colsf, et, cb, p.S);
                 else
-                    epi::store_col<MODE>(cols, et, cb, p.S);
+                    epi::store_col_ref(colsr, et, cb, p.S);
             }
             named_bar_sync(1, EPILOGUE);
             bool ready = !failed && mbar_wait(smem_u32(&accfull[ab]), (it >> 1) & 1,
@@ -301,7 +301,7 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 const int a = ta * BM + (int)rank * HM + q * 32 + lane;
                 const bool a_ok = a < p.m;
                 const uint32_t ca = a_ok ? p.bcA[a] : 0u;
-                const epi::ARow ra = epi::make_arow<MODE>(ca, p.S);
+                const epi::ARowR ra = epi::make_arow_ref(ca, p.S);
                 const epi::ARowF raf = epi::make_arow_f32(ca, p.S);
                 const uint32_t tbase =
                     tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)ab * ACC_STRIDE;
@@ -318,7 +318,7 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                                        dlo, dhi, p.r2, p.ldr, p.counts, p.ldc, p.out_row0, p.S);
                     } else {
                         // the F32 accumulators hold the counts as floats
-                        epi::chunk_ref<0, true>(v, ra, cols, c * 32, tb * BN + c * 32, a, a_ok,
+                        epi::chunk_ref<0, true>(v, ra, colsr, c * 32, tb * BN + c * 32, a, a_ok,
                                             n_tile, dlo, dhi, p.r2, p.ldr, p.counts, p.ldc,
                                             p.out_row0, p.S);
                     }

@@ -15,6 +15,9 @@
  * on device QLD_CUDA_DEVICE (default 0) and released by qld_cuda_thread_release().
  * r^2 mode: reference semantics (bit-identical results[], byte-identical
  * report) unless QLD_R2=exact selects the exact-D FP64-evaluated r^2.
+ * The pinned results[] buffer (correlate()'s m x n floats, gemm_cpu.c:467)
+ * is kept per thread and only grows, so an -inputList run pins host memory
+ * once instead of once per task (a 29,817-SNP region needs 3.6 GB).
  * Errors keep qLD-compute's behaviour: a message on stderr and exit(1).
  *
  * Single region: the symmetric (lower-triangle) computation is used only when
@@ -32,6 +35,8 @@
 #include "read_file.h"
 
 static __thread qld_ctx *tls_ctx = NULL;
+static __thread float *tls_results = NULL;   /* pinned, tls_cap floats */
+static __thread size_t tls_cap = 0;
 
 static void cuda_fail(const char *what, int rc)
 {
@@ -57,9 +62,29 @@ static qld_ctx *thread_ctx(void)
     return tls_ctx;
 }
 
+/* The thread's pinned results[] buffer, grown to at least `cells` floats. */
+static float *thread_results(qld_ctx *ctx, size_t cells)
+{
+    if (cells > tls_cap) {
+        if (tls_results)
+            qld_cuda_host_free(ctx, tls_results);
+        tls_results = NULL;
+        tls_cap = 0;
+        int rc = qld_cuda_host_alloc(ctx, cells * sizeof(float), (void **)&tls_results);
+        if (rc != QLD_OK)
+            cuda_fail("qld_cuda_host_alloc", rc);
+        tls_cap = cells;
+    }
+    return tls_results;
+}
+
 void qld_cuda_thread_release(void)
 {
     if (tls_ctx) {
+        if (tls_results)
+            qld_cuda_host_free(tls_ctx, tls_results);
+        tls_results = NULL;
+        tls_cap = 0;
         qld_cuda_release(tls_ctx);
         tls_ctx = NULL;
     }
@@ -86,15 +111,12 @@ void correlate_cuda(threadData_t *threadData,
     int m = tableAsize, n = tableBsize;
     int symmetric = (posWset2 == 0 && tableA == tableB && m == n);
     size_t cells = (size_t)m * (size_t)n;
-    float *results = NULL;
-    int rc = qld_cuda_host_alloc(ctx, (cells ? cells : 1) * sizeof(float), (void **)&results);
-    if (rc != QLD_OK)
-        cuda_fail("qld_cuda_host_alloc", rc);
+    float *results = thread_results(ctx, cells ? cells : 1);
 
     writeResultsHeader(fpOut);
     double t1 = gettime();
-    rc = qld_cuda_ld(ctx, tableA, tableA_bitcount, m, tableB, tableB_bitcount, n,
-                     compressed_snp_size, snp_size, symmetric, results, NULL);
+    int rc = qld_cuda_ld(ctx, tableA, tableA_bitcount, m, tableB, tableB_bitcount, n,
+                         compressed_snp_size, snp_size, symmetric, results, NULL);
     if (rc != QLD_OK)
         cuda_fail("qld_cuda_ld", rc);
     double t2 = gettime();
@@ -103,7 +125,6 @@ void correlate_cuda(threadData_t *threadData,
                  tableB_posIndex, tableB_IDindex, tableB_bitcount, n, snp_size,
                  results, threadData[0].r2limit, posWset2);
     double t3 = gettime();
-    qld_cuda_host_free(ctx, results);
 
 #if defined(VERBOSE) || defined(BENCHMARK)
     threadData[0].threadStats.init_time += t1 - t0;

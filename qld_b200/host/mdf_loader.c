@@ -75,42 +75,56 @@ static int dir_path(const char *dir, const char *name, char *out, size_t cap)
            (int)cap;
 }
 
+/* The dataset's header file: the lexically first regular file whose name
+ * contains "header" (qLD's readHeaderFile() takes the one readdir() finds). */
+static int header_file(const char *dir, char *name, size_t name_cap, char *path,
+                       size_t path_cap)
+{
+    DIR *dp = opendir(dir);
+    if (!dp)
+        return qld_host_fail(QLD_ERR_INVALID, "cannot open directory %s", dir);
+    name[0] = '\0';
+    struct dirent *e;
+    while ((e = readdir(dp))) {
+        char p[4096];
+        struct stat st;
+        if (!strstr(e->d_name, "header") || !dir_path(dir, e->d_name, p, sizeof p) ||
+            stat(p, &st) || !S_ISREG(st.st_mode))
+            continue;
+        if (!name[0] || strcmp(e->d_name, name) < 0)
+            snprintf(name, name_cap, "%s", e->d_name);
+    }
+    closedir(dp);
+    if (!name[0])
+        return qld_host_fail(QLD_ERR_INVALID, "no header file in %s", dir);
+    dir_path(dir, name, path, path_cap);
+    return QLD_OK;
+}
+
+static const char *const kVcfFields[9] = {"#CHROM", "POS", "ID", "REF", "ALT",
+                                          "QUAL", "FILTER", "INFO", "FORMAT"};
+
 int qld_mdf_read_header(const char *dir, qld_mdf_header *h)
 {
     if (!dir || !h)
         return qld_host_fail(QLD_ERR_INVALID, "NULL argument");
     memset(h, 0, sizeof *h);
-    DIR *dp = opendir(dir);
-    if (!dp)
-        return qld_host_fail(QLD_ERR_INVALID, "cannot open directory %s", dir);
-    char best[1024] = "";
-    struct dirent *e;
-    while ((e = readdir(dp))) {
-        char path[4096];
-        struct stat st;
-        if (!strstr(e->d_name, "header") || !dir_path(dir, e->d_name, path, sizeof path) ||
-            stat(path, &st) || !S_ISREG(st.st_mode))
-            continue;
-        if (!best[0] || strcmp(e->d_name, best) < 0)
-            snprintf(best, sizeof best, "%s", e->d_name);
-    }
-    closedir(dp);
-    if (!best[0])
-        return qld_host_fail(QLD_ERR_INVALID, "no header file in %s", dir);
+    char best[1024], path[4096];
+    int rc = header_file(dir, best, sizeof best, path, sizeof path);
+    if (rc)
+        return rc;
     /* alignment id: the name up to the first '_' (or quote), as sscanf("%[^'_']") */
     size_t k = strcspn(best, "_'");
     if (k == 0 || k >= sizeof h->id)
         return qld_host_fail(QLD_ERR_INVALID, "bad header file name %s", best);
     memcpy(h->id, best, k);
     h->id[k] = '\0';
-    char path[4096];
-    dir_path(dir, best, path, sizeof path);
     gzFile f = gzopen(path, "r");
     if (!f)
         return qld_host_fail(QLD_ERR_INVALID, "cannot open %s", path);
     char *buf = NULL;
     size_t cap = 0;
-    int rc = qld_host_fail(QLD_ERR_INVALID, "%s: no #CHROM line", path);
+    rc = qld_host_fail(QLD_ERR_INVALID, "%s: no #CHROM line", path);
     if (!gz_line(f, &buf, &cap)) {
         rc = qld_host_fail(QLD_ERR_INVALID, "%s: empty header", path);
         goto out;
@@ -118,14 +132,12 @@ int qld_mdf_read_header(const char *dir, qld_mdf_header *h)
     while (gz_line(f, &buf, &cap)) {
         if (strncmp(buf, "#CHROM", 6) != 0)
             continue;
-        static const char *fields[9] = {"#CHROM", "POS", "ID", "REF", "ALT",
-                                        "QUAL", "FILTER", "INFO", "FORMAT"};
         int nf = 0;
         for (char *save = NULL, *t = strtok_r(buf, " \t", &save); t;
              t = strtok_r(NULL, " \t", &save), ++nf)
-            if (nf < 9 && strcmp(t, fields[nf]) != 0) {
+            if (nf < 9 && strcmp(t, kVcfFields[nf]) != 0) {
                 rc = qld_host_fail(QLD_ERR_INVALID, "%s: VCF header field %s missing", path,
-                                   fields[nf]);
+                                   kVcfFields[nf]);
                 goto out;
             }
         h->samples = nf - 9;
@@ -144,6 +156,45 @@ int qld_mdf_read_header(const char *dir, qld_mdf_header *h)
         break;
     }
 out:
+    free(buf);
+    gzclose(f);
+    return rc;
+}
+
+int qld_mdf_listed_samples(const char *dir, const char *const *names, int nnames, int *listed)
+{
+    if (!dir || !listed || nnames < 0 || (nnames > 0 && !names))
+        return qld_host_fail(QLD_ERR_INVALID, "bad argument");
+    *listed = 0;
+    char best[1024], path[4096];
+    int rc = header_file(dir, best, sizeof best, path, sizeof path);
+    if (rc)
+        return rc;
+    gzFile f = gzopen(path, "r");
+    if (!f)
+        return qld_host_fail(QLD_ERR_INVALID, "cannot open %s", path);
+    char *buf = NULL;
+    size_t cap = 0;
+    rc = qld_host_fail(QLD_ERR_INVALID, "%s: no #CHROM line", path);
+    while (gz_line(f, &buf, &cap)) {
+        if (strncmp(buf, "#CHROM", 6) != 0)
+            continue;
+        /* makeValidList(): the words after the nine fixed VCF fields; a name
+         * counts if it equals an entry of the list (sample_isValid()) */
+        int nf = 0, count = 0;
+        for (char *save = NULL, *t = strtok_r(buf, " \t\r\n", &save); t;
+             t = strtok_r(NULL, " \t\r\n", &save), ++nf) {
+            if (nf < 9)
+                continue;
+            int hit = nnames == 0;
+            for (int i = 0; i < nnames && !hit; ++i)
+                hit = strcmp(names[i], t) == 0;
+            count += hit;
+        }
+        *listed = count;
+        rc = QLD_OK;
+        break;
+    }
     free(buf);
     gzclose(f);
     return rc;

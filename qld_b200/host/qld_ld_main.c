@@ -14,9 +14,21 @@
  * report of qLD-compute's -DCOUNTSTATES build, correlate_IO.c:430-516,
  * instead of r^2) and -timing (per-task phase times as JSON on stderr).
  * -competing, -sorted, -rTable and -gpu are accepted and change nothing
- * (scheduling switches); -sampleList is not supported; -seed is rejected as
- * qLD-compute rejects it (its parser falls through to the invalid-parameter
- * error, correlate_our_kernel.c:387-392,434-436).
+ * (scheduling switches); -seed is rejected as qLD-compute rejects it (its
+ * parser falls through to the invalid-parameter error,
+ * correlate_our_kernel.c:387-392,434-436).
+ * -sampleList FILE / -sampleList2 FILE (correlate_our_kernel.c:260-289):
+ * whitespace-separated sample names (getFilter, correlate_IO.c:35-58).  With
+ * MDF input qLD-compute uses a list only to size the rows: K =
+ * ceil(listed names on the #CHROM line x ploidy / 64) words
+ * (correlate_function.c:112-122), of which writeMDF_x64() keeps the first K
+ * words of every row (the words of the first samples, not the listed ones:
+ * MDF rows are already packed), with the file's BC and the header's
+ * snipSize as S.  qld-ld does the same, so its reports stay byte-identical.
+ * Table B takes K from -sampleList2 when it comes from -input2 (and K from
+ * -sampleList when it is a second window of -input, as qLD-compute reads it
+ * with table A's compSize); a K of table B that differs from table A's is
+ * refused, where qLD-compute would read table A with table B's stride.
  * Window resolution is preprocess_data()'s (load_balancer.c:122-345), the
  * single-region / two-table choice and the "input2 equals input" rule are
  * correlate_function()'s (correlate_function.c:94-104,239-295), and
@@ -51,6 +63,49 @@ typedef struct loaded {
     double load_s;
 } loaded;
 
+/* -sampleList / -sampleList2 names (no list: every sample counts). */
+static char **g_list[2];
+static int g_nlist[2];
+
+static int read_sample_list(const char *path, int which)
+{
+    FILE *f = fopen(path, "r");
+    if (!f) {
+        fprintf(stderr, "ERROR: cannot open sample list %s\n", path);
+        return 1;
+    }
+    char word[4096];
+    int cap = 0;
+    while (fscanf(f, "%4095s", word) == 1) {
+        if (g_nlist[which] == cap) {
+            cap = cap ? 2 * cap : 64;
+            char **nl = realloc(g_list[which], sizeof *nl * (size_t)cap);
+            if (!nl) {
+                fclose(f);
+                return 1;
+            }
+            g_list[which] = nl;
+        }
+        g_list[which][g_nlist[which]++] = strdup(word);
+    }
+    fclose(f);
+    return 0;
+}
+
+/* Words per row for a dataset: ceil(valid samples / 64), the valid count
+ * being the header's names that the list holds, times the ploidy. */
+static int words_for(const char *dir, int which, int ploidy, int *K)
+{
+    int listed = 0;
+    int rc = qld_mdf_listed_samples(dir, (const char *const *)g_list[which], g_nlist[which],
+                                    &listed);
+    if (rc)
+        return rc;
+    const long valid = (long)listed * ploidy;
+    *K = (int)((valid + 63) / 64);
+    return QLD_OK;
+}
+
 static double now_s(void)
 {
     struct timespec t;
@@ -64,6 +119,7 @@ static void usage(FILE *f)
           "unphased_diploid -mdf\n"
           "              [-posWmin1 P -posWmax1 P -posWmin2 P -posWmax2 P] [-inputList CSV]\n"
           "              [-r2limit R] [-threads T] [-device D] [-r2mode reference|exact]\n"
+          "              [-sampleList FILE] [-sampleList2 FILE]\n"
           "              [-filter gpu|host] [-countstates] [-timing]\n",
           f);
 }
@@ -169,13 +225,16 @@ static void *load_task(void *arg)
     /* correlate_function.c:94-104: the same directory twice is one input */
     if (t->in2set && strcmp(t->in1, t->in2) == 0)
         t->in2set = 0;
-    const long valid = (long)h1.samples * a->ploidy;
-    l->K = (int)((valid + 63) / 64);
+    if (words_for(t->in1, 0, a->ploidy, &l->K)) {
+        load_fail(l, QLD_ERR_INVALID, qld_host_last_error());
+        return NULL;
+    }
     l->S = h1.snip_size;
     l->single = !t->w2set && !t->in2set;
     l->tri = !t->w2set;
     if (l->K < 1) {
-        load_fail(l, QLD_ERR_INVALID, "no samples in the header");
+        load_fail(l, QLD_ERR_INVALID, g_nlist[0] ? "no sample of the list is in the header"
+                                                 : "no samples in the header");
         return NULL;
     }
     int rc = qld_mdf_load(a->ctx, t->in1, t->wmin1, t->wmax1, l->K, a->threads, &l->A);
@@ -189,7 +248,12 @@ static void *load_task(void *arg)
         l->B.K = l->K;
     } else if (rc == QLD_OK && !l->single) {
         /* table B: input2 with window 2, or input with window 2 */
-        const int K2 = t->in2set ? (int)(((long)h2.samples * a->ploidy + 63) / 64) : l->K;
+        int K2 = l->K;
+        if (t->in2set && words_for(t->in2, 1, a->ploidy, &K2)) {
+            load_fail(l, QLD_ERR_INVALID, qld_host_last_error());
+            qld_table_free(a->ctx, &l->A);
+            return NULL;
+        }
         if (K2 != l->K) {
             char m[256];
             snprintf(m, sizeof m, "the inputs' sample counts differ (%d vs %d words)", l->K, K2);
@@ -410,11 +474,6 @@ int main(int argc, char **argv)
         if (!strcmp(a, "-competing") || !strcmp(a, "-sorted") || !strcmp(a, "-rTable") ||
             !strcmp(a, "-gpu"))
             continue;
-        if (!strcmp(a, "-sampleList") || !strcmp(a, "-sampleList2")) {
-            fprintf(stderr, "ERROR: %s is not supported: qld-ld uses every sample of the header\n",
-                    a);
-            return 1;
-        }
         if (!v) {
             fprintf(stderr, "ERROR: %s needs a value\n", a);
             return 1;
@@ -429,6 +488,8 @@ int main(int argc, char **argv)
         else if (!strcmp(a, "-posWmin2")) { base.wmin2 = atoi(v); base.w2set = 1; }
         else if (!strcmp(a, "-posWmax2")) { base.wmax2 = atoi(v); base.w2set = 1; }
         else if (!strcmp(a, "-r2limit")) r2limit = (float)atof(v);
+        else if (!strcmp(a, "-sampleList")) { if (read_sample_list(v, 0)) return 1; }
+        else if (!strcmp(a, "-sampleList2")) { if (read_sample_list(v, 1)) return 1; }
         else if (!strcmp(a, "-threads")) threads = atoi(v);
         else if (!strcmp(a, "-device")) device = atoi(v);
         else if (!strcmp(a, "-ploidy")) {

@@ -74,6 +74,9 @@ def lib() -> ct.CDLL:
         L = ct.CDLL(LIB_PATH)
         L.qld_mdf_read_header.argtypes = [ct.c_char_p, ct.POINTER(_Header)]
         L.qld_mdf_read_header.restype = ct.c_int
+        L.qld_mdf_listed_samples.argtypes = [ct.c_char_p, ct.POINTER(ct.c_char_p), ct.c_int,
+                                             ct.POINTER(ct.c_int)]
+        L.qld_mdf_listed_samples.restype = ct.c_int
         L.qld_mdf_load.argtypes = [ct.c_void_p, ct.c_char_p, ct.c_int, ct.c_int, ct.c_int, ct.c_int,
                                    ct.POINTER(_Table)]
         L.qld_mdf_load.restype = ct.c_int
@@ -109,6 +112,17 @@ def read_header(path: str) -> Header:
     _check(lib().qld_mdf_read_header(os.fsencode(path), ct.byref(h)))
     return Header(h.id.decode(), h.snips_per_file, h.snip_size, h.total_snips, h.pos_min,
                   h.pos_max, h.samples)
+
+
+def listed_samples(path: str, names=None) -> int:
+    """Sample names of the dataset's #CHROM line that `names` holds (all of
+    them for None): the count qLD-compute's -sampleList gives
+    (qld_mdf_listed_samples)."""
+    names = list(names or [])
+    arr = (ct.c_char_p * max(1, len(names)))(*[n.encode() for n in names])
+    out = ct.c_int()
+    _check(lib().qld_mdf_listed_samples(os.fsencode(path), arr, len(names), ct.byref(out)))
+    return out.value
 
 
 def load_mdf(path: str, pos_min: int, pos_max: int, K: int, threads: int = 1,

@@ -169,3 +169,31 @@ def test_exact_mode_against_oracle(dataset, tmp_path):
     # the report truncates to 9 decimals: 1e-9 absolute on top of 1e-6 relative
     g, w = got[sel], want[sel]
     assert np.all(np.abs(g - w) <= 1e-6 * w + 1.1e-9)
+
+
+def test_sample_lists(dataset):
+    """-sampleList / -sampleList2 with MDF input: qLD-compute sizes the rows
+    from the listed names (K = ceil(listed x ploidy / 64)) and keeps each
+    row's first K words; qld-ld writes the same bytes.  One region, two
+    windows, and two inputs whose lists give the same K."""
+    tmp, d1, d2, _, _ = dataset
+    l1 = os.path.join(tmp, "samples1.txt")
+    l2 = os.path.join(tmp, "samples2.txt")
+    with open(l1, "w") as f:                      # 1,300 of 2,500 names: K 40 -> 21
+        f.write("\n".join(f"s{i}" for i in range(1, 2501, 2)))
+        f.write("\n" + " ".join(f"s{i}" for i in range(2, 102, 2)) + "\nnot_a_sample\n")
+    with open(l2, "w") as f:                      # 1,290 names: K 21 as well
+        f.write("\n".join(f"s{i}" for i in range(1211, 2501)) + "\n")
+    cases = {
+        "sl_single": ["-input", d1, "-sampleList", l1, "-r2limit", "0"],
+        "sl_windows": ["-input", d1, "-sampleList", l1, "-sampleList2", l2,
+                       "-posWmin1", "1000", "-posWmax1", "4000", "-posWmin2", "3000",
+                       "-posWmax2", "9000", "-r2limit", "0.01"],
+        "sl_inputs": ["-input", d1, "-input2", d2, "-sampleList", l1, "-sampleList2", l2,
+                      "-posWmin1", "1000", "-posWmax1", "9990", "-posWmin2", "100000",
+                      "-posWmax2", "104193", "-r2limit", "0.005"],
+    }
+    for name, args in cases.items():
+        ref, qld = _reports(tmp, name, [*args, "-ploidy", "haploid", "-mdf"])
+        assert ref and ref == qld, name
+        assert ref["out.txt"].count(b"\n") > 10, name

@@ -215,3 +215,23 @@ def test_cli_argument_errors(dataset, tmp_path):
     assert r.returncode == 1 and "not a valid" in r.stderr
     r = _cli("-help")
     assert r.returncode == 0 and "usage" in r.stdout
+
+
+def test_listed_samples(dataset, tmp_path):
+    """-sampleList's valid count: the #CHROM names the list holds (every name
+    without a list); unknown and repeated list entries count once or not at
+    all (sample_isValid, correlate_IO.c:60-76)."""
+    path, _, _ = dataset
+    assert host_api.listed_samples(path) == 300
+    assert host_api.listed_samples(path, ["s1", "s2", "s300", "s2", "nobody"]) == 3
+    assert host_api.listed_samples(path, [f"s{i}" for i in range(1, 301, 2)]) == 150
+    assert host_api.listed_samples(path, ["nobody"]) == 0
+
+
+def test_cli_sample_list_errors(dataset, tmp_path):
+    path, _, _ = dataset
+    if not os.path.exists(host_api.CLI_PATH):
+        pytest.skip("qld-ld not built")
+    r = _cli("-input", path, "-output", str(tmp_path / "o.txt"), "-ploidy", "haploid", "-mdf",
+             "-sampleList", str(tmp_path / "missing.txt"))
+    assert r.returncode == 1 and "sample list" in r.stderr
