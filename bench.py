@@ -65,7 +65,8 @@ def parse(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="single_region",
-                    choices=["single_region", "all_pairs", "batched", "windowed", "served"])
+                    choices=["single_region", "all_pairs", "batched", "windowed", "served",
+                             "dropin"])
     ap.add_argument("--sections", default=",".join(SECTIONS),
                     help="sub-objects of the headline line (comma list, or 'none')")
     ap.add_argument("--no-parity", action="store_true",
@@ -1118,18 +1119,104 @@ def section_served(args, local_rank, flush=None, check_queries=12):
     return out
 
 
+def section_dropin(args, local_rank, flush=None, windows=8):
+    """Drop-in arm: qLD-compute's own CLI on an MDF dataset of the headline
+    region's shape (29,817 SNPs x 16,622 haplotypes, K = 260), three ways --
+    the stock build with -blis (oracle/_ref/qLD-compute-blis: BLIS dsyrk /
+    dgemm on BLIS_IC_NT = physical cores, single-threaded epilogue), the same
+    CLI with correlate() routed to the GPU (oracle/_ref/qLD-compute-cuda,
+    QLD_CUDA=1: correlate_cuda()), and qld-ld (this package's native CLI,
+    GPU report filter) -- on one single-region task and on an -inputList of
+    window pairs (`windows` equal windows, every pair i < j: two-region
+    tasks).  Each figure is one process's wall time from start to exit:
+    MDF parse, counts + r^2, and the report at -r2limit 2 (which prints no
+    pair, so the text writer's cost is its scan alone)."""
+    import shutil
+    import numpy as np
+    import torch
+
+    from qld_b200 import host_api, mdf, synth
+    ref_blis = os.path.join(ROOT, "oracle", "_ref", "qLD-compute-blis")
+    ref_cuda = os.path.join(ROOT, "oracle", "_ref", "qLD-compute-cuda")
+    if not (os.path.exists(ref_blis) and os.path.exists(ref_cuda)):
+        return {"unavailable": "oracle/_ref/qLD-compute-blis or qLD-compute-cuda not built"}
+    dev = torch.device("cuda", local_rank)
+    T, S = synth.single_region_workload(device=dev, seed=2)
+    T_np = T.cpu().numpy().view(np.uint64)
+    m = T_np.shape[0]
+    tmp = tempfile.mkdtemp(prefix="qld_dropin_")
+    _, phys, _ = host_cpu()
+    try:
+        d = mdf.write_dataset(os.path.join(tmp, "region"), T_np, S, snps_per_file=1000)
+        pos = 1000 + 10 * np.arange(m)
+        edges = np.linspace(0, m, windows + 1).astype(int)
+        lst = os.path.join(tmp, "tasks.csv")
+        pairs_list = 0
+        with open(lst, "w") as f:
+            for i in range(windows):
+                for j in range(i + 1, windows):
+                    f.write(f"{d},{pos[edges[i]]},{pos[edges[i + 1] - 1]},"
+                            f"{d},{pos[edges[j]]},{pos[edges[j + 1] - 1]}\n")
+                    pairs_list += int(edges[i + 1] - edges[i]) * int(edges[j + 1] - edges[j])
+        env = dict(os.environ, BLIS_JC_NT="1", BLIS_IC_NT=str(phys), BLIS_JR_NT="1",
+                   BLIS_IR_NT="1", OMP_NUM_THREADS=str(phys))
+        env.pop("QLD_CUDA", None)
+        runs = {"reference_blis": (ref_blis, ["-blis"], env),
+                "reference_cli_cuda": (ref_cuda, [], dict(env, QLD_CUDA="1")),
+                "qld_ld": (host_api.CLI_PATH, ["-threads", str(phys)], env)}
+        common = ["-ploidy", "haploid", "-mdf", "-r2limit", "2"]
+        res = {"config": {"workload": "dropin_cli_29817x16622", "snps": m, "haplotypes": S,
+                          "words_per_snp": T_np.shape[1], "tasks_list": windows * (windows - 1) // 2,
+                          "pairs_single": m * (m - 1) // 2, "pairs_list": pairs_list,
+                          "r2limit": 2, "host_cores": phys},
+               "timing": "process wall clock, start to exit"}
+        outs = {}
+        for name, (exe, extra, e) in runs.items():
+            row = {}
+            for task, targs in (("single", ["-input", d]), ("list", ["-inputList", lst])):
+                wd = os.path.join(tmp, f"{name}_{task}")
+                os.makedirs(wd)
+                t0 = time.perf_counter()
+                r = subprocess.run([exe, *targs, *common, *extra, "-output",
+                                    os.path.join(wd, "out.txt")], cwd=wd, env=e,
+                                   capture_output=True, text=True, timeout=1800)
+                dt = time.perf_counter() - t0
+                if r.returncode != 0:
+                    row[task] = {"failed": r.returncode, "stderr": r.stderr[-300:]}
+                    continue
+                pairs = m * (m - 1) // 2 if task == "single" else pairs_list
+                row[task] = {"wall_s": dt, "pairs_per_s": pairs / dt}
+                outs[(name, task)] = {f: open(os.path.join(wd, f), "rb").read()
+                                      for f in sorted(os.listdir(wd)) if f.startswith("out")}
+            res[name] = row
+        res["reports_identical"] = all(
+            outs.get(("reference_blis", t)) == outs.get((n, t))
+            for n in ("reference_cli_cuda", "qld_ld") for t in ("single", "list"))
+        for task in ("single", "list"):
+            try:
+                res[f"speedup_cli_cuda_{task}"] = (res["reference_blis"][task]["wall_s"] /
+                                                   res["reference_cli_cuda"][task]["wall_s"])
+                res[f"speedup_qld_ld_{task}"] = (res["reference_blis"][task]["wall_s"] /
+                                                 res["qld_ld"][task]["wall_s"])
+            except KeyError:
+                pass
+        return res
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def standalone(args, rank, world, local_rank):
-    """--workload windowed|batched|served: that section alone, as its own
-    line."""
+    """--workload windowed|batched|served|dropin: that section alone, as its
+    own line."""
     import torch
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
     fn = {"windowed": section_windowed, "batched": section_batched,
-          "served": section_served}[args.workload]
+          "served": section_served, "dropin": section_dropin}[args.workload]
     res = fn(args, local_rank, flush)
     suffix = {"windowed": ", windowed band", "batched": ", batched tasks",
-              "served": ", served queries"}[args.workload]
+              "served": ", served queries", "dropin": ", qLD-compute CLI drop-in"}[args.workload]
     line = {"metric": METRIC + suffix, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64 popcount / f32 r2", "data": "synthetic", **res}

@@ -235,8 +235,12 @@ int qld_cuda_ld_band_device(qld_ctx *ctx, const uint64_t *A, const uint32_t *bcA
  * a work item taken from a device work queue by the SMs as they free up.
  * Same per-task contract as qld_cuda_ld_device(); asynchronous on `stream`,
  * collect with qld_cuda_sync().  The tasks of one call must not overlap in
- * their outputs.  A task needs K * 64 <= 2^24 samples (the 4-bit tensor-core
- * path's exact range), else QLD_ERR_UNSUPPORTED.  qLD runs such task
+ * their outputs.  Each task gets the kernel qld_cuda_ld_device() would give
+ * it (QLD_OPT_KERNEL, else the autotuner's entry for its shape class, else
+ * the 4-bit kernel while K * 64 <= 2^24 and the popcount kernel past it):
+ * the 4-bit tasks share the persistent launch, the others follow it on the
+ * same stream as their own launches.  A forced kernel that is not exact for
+ * a task returns QLD_ERR_UNSUPPORTED before anything runs.  qLD runs such task
  * lists one task at a time (-inputList: src/correlator/src/input_list.c:205-323,
  * correlate_function.c:59-83); this is their batched replacement.
  */

@@ -1152,13 +1152,21 @@ int qld_cuda_ld_band(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m, 
     return finish(c, c->stream);
 }
 
+// Per-job kernel choice: a job goes into the persistent launch when its
+// kernel (variant_of: the context's forced kernel, else the autotuner's entry
+// for its shape class, else the built-in rule) is the 4-bit one, and runs as
+// its own launch of the chosen kernel after it otherwise (the popcount
+// kernel past 2^24 samples, or a class the tuner found faster elsewhere).
 int qld_cuda_ld_batch(qld_ctx *c, const qld_ld_args *jobs, int njobs, void *stream) {
     if (!c || (njobs > 0 && !jobs) || njobs < 0) return QLD_ERR_INVALID;
     if (njobs == 0) return QLD_OK;
     CUDA_TRY(c, cudaSetDevice(c->device));
     const KernelShape &ks = kBatchShape;
     std::vector<long long> tiles(njobs), cost(njobs);
-    std::vector<int> order(njobs);
+    std::vector<int> order;
+    std::vector<Task> routed;
+    std::vector<int> routed_job;
+    order.reserve(njobs);
     for (int j = 0; j < njobs; ++j) {
         qld_ld_args a = jobs[j];
         if (a.symmetric) { a.B = a.A; a.bcB = a.bcA; a.n = a.m; a.ldb = a.lda; }
@@ -1166,21 +1174,30 @@ int qld_cuda_ld_batch(qld_ctx *c, const qld_ld_args *jobs, int njobs, void *stre
             (a.lda & 1) || (a.ldb & 1) || a.ldr < a.m || (a.counts && a.ldc < a.m) || !a.A ||
             !a.B || !a.bcA || !a.bcB || !a.r2 || !aligned16(a.A) || !aligned16(a.B))
             return set_err(c, QLD_ERR_INVALID, "batch job %d: bad sizes, strides or pointers", j);
-        if ((long long)a.K * 64 > kBatchMaxSamples)
-            return set_err(c, QLD_ERR_UNSUPPORTED,
-                           "batch job %d: K*64 > %d samples (use qld_cuda_ld_device)", j,
-                           kBatchMaxSamples);
         Task t{a.A, a.bcA, a.m, a.lda, a.B, a.bcB, a.n, a.ldb, a.K, a.S, a.symmetric, 0};
+        const int variant = variant_of(c, t);
+        if (!exact_for(variant, t))
+            return set_err(c, QLD_ERR_UNSUPPORTED,
+                           "batch job %d: the forced kernel is not exact for K*64 = %lld samples",
+                           j, (long long)a.K * 64);
         tiles[j] = (a.m == 0 || a.n == 0) ? 0 : tile_count(t, ks.bm, ks.bn, 0, a.n);
+        if (variant != QLD_KERNEL_FP4 || (long long)a.K * 64 > kBatchMaxSamples) {
+            if (tiles[j] > 0) {
+                routed.push_back(t);
+                routed_job.push_back(j);
+            }
+            continue;
+        }
         cost[j] = tiles[j] * (long long)a.K;
-        order[j] = j;
+        order.push_back(j);
     }
     // Most expensive tasks first, so the queue ends on small items.
     std::stable_sort(order.begin(), order.end(),
                      [&](int x, int y) { return cost[x] > cost[y]; });
-    c->hJobs.resize(njobs);
+    const int nb = (int)order.size();
+    c->hJobs.resize(nb > 0 ? nb : 1);
     long long items = 0;
-    for (int i = 0; i < njobs; ++i) {
+    for (int i = 0; i < nb; ++i) {
         const int j = order[i];
         qld_ld_args a = jobs[j];
         if (a.symmetric) { a.B = a.A; a.bcB = a.bcA; a.n = a.m; a.ldb = a.lda; }
@@ -1199,31 +1216,38 @@ int qld_cuda_ld_batch(qld_ctx *c, const qld_ld_args *jobs, int njobs, void *stre
         }
         items += tiles[j];
     }
-    if (items == 0) return QLD_OK;
-    int rc;
-    if ((rc = ensure(c, c->dJobs, sizeof(BatchJob) * (size_t)njobs)) ||
-        (rc = ensure(c, c->dQueue, sizeof(unsigned long long))))
-        return rc;
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
-    CUDA_TRY(c, cudaMemcpyAsync(c->dJobs.p, c->hJobs.data(), sizeof(BatchJob) * (size_t)njobs,
-                                cudaMemcpyHostToDevice, st));
-    CUDA_TRY(c, cudaMemsetAsync(c->dQueue.p, 0, sizeof(unsigned long long), st));
-    BatchParams bp{};
-    bp.jobs = static_cast<const BatchJob *>(c->dJobs.p);
-    bp.njobs = njobs;
-    bp.nitems = items;
-    bp.queue = static_cast<unsigned long long *>(c->dQueue.p);
-    bp.status = c->d_status;
-    bp.timeout_cycles = c->timeout_cycles;
-    cudaEvent_t e1 = nullptr;
-    if ((rc = prof_begin(c, st, &e1))) return rc;
-    cudaError_t e = launch_batch(bp, c->r2_mode, 0, st);
-    if (e != cudaSuccess)
-        return set_err(c, QLD_ERR_CUDA, "batched launch failed: %s", cudaGetErrorString(e));
-    if (e1) CUDA_TRY(c, cudaEventRecord(e1, st));
-    c->stats.counts_launches++;
-    c->stats.kernel_launches++;
-    c->stats.last_kernel = QLD_KERNEL_FP4;
+    int rc;
+    if (items > 0) {
+        if ((rc = ensure(c, c->dJobs, sizeof(BatchJob) * (size_t)nb)) ||
+            (rc = ensure(c, c->dQueue, sizeof(unsigned long long))))
+            return rc;
+        CUDA_TRY(c, cudaMemcpyAsync(c->dJobs.p, c->hJobs.data(), sizeof(BatchJob) * (size_t)nb,
+                                    cudaMemcpyHostToDevice, st));
+        CUDA_TRY(c, cudaMemsetAsync(c->dQueue.p, 0, sizeof(unsigned long long), st));
+        BatchParams bp{};
+        bp.jobs = static_cast<const BatchJob *>(c->dJobs.p);
+        bp.njobs = nb;
+        bp.nitems = items;
+        bp.queue = static_cast<unsigned long long *>(c->dQueue.p);
+        bp.status = c->d_status;
+        bp.timeout_cycles = c->timeout_cycles;
+        cudaEvent_t e1 = nullptr;
+        if ((rc = prof_begin(c, st, &e1))) return rc;
+        cudaError_t e = launch_batch(bp, c->r2_mode, 0, st);
+        if (e != cudaSuccess)
+            return set_err(c, QLD_ERR_CUDA, "batched launch failed: %s", cudaGetErrorString(e));
+        if (e1) CUDA_TRY(c, cudaEventRecord(e1, st));
+        c->stats.counts_launches++;
+        c->stats.kernel_launches++;
+        c->stats.last_kernel = QLD_KERNEL_FP4;
+    }
+    for (size_t i = 0; i < routed.size(); ++i) {
+        const qld_ld_args &a = jobs[routed_job[i]];
+        if ((rc = launch_counts(c, routed[i], 0, routed[i].n, a.r2, a.ldr, a.counts, a.ldc, 0,
+                                st)))
+            return rc;
+    }
     return QLD_OK;
 }
 

@@ -162,8 +162,87 @@ def test_batch_past_the_int8_limit(gpu_ctx):
         assert_r2_close(j["r2"].cpu().numpy(), oracle.r2_exact(bcA, bcB, want_c, N), mask=mask)
 
 
-def test_batch_rejects_past_2_24_samples(gpu_ctx):
-    """K * 64 > 2^24: the F32 accumulators would round; refused before launch."""
+def _device_job(A, B, N, sym, dev):
+    """One task's device buffers from host tables (rows padded to an even pitch)."""
+    K = A.shape[1]
+    lda = K + (K & 1)
+    m, n = A.shape[0], B.shape[0]
+    dA = torch.zeros(m, lda, dtype=torch.int64, device=dev)
+    dA[:, :K] = torch.from_numpy(np.ascontiguousarray(A).view(np.int64)).to(dev)
+    dB = dA
+    if not sym:
+        dB = torch.zeros(n, lda, dtype=torch.int64, device=dev)
+        dB[:, :K] = torch.from_numpy(np.ascontiguousarray(B).view(np.int64)).to(dev)
+    bcA, bcB = oracle.bitcounts(A), oracle.bitcounts(B)
+    return dict(A=dA, bcA=torch.from_numpy(bcA.view(np.int32).copy()).to(dev), m=m, lda=lda,
+                B=dB, bcB=torch.from_numpy(bcB.view(np.int32).copy()).to(dev), n=n, ldb=lda,
+                K=K, S=N, symmetric=sym,
+                r2=torch.full((n, m), -5.0, dtype=torch.float32, device=dev), ldr=m,
+                counts=torch.zeros((n, m), dtype=torch.int32, device=dev), ldc=m)
+
+
+def _check_job(j, A, B, N, sym):
+    n, m = j["n"], j["m"]
+    mask = lower_mask(n, m) if sym else np.ones((n, m), bool)
+    want_c = oracle.counts(A, B)
+    assert np.array_equal(j["counts"].cpu().numpy().view(np.uint32)[mask], want_c[mask])
+    assert_r2_close(j["r2"].cpu().numpy(), oracle.r2_exact(oracle.bitcounts(A),
+                                                           oracle.bitcounts(B), want_c, N),
+                    mask=mask)
+
+
+def test_batch_routes_past_2_24_samples_to_popcount(gpu_ctx):
+    """K * 64 > 2^24: the 4-bit path's F32 accumulators would round, so that
+    task runs on the popcount kernel after the persistent launch, beside 4-bit
+    tasks in the same call; every task matches the oracle."""
+    dev = torch.device("cuda", 0)
+    specs = [(40, (1 << 24) + 200, True, 90), (30, (1 << 24) + 64 * 7, False, 91),
+             (500, 3000, True, 92), (300, 7000, False, 93)]
+    jobs, host = [], []
+    for m, N, sym, seed in specs:
+        t, _ = synth.all_pairs_workload(m=m + (0 if sym else 25), n=N, seed=seed)
+        T = t.numpy().view(np.uint64)
+        A, B = T[:m], (T[:m] if sym else T[m:])
+        jobs.append(_device_job(A, B, N, sym, dev))
+        host.append((A, B, N, sym))
+    st = torch.cuda.current_stream()
+    gpu_ctx.stats(reset=True)
+    gpu_ctx.ld_batch(jobs, stream=st)
+    gpu_ctx.sync(stream=st)
+    stats = gpu_ctx.stats(reset=True)
+    assert stats.counts_launches >= 3          # the persistent launch + two popcount launches
+    for j, (A, B, N, sym) in zip(jobs, host):
+        _check_job(j, A, B, N, sym)
+
+
+def test_batch_follows_the_autotuner_per_job(tmp_path):
+    """A tuned class that prefers the popcount kernel takes its jobs out of the
+    persistent launch; the other jobs stay in it; results match the oracle."""
+    dev = torch.device("cuda", 0)
+    path = tmp_path / "tune.txt"
+    path.write_text("qld-tune 1\n9 9 5 1 1 0 0.9\n")   # 512-1023 SNPs, 32-63 words, single
+    jobs, host = [], []
+    for m, N, sym, seed in [(700, 2500, True, 94), (700, 2500, False, 95),
+                            (200, 2500, True, 96)]:
+        t, _ = synth.all_pairs_workload(m=m + (0 if sym else 100), n=N, seed=seed)
+        T = t.numpy().view(np.uint64)
+        A, B = T[:m], (T[:m] if sym else T[m:])
+        jobs.append(_device_job(A, B, N, sym, dev))
+        host.append((A, B, N, sym))
+    with api.Context(0) as ctx:                      # its own tuning table
+        ctx.tune_load(str(path))
+        st = torch.cuda.current_stream()
+        ctx.ld_batch(jobs, stream=st)
+        ctx.sync(stream=st)
+        stats = ctx.stats(reset=True)
+    assert stats.counts_launches == 2               # the persistent launch + one popcount launch
+    assert stats.last_kernel == api.KERNEL_POPC
+    for j, (A, B, N, sym) in zip(jobs, host):
+        _check_job(j, A, B, N, sym)
+
+
+def test_batch_rejects_a_forced_kernel_that_is_not_exact(gpu_ctx):
+    """A forced 4-bit kernel past 2^24 samples: refused before anything runs."""
     dev = torch.device("cuda", 0)
     K = (1 << 24) // 64 + 2
     A = torch.zeros(2, K, dtype=torch.int64, device=dev)
@@ -171,6 +250,10 @@ def test_batch_rejects_past_2_24_samples(gpu_ctx):
     r2 = torch.zeros(2, 2, dtype=torch.float32, device=dev)
     job = dict(A=A, bcA=bc, m=2, lda=K, B=A, bcB=bc, n=2, ldb=K, K=K, S=K * 64, symmetric=True,
                r2=r2, ldr=2, counts=None, ldc=2)
-    with pytest.raises(api.QldError) as e:
-        gpu_ctx.ld_batch([job])
+    gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_FP4)
+    try:
+        with pytest.raises(api.QldError) as e:
+            gpu_ctx.ld_batch([job])
+    finally:
+        gpu_ctx.set_option(api.OPT_KERNEL, api.KERNEL_AUTO)
     assert e.value.code == api.ERR_UNSUPPORTED
