@@ -253,10 +253,9 @@ def kernel_roofline(ctx, variant, bitops, kern_ms, dev, int8_context=True):
 def measured_traffic(variant, workload, sm_pair=0, r2_mode="exact"):
     """DRAM bytes per launch of the counts kernel from the ncu capture
     summarised under profiles/ (None when no capture covers this case).
-    sm_pair 0 is the automatic choice: SM pairs for exact r^2, single SMs
-    for reference r^2."""
+    sm_pair 0 is the automatic choice: SM pairs in both r^2 modes."""
     if sm_pair == 0:
-        sm_pair = 1 if r2_mode == "reference" else 2
+        sm_pair = 2
     names = {2: "k_ld_mma_wide_traffic_16384.md",
              3: "k_ld_mxf4_traffic_16384.md" if sm_pair == 1 else "k_ld_mxf4_pair_traffic_16384.md"}
     if variant not in names or workload != "single_region_29817x16622_lower_triangle":

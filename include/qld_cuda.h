@@ -78,9 +78,8 @@ extern "C" {
                                 rounded down to whole tile rows of the kernel */
 #define QLD_OPT_MMA_TILE  5  /* QLD_KERNEL_MMA output tile rows: 128, 256, 0 = per shape */
 #define QLD_OPT_SM_PAIR   6  /* QLD_KERNEL_FP4 SMs per output tile: 1, 2 (a cluster of two
-                                CTAs, tcgen05 cta_group::2), 0 = automatic (2 with
-                                QLD_R2_EXACT, 1 with QLD_R2_REFERENCE, whose FP64
-                                epilogue runs faster on the single-SM kernel's 16 warps) */
+                                CTAs, tcgen05 cta_group::2), 0 = automatic (the tuned
+                                choice for the task's class, else 2) */
 #define QLD_OPT_WAIT_CYCLES 7 /* budget of every bounded wait inside the kernels' pipelines,
                                 in SM clock cycles (0 = the default 4e9, ~2 s; the environment
                                 variable QLD_TIMEOUT_CYCLES sets the initial value).  A wait

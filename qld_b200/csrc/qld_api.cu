@@ -240,19 +240,16 @@ const KernelShape &mma_shape(qld_ctx *c, const Task &t, int b0, int b1) {
     return tile_count(t, 256, 256, b0, b1) >= 4LL * c->sm_count ? kMmaWideShape : kMmaShape;
 }
 
-// The 4-bit kernel on SM pairs or single SMs (same 256 x 240 tiles).  With
-// R2_EXACT the pair kernel overlaps each tile's epilogue with the next
-// tile's MMAs and finishes a tile on two SMs in half the time: the faster one
-// for every task size measured (a single region of 29,817 SNPs x 16,622
-// samples: 2.49 ms against 3.16 ms).  R2_REFERENCE's epilogue (the
-// reference's float/double sequence) is the bound, and the single-SM kernel
-// runs it on 16 warps instead of 8: 4.66 ms against 5.11 ms there.
+// The 4-bit kernel on SM pairs or single SMs (same 256 x 240 tiles).  The
+// pair kernel overlaps each tile's epilogue with the next tile's MMAs and
+// finishes a tile on two SMs in half the time: the faster one in both r^2
+// modes (a single region of 29,817 SNPs x 16,622 samples: 2.49 against
+// 3.16 ms exact, 2.82 against 4.14 ms reference).
 const KernelShape &fp4_shape(qld_ctx *c, const Task &t, int b0, int b1) {
     (void)b0; (void)b1;
     if (c->sm_pair == 0)
         if (const TuneChoice *tc = tuned_for(c, t))
             if (tc->kernel == QLD_KERNEL_FP4) return tc->option == 1 ? kMxf4Shape : kMxf4PairShape;
-    if (c->sm_pair == 0) return c->r2_mode == QLD_R2_REFERENCE ? kMxf4Shape : kMxf4PairShape;
     return c->sm_pair == 1 ? kMxf4Shape : kMxf4PairShape;
 }
 

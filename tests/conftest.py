@@ -76,3 +76,17 @@ def gpu_ctx():
     ctx = api.Context(0)
     yield ctx
     ctx.close()
+
+
+@pytest.fixture(autouse=True)
+def _reset_gpu_ctx_options(request):
+    """Tests share one context: each starts from its default options, whatever
+    the previous test set (kernel, tiles, SM pairs, r^2 mode, band rows)."""
+    if "gpu_ctx" in request.fixturenames:
+        from qld_b200 import api
+        ctx = request.getfixturevalue("gpu_ctx")
+        for opt, val in ((api.OPT_KERNEL, api.KERNEL_AUTO), (api.OPT_MMA_TILE, 0),
+                         (api.OPT_SM_PAIR, 0), (api.OPT_R2_MODE, api.R2_EXACT),
+                         (api.OPT_BAND_ROWS, 4096)):
+            ctx.set_option(opt, val)
+    yield

@@ -36,7 +36,7 @@ def test_traffic_follows_the_kernel_the_mode_runs():
     single = _profile_value("k_ld_mxf4_traffic_16384.md")
     fp4, mma = 3, 2
     assert bench.measured_traffic(fp4, WORKLOAD, 0, "exact") == pair
-    assert bench.measured_traffic(fp4, WORKLOAD, 0, "reference") == single
+    assert bench.measured_traffic(fp4, WORKLOAD, 0, "reference") == pair
     assert bench.measured_traffic(fp4, WORKLOAD, 1, "exact") == single
     assert bench.measured_traffic(fp4, WORKLOAD, 2, "reference") == pair
     assert bench.measured_traffic(mma, WORKLOAD) == _profile_value(

@@ -43,7 +43,7 @@ def region():
 
 
 @pytest.mark.parametrize("mode,sm_pair", [("exact", 0), ("reference", 0), ("exact", 1),
-                                          ("reference", 2)])
+                                          ("reference", 1)])
 def test_single_region_full_size(region, mode, sm_pair):
     Tp, lda, bc, m, K, S, out = region
     assert (m, K, S) == (29_817, 260, 16_622)
