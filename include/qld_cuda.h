@@ -123,7 +123,9 @@ int qld_cuda_ld(qld_ctx *ctx,
 
 /*
  * The same task on device-resident buffers, enqueued on `stream`
- * (a cudaStream_t; NULL = the context's stream), asynchronous.
+ * (a cudaStream_t; NULL = the context's own stream, which is non-blocking:
+ * pass cudaStreamLegacy, or the stream that writes the inputs, to order the
+ * call after work on the legacy default stream), asynchronous.
  *   lda/ldb   words between consecutive rows in device memory (>= K, even;
  *             row starts 16-byte aligned).  Words past K are never read.
  *   ldr/ldc   elements between consecutive B rows of r2 / counts (>= m).
@@ -289,7 +291,9 @@ typedef struct qld_query_result {
 } qld_query_result;
 
 int qld_srv_create(int device, size_t pool_bytes, int max_inflight, qld_server **srv);
-/* A and bc may be host or device pointers (K words per row, no padding). */
+/* A and bc may be host or device pointers (K words per row, no padding).
+ * The copy is synchronous but does not wait for work on other streams: a
+ * device table written on a non-blocking stream must be complete first. */
 int qld_srv_add_table(qld_server *srv, const uint64_t *A, const uint32_t *bc, int m, int K,
                       int S, int *table_id);
 int qld_srv_submit(qld_server *srv, const qld_query *q, long long *id);

@@ -442,12 +442,21 @@ def _p(x):
     return _ptr(x)
 
 
+CUDA_STREAM_LEGACY = 1   # cudaStreamLegacy: the legacy default stream's handle
+
+
 def _stream(s):
+    """A cudaStream_t for the C ABI.  None (or 0) keeps the C meaning: the
+    context's own stream.  A torch stream object is passed as itself; torch's
+    default stream is the legacy NULL stream, which the C ABI would read as
+    the context's stream (not ordered with torch's work), so it goes as
+    cudaStreamLegacy instead."""
     if s is None:
         return None
     if isinstance(s, int):
         return s
-    return s.cuda_stream  # torch.cuda.Stream
+    h = s.cuda_stream  # torch.cuda.Stream
+    return h if h else CUDA_STREAM_LEGACY
 
 
 @dataclass
@@ -479,10 +488,17 @@ class Server:
 
     def add_table(self, A, bc, S) -> int:
         """A: (m, K) uint64 numpy array or contiguous int64 torch tensor (host
-        or device); bc: its row bit counts."""
+        or device); bc: its row bit counts.  The copy does not wait for other
+        streams, so the torch streams that write device tensors are
+        synchronized first."""
         if isinstance(A, np.ndarray):
             A = np.ascontiguousarray(A).view(np.uint64)
             bc = np.ascontiguousarray(bc, dtype=np.uint32)
+        else:
+            import torch
+            for t in (A, bc):
+                if isinstance(t, torch.Tensor) and t.is_cuda:
+                    torch.cuda.current_stream(t.device).synchronize()
         tid = ct.c_int()
         self._check(self.lib.qld_srv_add_table(self.h, _ptr(A), _ptr(bc), A.shape[0], A.shape[1],
                                                int(S), ct.byref(tid)))
