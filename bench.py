@@ -93,6 +93,9 @@ def parse(argv=None):
                     help="tensor-core tile rows (0: per shape)")
     ap.add_argument("--snps", type=int, default=0,
                     help="use only the first N SNPs of the workload (profiling captures)")
+    ap.add_argument("--split", action="store_true",
+                    help="with --gpus N: the ranks split ONE region by tile rows "
+                         "(qld_cuda_ld_device_part; strong scaling) instead of one region each")
     return ap.parse_args(argv)
 
 
@@ -109,7 +112,9 @@ def workload_config(name):
 def arm_config(args, world):
     """The `config` of the headline line; both arms print the same dict."""
     cfg = workload_config(args.workload)
-    cfg["parallelism"] = f"replicas x{world} (independent regions, no collective)"
+    cfg["parallelism"] = (f"tile-row split x{world} (one region, no collective)"
+                          if args.split and world > 1 else
+                          f"replicas x{world} (independent regions, no collective)")
     cfg["l2"] = "512 MB flush write between timed steps"
     if args.snps:
         cfg["snps"] = args.snps
@@ -551,13 +556,17 @@ def ours_arm(args, rank, world, local_rank):
     torch.cuda.set_device(dev)
     cfg = arm_config(args, world)
 
-    T, S = make_table(args.workload, dev, seed_offset=rank)
+    split = args.split and world > 1
+    T, S = make_table(args.workload, dev, seed_offset=0 if split else rank)
     if args.snps:
         T = T[:args.snps].contiguous()
     m, K = T.shape
     Tp, lda = padded(T, dev)
     bc = synth.popcount_rows(T).to(torch.int32)
-    out = torch.empty(m, m, dtype=torch.float32, device=dev)
+    r0, r1 = 0, m
+    if split:   # this rank's tile rows of the one region
+        r0, r1 = api.split_rows(m, m, K, True, api.KERNEL_AUTO, rank, world)
+    out = torch.empty(max(1, r1 - r0), m, dtype=torch.float32, device=dev)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
 
     ctx = new_context(local_rank, args)
@@ -567,7 +576,11 @@ def ours_arm(args, rank, world, local_rank):
     torch.cuda.set_stream(st)
 
     def step():
-        ctx.ld_device(Tp, bc, m, lda, Tp, bc, m, lda, K, S, True, out, m, stream=st)
+        if split:
+            ctx.ld_device_part(Tp, bc, m, lda, Tp, bc, m, lda, K, S, True, out, m, rank, world,
+                               stream=st)
+        else:
+            ctx.ld_device(Tp, bc, m, lda, Tp, bc, m, lda, K, S, True, out, m, stream=st)
 
     tuned = None
     if args.autotune and args.kernel == "auto":
@@ -589,14 +602,17 @@ def ours_arm(args, rank, world, local_rank):
 
     pairs = m * (m - 1) / 2
     total_ms_max = max_over_ranks(total_ms, world, dev)
-    value = pairs * args.steps * world / (total_ms_max * 1e-3)
+    regions = 1 if split else world   # the split ranks share one region
+    value = pairs * args.steps * regions / (total_ms_max * 1e-3)
 
     # roofline of the counts kernel
     kern_ms = stats.counts_kernel_ms / max(1, stats.counts_launches)
     bitops = pairs * 64 * K
+    # this rank's pairs: B rows [r0, r1) of the triangle (all of it unless split)
+    rank_pairs = sum(m - 1 - i for i in range(r0, r1)) if split else pairs
     variant = stats.last_kernel
-    roof = kernel_roofline(ctx, variant, bitops, kern_ms, dev)
-    alg_bytes = m * K * 8 * 2 + pairs * 4
+    roof = kernel_roofline(ctx, variant, rank_pairs * 64 * K, kern_ms, dev)
+    alg_bytes = m * K * 8 * 2 + rank_pairs * 4
     sm_pair = args.sm_pair
     if tuned is not None and tuned["kernel"] == 3 and sm_pair == 0:
         sm_pair = tuned["option"]
@@ -610,21 +626,26 @@ def ours_arm(args, rank, world, local_rank):
 
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong" if split else "weak",
+            "vs_baseline": None,
             "dtype": "u64 popcount / f32 r2", "data": "synthetic", "config": cfg,
-            "bitops_per_s": bitops * args.steps * world / (total_ms_max * 1e-3),
+            "bitops_per_s": bitops * args.steps * regions / (total_ms_max * 1e-3),
             "gpu_launches": stats.kernel_launches, "kernel_variant": variant,
             "roofline": roof, "clocks": clocks}
     if tuned is not None:
         line["autotune"] = tuned
 
+    if split:
+        line["split_rows"] = [r0, r1]
     # ---- sampled oracle check of the output the timed steps wrote
-    if not args.no_parity and rank == 0:
+    if not args.no_parity and rank == 0 and not split:
         line["parity"] = region_parity(ctx, Tp, bc, m, lda, K, S, out, st, args.r2_mode,
                                        seed=11)
 
     # ---- e2e through the host-buffer C-ABI call
-    if not args.no_e2e:
+    if split and not args.no_e2e:
+        line["e2e_note"] = "no host-buffer form of a split task: e2e is measured without --split"
+    if not args.no_e2e and not split:
         Th = ctx.pinned_empty((m, K), np.uint64)
         Th[:] = T.cpu().numpy().view(np.uint64)
         bch = ctx.pinned_empty((m,), np.uint32)

@@ -143,6 +143,24 @@ int qld_cuda_ld_device(qld_ctx *ctx, const qld_ld_args *args, void *stream);
 int qld_cuda_sync(qld_ctx *ctx, void *stream);
 
 /*
+ * One task split over several GPUs (one context per GPU, each holding the
+ * whole tables): part `part` of `nparts` computes the B rows
+ * [*row0, *row1) -- consecutive whole tile rows of the kernel the context
+ * chooses, with (nearly) equal numbers of output tiles, i.e. equal bit-ops --
+ * into args->r2 / args->counts, whose row 0 is B row *row0 (so they need
+ * *row1 - *row0 rows).  No exchange between the parts: each GPU keeps its
+ * rows.  Parts past a task's last tile row are empty (*row0 == *row1).
+ * qld_cuda_split_rows gives the same ranges without a context or a GPU, for
+ * kernel QLD_KERNEL_POPC / _MMA / _FP4 (AUTO: the built-in rule).
+ * No counterpart in the reference (its tasks are split by the user's window
+ * lists, load_balancer.c / utilities/split_region, one CPU thread each).
+ */
+int qld_cuda_ld_device_part(qld_ctx *ctx, const qld_ld_args *args, int part, int nparts,
+                            int *row0, int *row1, void *stream);
+int qld_cuda_split_rows(int m, int n, int K, int symmetric, int kernel, int part, int nparts,
+                        int *row0, int *row1);
+
+/*
  * The report's pairs only, filtered on the GPU.  Computes the task as
  * qld_cuda_ld() does, one block of QLD_OPT_BAND_ROWS B rows at a time, and
  * keeps the pairs qLD's writeResults() prints (src/correlator/src/

@@ -33,6 +33,7 @@ OPT_WAIT_CYCLES, OPT_MEM_CAP = 7, 8
 EXPORTED = (
     "qld_cuda_init", "qld_cuda_release", "qld_cuda_last_error", "qld_cuda_set_option",
     "qld_cuda_ld", "qld_cuda_ld_device", "qld_cuda_ld_hits", "qld_cuda_ld_batch",
+    "qld_cuda_ld_device_part", "qld_cuda_split_rows",
     "qld_cuda_count_states", "qld_cuda_count_states_device", "qld_cuda_vcf_pack",
     "qld_cuda_ld_band",
     "qld_cuda_ld_band_device", "qld_cuda_sync",
@@ -118,6 +119,9 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.qld_cuda_ld.argtypes = [vp, vp, vp, i, vp, vp, i, i, i, i, vp, vp]
     lib.qld_cuda_ld_device.argtypes = [vp, ct.POINTER(_LdArgs), vp]
     lib.qld_cuda_ld_batch.argtypes = [vp, ct.POINTER(_LdArgs), i, vp]
+    lib.qld_cuda_ld_device_part.argtypes = [vp, ct.POINTER(_LdArgs), i, i, ct.POINTER(i),
+                                            ct.POINTER(i), vp]
+    lib.qld_cuda_split_rows.argtypes = [i, i, i, i, i, i, i, ct.POINTER(i), ct.POINTER(i)]
     lib.qld_cuda_count_states.argtypes = [vp, vp, i, vp, i, i, i, vp]
     lib.qld_cuda_vcf_pack.argtypes = [vp, ct.c_char_p, ct.c_size_t, vp, i, vp, i, i, i, RAND_FN,
                                       vp, vp, vp, vp, vp, ct.POINTER(i)]
@@ -395,6 +399,17 @@ class Context:
                     int(S), int(bool(symmetric)), _p(r2), int(ldr), _p(counts), int(ldc))
         self._check(self.lib.qld_cuda_ld_device(self.h, ct.byref(a), _stream(stream)))
 
+    def ld_device_part(self, A, bcA, m, lda, B, bcB, n, ldb, K, S, symmetric, r2, ldr, part,
+                       nparts, counts=None, ldc=0, stream=None):
+        """Part `part` of `nparts` of a task split over GPUs: enqueues B rows
+        [row0, row1) into r2 (row 0 = B row row0); returns (row0, row1)."""
+        a = _LdArgs(_p(A), _p(bcA), int(m), int(lda), _p(B), _p(bcB), int(n), int(ldb), int(K),
+                    int(S), int(bool(symmetric)), _p(r2), int(ldr), _p(counts), int(ldc))
+        r0, r1 = ct.c_int(), ct.c_int()
+        self._check(self.lib.qld_cuda_ld_device_part(self.h, ct.byref(a), int(part), int(nparts),
+                                                     ct.byref(r0), ct.byref(r1), _stream(stream)))
+        return r0.value, r1.value
+
     def ld_batch(self, jobs, stream=None):
         """Enqueue many tasks in one launch.  `jobs`: sequence of dicts with
         the ld_device keyword names (A, bcA, m, lda, B, bcB, n, ldb, K, S,
@@ -432,6 +447,18 @@ class Context:
 
     def sync(self, stream=None):
         self._check(self.lib.qld_cuda_sync(self.h, _stream(stream)))
+
+
+def split_rows(m, n, K, symmetric, kernel, part, nparts):
+    """(row0, row1) of part `part` of `nparts` (qld_cuda_split_rows; no GPU
+    needed)."""
+    lib = load_library()
+    r0, r1 = ct.c_int(), ct.c_int()
+    rc = lib.qld_cuda_split_rows(int(m), int(n), int(K), int(bool(symmetric)), int(kernel),
+                                 int(part), int(nparts), ct.byref(r0), ct.byref(r1))
+    if rc != OK:
+        raise QldError(rc, "qld_cuda_split_rows: bad arguments")
+    return r0.value, r1.value
 
 
 def _p(x):

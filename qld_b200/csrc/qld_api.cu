@@ -525,6 +525,36 @@ struct OptionGuard {
 
 constexpr int kTuneMaxSide = 16384;   // the tuner measures at most 16,384 x 16,384
 
+// Part `part` of `nparts` of a task's B rows for a split over GPUs:
+// consecutive whole B tile rows of the kernel's tiles, with (nearly) equal
+// numbers of output tiles -- equal bit-ops, since every tile of a task costs
+// K words.  Part k starts at the first tile row before which k/nparts of the
+// task's tiles lie; trailing parts of a task with fewer tile rows than parts
+// are empty (row0 == row1).
+void split_rows(const Task &t, int bm, int bn, int part, int nparts, int *r0, int *r1) {
+    const int nb = (t.n + bn - 1) / bn;
+    const long long total = tile_count(t, bm, bn, 0, t.n);
+    auto boundary = [&](int k) -> int {
+        if (k <= 0) return 0;
+        if (k >= nparts) return t.n;
+        const long long target = total * k / nparts;
+        long long cum = 0;
+        for (int tb = 0; tb < nb; ++tb) {
+            if (cum >= target) return tb * bn;
+            const int e = (tb + 1) * bn < t.n ? (tb + 1) * bn : t.n;
+            cum += tile_count(t, bm, bn, tb * bn, e);
+        }
+        return t.n;
+    };
+    *r0 = boundary(part);
+    *r1 = boundary(part + 1);
+}
+
+const KernelShape &split_shape(int variant) {
+    return variant == QLD_KERNEL_FP4 ? kMxf4PairShape
+           : variant == QLD_KERNEL_MMA ? kMmaShape : kPopcShape;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1066,6 +1096,42 @@ int qld_cuda_ld_device(qld_ctx *c, const qld_ld_args *a, void *stream) {
     CUDA_TRY(c, cudaSetDevice(c->device));
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     return launch_counts(c, t, 0, t.n, a->r2, a->ldr, a->counts, a->ldc, 0, st);
+}
+
+int qld_cuda_split_rows(int m, int n, int K, int symmetric, int kernel, int part, int nparts,
+                        int *row0, int *row1) {
+    if (symmetric) n = m;
+    if (m < 0 || n < 0 || K < 1 || nparts < 1 || part < 0 || part >= nparts || !row0 || !row1)
+        return QLD_ERR_INVALID;
+    Task t{nullptr, nullptr, m, K + (K & 1), nullptr, nullptr, n, K + (K & 1), K, 64 * K,
+           symmetric, 0};
+    if (kernel == QLD_KERNEL_AUTO) kernel = fp4_exact_for(t) ? QLD_KERNEL_FP4 : QLD_KERNEL_POPC;
+    if (kernel != QLD_KERNEL_POPC && kernel != QLD_KERNEL_MMA && kernel != QLD_KERNEL_FP4)
+        return QLD_ERR_INVALID;
+    const KernelShape &ks = split_shape(kernel);
+    split_rows(t, ks.bm, ks.bn, part, nparts, row0, row1);
+    return QLD_OK;
+}
+
+int qld_cuda_ld_device_part(qld_ctx *c, const qld_ld_args *a, int part, int nparts, int *row0,
+                            int *row1, void *stream) {
+    if (!c || !a || !row0 || !row1 || nparts < 1 || part < 0 || part >= nparts)
+        return QLD_ERR_INVALID;
+    Task t{a->A, a->bcA, a->m, a->lda, a->B, a->bcB, a->n, a->ldb, a->K, a->S, a->symmetric, 0};
+    if (t.symmetric) { t.B = t.A; t.bcB = t.bcA; t.n = t.m; t.ldb = t.lda; }
+    if (t.m < 0 || t.n < 0 || t.K < 1 || t.S < 1 || t.lda < t.K || t.ldb < t.K || (t.lda & 1) ||
+        (t.ldb & 1) || a->ldr < t.m || (a->counts && a->ldc < t.m))
+        return set_err(c, QLD_ERR_INVALID, "bad sizes/strides m=%d n=%d K=%d lda=%lld ldb=%lld",
+                       t.m, t.n, t.K, t.lda, t.ldb);
+    const int variant = variant_of(c, t);
+    const KernelShape &ks = shape_of(c, variant, t, 0, t.n);
+    split_rows(t, ks.bm, ks.bn, part, nparts, row0, row1);
+    if (t.m == 0 || *row0 >= *row1) return QLD_OK;
+    if (!t.A || !t.B || !t.bcA || !t.bcB || !a->r2 || !aligned16(t.A) || !aligned16(t.B))
+        return set_err(c, QLD_ERR_INVALID, "NULL or misaligned device pointer");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    return launch_counts(c, t, *row0, *row1, a->r2, a->ldr, a->counts, a->ldc, *row0, st);
 }
 
 int qld_cuda_ld_band_device(qld_ctx *c, const uint64_t *A, const uint32_t *bcA, int m,
