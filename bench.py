@@ -835,7 +835,7 @@ def section_windowed(args, local_rank, flush, m_full=None):
         del cnt
         T_np = T.cpu().numpy().view(np.uint64)
         bc_np = bc.cpu().numpy().astype(np.uint32)
-        par = band_parity(T_np, bc_np, S, got, rows, W, counts_rows=got_c)
+        par = band_parity(T_np, bc_np, S, got, rows, W, mode=args.r2_mode, counts_rows=got_c)
         inside = np.arange(W)[None, :] < (m - 1 - rows)[:, None]
         par["rerun_bit_identical"] = bool(np.array_equal(got[inside].view(np.uint32),
                                                          again[inside].view(np.uint32)))
@@ -902,7 +902,7 @@ def make_batched_jobs(njobs, dev, seed=0):
     return jobs, pairs, bitops
 
 
-def batch_parity(jobs, rows_per_job=2, seed=0, chunk=256):
+def batch_parity(jobs, rows_per_job=2, seed=0, chunk=256, mode="exact"):
     """Every job of a batched call, a few B rows each (one random row and the
     last row, whose tile is among the last the queue hands out), checked
     against the oracle over all of the job's A rows."""
@@ -927,7 +927,7 @@ def batch_parity(jobs, rows_per_job=2, seed=0, chunk=256):
             valid = (np.arange(m)[None, :] >= r[:, None]) if j["symmetric"] \
                 else np.ones((len(rows), m), bool)
             groups.append(dict(A=A, bcA=bcA, B=B, bcB=bcB, S=j["S"], got=got, valid=valid))
-        res = oracle.check_groups(groups, mode="exact")
+        res = oracle.check_groups(groups, mode=mode)
         if total is None:
             total = res
         else:
@@ -935,7 +935,9 @@ def batch_parity(jobs, rows_per_job=2, seed=0, chunk=256):
                 total[k] += res[k]
             total["r2_mean_rel"] = max(total["r2_mean_rel"], res["r2_mean_rel"])
             total["r2_max_rel"] = max(total["r2_max_rel"], res["r2_max_rel"])
-            total["r2_within_tol"] = total["r2_within_tol"] and res["r2_within_tol"]
+            for k in ("r2_within_tol", "r2_bit_identical"):
+                if k in res:
+                    total[k] = total[k] and res[k]
             total["ok"] = total["ok"] and res["ok"]
     total["r2_mean_rel_note"] = "largest per-chunk mean over chunks of 256 jobs"
     total["sample"] = f"all {len(jobs)} jobs x {rows_per_job} B rows x all A rows"
@@ -952,6 +954,8 @@ def section_batched(args, local_rank, flush):
     jobs, pairs, bitops = make_batched_jobs(args.jobs, dev, seed=0)
     ctx = api.Context(local_rank)
     ctx.set_option(api.OPT_PROFILE, 1)
+    ctx.set_option(api.OPT_R2_MODE,
+                   api.R2_REFERENCE if args.r2_mode == "reference" else api.R2_EXACT)
     st = torch.cuda.current_stream(dev)
 
     def batched():
@@ -987,7 +991,7 @@ def section_batched(args, local_rank, flush):
            "speedup_vs_plain": ms_p / ms_b}
     if not args.no_parity:
         # the batched call ran last: its outputs are what the jobs hold now
-        out["parity"] = batch_parity(jobs, seed=15)
+        out["parity"] = batch_parity(jobs, seed=15, mode=args.r2_mode)
     ctx.close()
     del jobs
     return out
