@@ -14,21 +14,24 @@
 // the MMAs fill the other, and each SM's shared memory supplies every
 // unpacked row once per MMA.
 //
-// Roles (both CTAs of a pair, 576 threads):
+// Roles (both CTAs of a pair, 640 threads):
 //   warp 0       TMA producer: the CTA's 128 A rows and 120 B rows, 8 packed
 //                words (512 samples) per stage, 64-byte swizzle.
 //   warp 1       TMEM allocation for the pair (cta_group::2); in rank 0 the
 //                MMA issuer: per unpacked stage (256 samples) 4 MMAs of
 //                256 x 240 x 64, then one commit that arrives on the stage's
 //                "empty" barrier in both CTAs.
-//   warps 2-9    unpack (w -> four words of nibbles, as ld_mxf4.cu) into the
+//   warps 2-11   unpack (w -> four words of nibbles, as ld_mxf4.cu) into the
 //                CTA's stage; they arrive on rank 0's "full" barrier.  Two
-//                groups of four warps take alternate unpacked stages (each
-//                thread 2 rows of every other stage): two stages in flight per
-//                CTA, which the per-warp latency of a stage (load, spread,
-//                store, proxy fence, remote arrive) needs to keep up with the
-//                MMAs.
-//   warps 10-17  epilogue: warp w reads TMEM lane quarter w % 4 of the
+//                groups of five warps take alternate unpacked stages (each
+//                thread one or two rows of every other stage): two stages in
+//                flight per CTA, which the per-warp latency of a stage (load,
+//                spread, store, proxy fence, remote arrive) needs to keep up
+//                with the MMAs.  Five warps per group measured 3 % faster than
+//                four (2.44 / 2.76 ms against 2.52 / 2.83 ms, exact /
+//                reference r^2); six, at the 80 registers 22 warps leave, 4 %
+//                slower.
+//   warps 12-19  epilogue: warp w reads TMEM lane quarter w % 4 of the
 //                accumulator buffer the tile used, four of its eight 32-column
 //                chunks, applies the r^2 epilogue (gemm_cpu.c:343-404) and
 //                stores; they arrive on rank 0's "accumulator empty" barrier.
@@ -56,12 +59,12 @@ constexpr int PB_TX = HN * PW * 8;       // 7.5 KB delivered per stage
 constexpr int PB_BYTES = 8192;           // stage stride, 1024-byte aligned
 constexpr int UA_BYTES = HM * 128;       // 16 KB: 256 E2M1 per row
 constexpr int UB_BYTES = HN * 128;       // 15 KB
-constexpr int UNPACK_WARPS = 8, EPI_WARPS = 8;
+constexpr int UNPACK_WARPS = 10, EPI_WARPS = 8;
 constexpr int FIRST_UNPACK_WARP = 2;
 constexpr int FIRST_EPI_WARP = FIRST_UNPACK_WARP + UNPACK_WARPS;
 constexpr int UNPACKERS = UNPACK_WARPS * 32;
 constexpr int EPILOGUE = EPI_WARPS * 32;
-constexpr int THREADS = (FIRST_EPI_WARP + EPI_WARPS) * 32;   // 576
+constexpr int THREADS = (FIRST_EPI_WARP + EPI_WARPS) * 32;   // 640
 constexpr int GROUP_THREADS = UNPACKERS / 2;                 // unpackers per stage
 constexpr int NTASK = HM + HN;                               // row tasks
 constexpr int TASKS = (NTASK + GROUP_THREADS - 1) / GROUP_THREADS;
