@@ -931,15 +931,16 @@ def batch_parity(jobs, rows_per_job=2, seed=0, chunk=256, mode="exact"):
         if total is None:
             total = res
         else:
-            for k in ("rows_checked", "pairs_checked"):
+            n0, n1 = total["r2_rel_count"], res["r2_rel_count"]
+            if n0 + n1:
+                total["r2_mean_rel"] = (total["r2_mean_rel"] * n0 + res["r2_mean_rel"] * n1) / (n0 + n1)
+            for k in ("rows_checked", "pairs_checked", "r2_rel_count"):
                 total[k] += res[k]
-            total["r2_mean_rel"] = max(total["r2_mean_rel"], res["r2_mean_rel"])
             total["r2_max_rel"] = max(total["r2_max_rel"], res["r2_max_rel"])
             for k in ("r2_within_tol", "r2_bit_identical"):
                 if k in res:
                     total[k] = total[k] and res[k]
             total["ok"] = total["ok"] and res["ok"]
-    total["r2_mean_rel_note"] = "largest per-chunk mean over chunks of 256 jobs"
     total["sample"] = f"all {len(jobs)} jobs x {rows_per_job} B rows x all A rows"
     return total
 

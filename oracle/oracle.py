@@ -393,9 +393,9 @@ def check_groups(groups, mode="exact", rtol=1e-6, workers=None):
         pairs += int(v.sum())
     got = np.concatenate(got) if got else np.zeros(0, np.float32)
     w64 = np.concatenate(w64) if w64 else np.zeros(0)
-    specials, max_rel, mean_rel, _ = r2_errors(got, w64)
+    specials, max_rel, mean_rel, n_rel = r2_errors(got, w64)
     res = {"rows_checked": rows, "pairs_checked": pairs, "r2_max_rel": max_rel,
-           "r2_mean_rel": mean_rel, "r2_mode": mode}
+           "r2_mean_rel": mean_rel, "r2_rel_count": n_rel, "r2_mode": mode}
     has_counts = any(g.get("counts") is not None for g in groups)
     if has_counts:
         res["counts_exact"] = cnt_ok
