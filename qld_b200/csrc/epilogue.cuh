@@ -151,7 +151,8 @@ __device__ __forceinline__ float pair_r2_exact(uint32_t cnt, const ARow &ra, con
 //    Pairs failing it (~1e-5 at realistic S; more at S <= 100, whose simple
 //    fractions meet midpoints more often), with a row whose v >= 1 (NaN
 //    factors), or with 0 < x < 2^-100 (a subnormal-range quotient) are
-//    flagged and recomputed with r2_reference.
+//    flagged and recomputed by r2_flagged: a fixed SNP (v = 1) from x alone,
+//    the rest with r2_reference.
 //  * (double)r > 1.0001 is r > 1 + 838 * 2^-23, the largest float not above
 //    1.0001.
 // Exact zeros need no test: a zero row's factors are 0, so q = 0.
@@ -181,13 +182,30 @@ __device__ __forceinline__ float r2_reference_ff(float cab, const ARowR &A, floa
     return rh > __uint_as_float(0x3F800000u + 838u) ? 123.456f : rh;
 }
 
-// The reference-mode chunk: every pair on the fast path, the flagged ones
-// (their accumulator word kept in v, a bit in `redo`) redone with
-// r2_reference.
+// A pair the fast path flagged.  A fixed SNP (v = 1: every sample carries
+// the allele) makes the reference's denominator p12 (1 - vA)(1 - vB) exactly
+// +0, so its quotient is x / +0 = +inf, hence 123.456, or 0 / 0, the x86
+// default NaN 0xFFC00000 (gemm_cpu.c:363-389); that needs x alone, with the
+// reference's float rounding, and no FP64 division.  Empty SNPs keep the
+// zero rule; bit counts above S and the rare rounding cases run the literal
+// sequence.
+__device__ __forceinline__ float r2_flagged(uint32_t cab, const RowRef &A, const RowRef &B,
+                                            int S) {
+    if (A.v == 0.0f || B.v == 0.0f) return 0.0f;
+    if (A.v <= 1.0f && B.v <= 1.0f && (A.v == 1.0f || B.v == 1.0f)) {
+        const float d = __fsub_rn(__fdiv_rn((float)cab, (float)S), __fmul_rn(A.v, B.v));
+        return __fmul_rn(d, d) == 0.0f ? __uint_as_float(0xFFC00000u) : 123.456f;
+    }
+    return r2_reference(cab, A, B, S);
+}
+
+// The reference-mode chunk of CW (<= 32) columns: every pair on the fast
+// path, the flagged ones (their accumulator word kept in v, a bit in `redo`)
+// redone with r2_flagged.
 // FLOATCNT: v holds each count as F32 bits (the 4-bit kernels' accumulators),
 // else as an integer shifted left by SHIFT.
-template <int SHIFT, bool FLOATCNT>
-__device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARowR &ra, const ColsR &f,
+template <int SHIFT, bool FLOATCNT, int CW = 32>
+__device__ __forceinline__ void chunk_ref(uint32_t (&v)[CW], const ARowR &ra, const ColsR &f,
                                           int bl0, int b0, int a, bool a_ok, int n, int dlo,
                                           int dhi, float *r2, long long ldr, uint32_t *counts,
                                           long long ldc, int row0, int S) {
@@ -195,7 +213,7 @@ __device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARowR &ra, co
     uint32_t redo = 0;
     if (S <= (1 << 24)) {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
+        for (int t = 0; t < CW; ++t) {
             const uint32_t raw = v[t];
             const float cf = FLOATCNT ? __uint_as_float(raw) : (float)(raw >> SHIFT);
             const int b = b0 + t;
@@ -208,12 +226,12 @@ __device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARowR &ra, co
         }
     } else {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
+        for (int t = 0; t < CW; ++t) {
             const uint32_t cnt = FLOATCNT ? (uint32_t)__uint_as_float(v[t]) : v[t] >> SHIFT;
             const int b = b0 + t;
             if (oc && b < n && a - b >= dlo && a - b <= dhi) oc[(long long)t * ldc] = cnt;
         }
-        redo = 0xFFFFFFFFu;
+        redo = CW == 32 ? 0xFFFFFFFFu : (1u << CW) - 1u;
     }
     if (!a_ok) redo = 0;
     if (__any_sync(0xffffffffu, redo != 0)) {
@@ -222,7 +240,7 @@ __device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARowR &ra, co
         rA.v = ra.k.x;
         rA.one_minus = __dsub_rn(1.0, (double)ra.k.x);
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
+        for (int t = 0; t < CW; ++t) {
             const bool rd = (redo >> t) & 1u;
             if (__any_sync(0xffffffffu, rd) && rd) {
                 const float4 cb = f.f[bl0 + t];
@@ -231,19 +249,19 @@ __device__ __forceinline__ void chunk_ref(uint32_t (&v)[32], const ARowR &ra, co
                 rb.v = cb.x;
                 rb.one_minus = __dsub_rn(1.0, (double)cb.x);
                 const uint32_t cnt = FLOATCNT ? (uint32_t)__uint_as_float(v[t]) : v[t] >> SHIFT;
-                v[t] = __float_as_uint(r2_reference(cnt, rA, rb, S));
+                v[t] = __float_as_uint(r2_flagged(cnt, rA, rb, S));
             }
         }
     }
     if (!a_ok) return;
     float *o = r2 + (long long)(b0 - row0) * ldr + a;
-    const bool interior = (b0 + 31 < n) && (a - (b0 + 31) >= dlo) && (a - b0 <= dhi);
+    const bool interior = (b0 + CW - 1 < n) && (a - (b0 + CW - 1) >= dlo) && (a - b0 <= dhi);
     if (interior) {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) o[(long long)t * ldr] = __uint_as_float(v[t]);
+        for (int t = 0; t < CW; ++t) o[(long long)t * ldr] = __uint_as_float(v[t]);
     } else {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
+        for (int t = 0; t < CW; ++t) {
             const int b = b0 + t;
             if (b < n && a - b >= dlo && a - b <= dhi) o[(long long)t * ldr] = __uint_as_float(v[t]);
         }
@@ -347,19 +365,20 @@ __device__ __forceinline__ float pair_r2_f64(float c, float ca, float cb, int S)
     return __double2float_rn(r);
 }
 
-// One 32-column chunk of F32 accumulators v[t] (count c as float bits), as
+// One chunk of CW (<= 32) columns of F32 accumulators v[t] (count c as float bits), as
 // chunk<R2_EXACT, 0> with the FP32 evaluation above.  taddr is the TMEM
 // address the chunk was loaded from: the rare pairs whose FP32 value lies
 // above 1.00009 are re-evaluated in FP64 from their count, reloaded one
 // column at a time (warp-uniform loads, off the common path).
-__device__ __forceinline__ void chunk_f32(uint32_t (&v)[32], uint32_t taddr, const ARowF &ra,
+template <int CW = 32>
+__device__ __forceinline__ void chunk_f32(uint32_t (&v)[CW], uint32_t taddr, const ARowF &ra,
                                           const ColsF &f, int bl0, int b0, int a, bool a_ok,
                                           int n, int dlo, int dhi, float *r2, long long ldr,
                                           uint32_t *counts, long long ldc, int row0, int S) {
     const float S_f = (float)S;
     if (counts && a_ok) {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
+        for (int t = 0; t < CW; ++t) {
             const int b = b0 + t;
             if (b < n && a - b >= dlo && a - b <= dhi)
                 counts[(long long)(b - row0) * ldc + a] = (uint32_t)__uint_as_float(v[t]);
@@ -367,14 +386,14 @@ __device__ __forceinline__ void chunk_f32(uint32_t (&v)[32], uint32_t taddr, con
     }
     float rmax = 0.0f;
 #pragma unroll
-    for (int t = 0; t < 32; ++t) {
+    for (int t = 0; t < CW; ++t) {
         const float r = pair_r2_f32(__uint_as_float(v[t]), S_f, ra, f.f[bl0 + t]);
         rmax = fmaxf(rmax, r);
         v[t] = __float_as_uint(r);
     }
     if (__any_sync(0xffffffffu, rmax > 1.00009f)) {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
+        for (int t = 0; t < CW; ++t) {
             const bool redo = __uint_as_float(v[t]) > 1.00009f;
             if (__any_sync(0xffffffffu, redo)) {
                 uint32_t w;
@@ -390,13 +409,13 @@ __device__ __forceinline__ void chunk_f32(uint32_t (&v)[32], uint32_t taddr, con
     }
     if (!a_ok) return;
     float *o = r2 + (long long)(b0 - row0) * ldr + a;
-    const bool interior = (b0 + 31 < n) && (a - (b0 + 31) >= dlo) && (a - b0 <= dhi);
+    const bool interior = (b0 + CW - 1 < n) && (a - (b0 + CW - 1) >= dlo) && (a - b0 <= dhi);
     if (interior) {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) o[(long long)t * ldr] = __uint_as_float(v[t]);
+        for (int t = 0; t < CW; ++t) o[(long long)t * ldr] = __uint_as_float(v[t]);
     } else {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
+        for (int t = 0; t < CW; ++t) {
             const int b = b0 + t;
             if (b < n && a - b >= dlo && a - b <= dhi) o[(long long)t * ldr] = __uint_as_float(v[t]);
         }
@@ -410,11 +429,12 @@ struct SumAcc {
     double sum = 0.0;
     unsigned long long cnt = 0;
     float mx = 0.0f;
-    __device__ __forceinline__ void fold(const uint32_t (&v)[32], int b0, int a, bool a_ok,
+    template <int CW>
+    __device__ __forceinline__ void fold(const uint32_t (&v)[CW], int b0, int a, bool a_ok,
                                          int n, int symmetric, float threshold) {
         if (!a_ok) return;
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
+        for (int t = 0; t < CW; ++t) {
             const int b = b0 + t;
             const float r = __uint_as_float(v[t]);
             // a pair of the task, and not NaN or the 123.456 sentinel

@@ -398,23 +398,27 @@ k_ld_batch(const BatchParams bp) {
                 const int n_tile = it.tb * BN + BN < J.n ? it.tb * BN + BN : J.n;
                 const int dlo = diag_lo(J.symmetric, 0), dhi = diag_hi(0);
                 epi::SumAcc acc;
+                // chunks of CW columns: 32 in exact mode; 16 in reference mode, whose
+                // longer epilogue runs faster on fewer live registers (182 against
+                // 199 ms on the 4,096-task mix; exact mode: 70.5 against 71.7 ms)
+                constexpr int CW = MODE == R2_EXACT ? 32 : 16;
 #pragma unroll 1
-                for (int c = colh; c < 8; c += 2) {
-                    uint32_t v[32];
+                for (int c = colh; c < 256 / CW; c += 2) {
+                    uint32_t v[CW];
                     __syncwarp();
-                    tc_ld_32x32b_x32(tbase + (uint32_t)(c * 32), v);
+                    tc_ld_32x32b<CW>(tbase + (uint32_t)(c * CW), v);
                     if constexpr (MODE == R2_EXACT) {
-                        epi::chunk_f32(v, tbase + (uint32_t)(c * 32), raf, colsf, c * 32,
-                                       it.tb * BN + c * 32, a, a_ok, n_tile, dlo, dhi, J.r2,
-                                       J.ldr, J.counts, J.ldc, 0, J.S);
+                        epi::chunk_f32<CW>(v, tbase + (uint32_t)(c * CW), raf, colsf, c * CW,
+                                           it.tb * BN + c * CW, a, a_ok, n_tile, dlo, dhi, J.r2,
+                                           J.ldr, J.counts, J.ldc, 0, J.S);
                         if (J.summary)
-                            acc.fold(v, it.tb * BN + c * 32, a, a_ok, J.n, J.symmetric,
+                            acc.fold(v, it.tb * BN + c * CW, a, a_ok, J.n, J.symmetric,
                                      J.threshold);
                     } else {
                         // the F32 accumulators hold the counts as floats
-                        epi::chunk_ref<0, true>(v, ra, colsr, c * 32, it.tb * BN + c * 32, a, a_ok,
-                                            n_tile, dlo, dhi, J.r2, J.ldr, J.counts, J.ldc, 0,
-                                            J.S);
+                        epi::chunk_ref<0, true, CW>(v, ra, colsr, c * CW, it.tb * BN + c * CW, a,
+                                                    a_ok, n_tile, dlo, dhi, J.r2, J.ldr,
+                                                    J.counts, J.ldc, 0, J.S);
                     }
                 }
                 tc_fence_before();

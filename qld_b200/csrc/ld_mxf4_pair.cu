@@ -32,8 +32,8 @@
 //                reference r^2); six, at the 80 registers 22 warps leave, 4 %
 //                slower.
 //   warps 12-19  epilogue: warp w reads TMEM lane quarter w % 4 of the
-//                accumulator buffer the tile used, four of its eight 32-column
-//                chunks, applies the r^2 epilogue (gemm_cpu.c:343-404) and
+//                accumulator buffer the tile used, eight of its sixteen
+//                16-column chunks, applies the r^2 epilogue (gemm_cpu.c:343-404) and
 //                stores; they arrive on rank 0's "accumulator empty" barrier.
 // Every wait is bounded.  No thread returns early: both CTAs meet at the
 // cluster barriers at start and end on every path, including after a
@@ -310,18 +310,20 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                     tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)ab * ACC_STRIDE;
                 // columns past the tile's 240 B rows are read but not written
                 const int n_tile = tb * BN + BN < p.n ? tb * BN + BN : p.n;
+                // 16-column chunks: fewer live registers than 32 (2.41 / 2.66 ms
+                // against 2.43 / 2.75 ms, exact / reference r^2)
 #pragma unroll 1
-                for (int c = colh; c < 8; c += 2) {
-                    uint32_t v[32];
+                for (int c = colh; c < 16; c += 2) {
+                    uint32_t v[16];
                     __syncwarp();
-                    tc_ld_32x32b_x32(tbase + (uint32_t)(c * 32), v);
+                    tc_ld_32x32b_x16(tbase + (uint32_t)(c * 16), v);
                     if constexpr (MODE == R2_EXACT) {
-                        epi::chunk_f32(v, tbase + (uint32_t)(c * 32), raf, colsf, c * 32,
-                                       tb * BN + c * 32, a, a_ok, n_tile,
-                                       dlo, dhi, p.r2, p.ldr, p.counts, p.ldc, p.out_row0, p.S);
+                        epi::chunk_f32<16>(v, tbase + (uint32_t)(c * 16), raf, colsf, c * 16,
+                                           tb * BN + c * 16, a, a_ok, n_tile,
+                                           dlo, dhi, p.r2, p.ldr, p.counts, p.ldc, p.out_row0, p.S);
                     } else {
                         // the F32 accumulators hold the counts as floats
-                        epi::chunk_ref<0, true>(v, ra, colsr, c * 32, tb * BN + c * 32, a, a_ok,
+                        epi::chunk_ref<0, true, 16>(v, ra, colsr, c * 16, tb * BN + c * 16, a, a_ok,
                                             n_tile, dlo, dhi, p.r2, p.ldr, p.counts, p.ldc,
                                             p.out_row0, p.S);
                     }

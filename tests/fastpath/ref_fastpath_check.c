@@ -5,8 +5,8 @@
  * monomorphic SNPs, near-independence counts, bit counts above S.  The same
  * steps in C: per-row factors v = c/S, 1/(v(1-v)) as a float pair and 1/v;
  * the Markstein-corrected FP32 quotient cab/S; the FMA TwoProduct error of
- * p12; the quotient as a float pair; the rounding test and its fallback to
- * the literal sequence.  Build with -ffp-contract=off so the reference
+ * p12; the quotient as a float pair; the rounding test and its fallback
+ * (the fixed-SNP shortcut, else the literal sequence).  Build with -ffp-contract=off so the reference
  * sequence is not fused (fmaf() is an explicit FMA either way).
  *   usage: ref_fastpath_check N_PAIRS      exit 0 iff every pair matches */
 #include <math.h>
@@ -62,7 +62,17 @@ static float ff_r2(uint32_t cab, uint32_t ca, uint32_t cb, int S) {
     int redo = (rh != rl) || tiny;
     float r = rh;
     if (r > b2f(0x3F800000u + 838u)) r = 123.456f;
-    if (redo) { if (!(A.v > 0 && A.v < 1 && B.v > 0 && B.v < 1)) ++fb_spec; else if (tiny) ++fb_tiny; else ++fb_amb; ++fallbacks; r = ref_r2(cab, ca, cb, S); }
+    if (redo) {
+        if (!(A.v > 0 && A.v < 1 && B.v > 0 && B.v < 1)) ++fb_spec; else if (tiny) ++fb_tiny; else ++fb_amb;
+        ++fallbacks;
+        /* the device's r2_flagged: zero rule, fixed SNP (v = 1: den = +0), else the sequence */
+        if (A.v == 0.0f || B.v == 0.0f) r = 0.0f;
+        else if (A.v <= 1.0f && B.v <= 1.0f && (A.v == 1.0f || B.v == 1.0f)) {
+            volatile float q = (float)cab / (float)S, p = A.v * B.v;
+            volatile float dd = q - p, xx = dd * dd;
+            r = xx == 0.0f ? b2f(0xFFC00000u) : 123.456f;
+        } else r = ref_r2(cab, ca, cb, S);
+    }
     return r;
 }
 int main(int argc, char **argv) {
