@@ -515,9 +515,10 @@ class Server:
 
     def add_table(self, A, bc, S) -> int:
         """A: (m, K) uint64 numpy array or contiguous int64 torch tensor (host
-        or device); bc: its row bit counts.  The copy does not wait for other
-        streams, so the torch streams that write device tensors are
-        synchronized first."""
+        or device); bc: its row bit counts.  The copy does not wait for work
+        on other streams, so torch's current stream on a device tensor's
+        device is synchronized first (a table written on another stream must
+        be complete before the call)."""
         if isinstance(A, np.ndarray):
             A = np.ascontiguousarray(A).view(np.uint64)
             bc = np.ascontiguousarray(bc, dtype=np.uint32)
