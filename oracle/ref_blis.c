@@ -1,7 +1,7 @@
 /*
  * ref_blis.c -- the reference's stock fast CPU path, timed.
  *
- * BASELINE / TEST INFRASTRUCTURE ONLY.  oracle/Makefile links this file with
+ * CPU-BASELINE AND TEST INFRASTRUCTURE ONLY.  oracle/Makefile links this file with
  * the reference's unmodified gemm_cpu.c compiled as its `cblas_cpu_syrk`
  * target compiles it (-DCBLAS_USE -DSYRK, src/correlator/Makefile:31-39) and
  * with BLIS 0.1.8 configured for `binary_gemm` (the qLD-vendored BLIS, its

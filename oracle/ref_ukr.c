@@ -2,7 +2,7 @@
  * ref_ukr.c -- a BLIS-style blocked loop around the reference's own binary
  * GEMM micro-kernel bin_gemm_2x2 (blis/config/binary_gemm/kernels/3/bin_gemm.c:4-141).
  *
- * TEST / BASELINE INFRASTRUCTURE ONLY.  qLD's fast CPU path is BLIS 0.1.8's
+ * TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.  qLD's fast CPU path is BLIS 0.1.8's
  * dsyrk/dgemm with this micro-kernel plugged in (gemm_cpu.c:195-237).  The
  * BLIS framework itself is only buildable through BLIS's own configure/make,
  * so this file stands in for BLIS's blocking and packing around the
