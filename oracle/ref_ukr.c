@@ -3,13 +3,14 @@
  * GEMM micro-kernel bin_gemm_2x2 (blis/config/binary_gemm/kernels/3/bin_gemm.c:4-141).
  *
  * TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.  qLD's fast CPU path is BLIS 0.1.8's
- * dsyrk/dgemm with this micro-kernel plugged in (gemm_cpu.c:195-237).  The
- * BLIS framework itself is only buildable through BLIS's own configure/make,
- * so this file stands in for BLIS's blocking and packing around the
- * reference kernel, with the block sizes of the binary_gemm configuration
+ * dsyrk/dgemm with this micro-kernel plugged in (gemm_cpu.c:195-237), which
+ * oracle/Makefile builds from BLIS's sources (ref_blis.c times it).  This
+ * file is the stand-in bench.py falls back to, and says so, where that BLIS
+ * build is absent: BLIS's blocking and packing around the reference kernel,
+ * with the block sizes of the binary_gemm configuration
  * (blis/config/binary_gemm/bli_kernel.h:84-89: MC=72, KC=256, NC=4080,
  * MR=NR=2) and OpenMP threads over column blocks, as BLIS_JC_NT would split
- * them.  It is what bench.py times as the reference CPU path.
+ * them.
  *
  * Packing follows what the micro-kernel reads: an MR x KC micro-panel of A
  * stored k-major (a[ir + l*MR]), a KC x NR micro-panel of B stored the same
