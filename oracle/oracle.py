@@ -7,6 +7,9 @@ Thin ctypes/numpy layer over two libraries:
 * ``_ref/libqldref.so`` -- the reference's own functions compiled from the qLD
   sources (``gemm()``/``mlt()``/``get_pairwise_ld_score()``/``writeResults()``
   /``correlate()`` and the BLIS ``bin_gemm_2x2`` micro-kernel), see Makefile.
+* ``_ref/libqldref_blis.so`` -- the reference's stock ``-blis`` path:
+  ``blis_gemm()`` on BLIS 0.1.8 ``binary_gemm`` built from its sources, then
+  ``get_pairwise_ld_score()`` (``ref_blis_counts_ld``).
 
 Only tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
 this module.  The library under test never does.
