@@ -266,6 +266,29 @@ int qld_cuda_ld_band_device(qld_ctx *ctx, const uint64_t *A, const uint32_t *bcA
 int qld_cuda_ld_batch(qld_ctx *ctx, const qld_ld_args *jobs, int njobs, void *stream);
 
 /*
+ * A batched call captured once as a CUDA graph and replayed.
+ * qld_cuda_batch_plan checks and routes `jobs` exactly as qld_cuda_ld_batch()
+ * does, builds their tensor maps and device job table once, and captures the
+ * launch sequence (work-queue ticket reset, the persistent launch, the routed
+ * tasks' own launches) into an executable graph; nothing runs.
+ * qld_cuda_batch_run replays it on `stream` (NULL: the context's stream),
+ * asynchronously: collect with qld_cuda_sync() as after qld_cuda_ld_batch().
+ * The plan keeps the tasks' device pointers, so their tables, bit counts and
+ * outputs must stay allocated while it lives; each replay reads the tables
+ * as they are then (rewritten contents of the same shapes, e.g. resampled
+ * haplotypes, need no new plan).  The context options in force when the plan
+ * is made (r^2 mode, kernel choice, wait budget) hold for every replay.
+ * Replays of one plan run one after another whatever their streams.
+ * qld_cuda_batch_free waits for the plan's replays and frees it;
+ * qld_cuda_release frees the plans still alive.  qLD has no equivalent: an
+ * -inputList run re-reads and re-plans every task each time.
+ */
+typedef struct qld_batch_plan qld_batch_plan;
+int qld_cuda_batch_plan(qld_ctx *ctx, const qld_ld_args *jobs, int njobs, qld_batch_plan **plan);
+int qld_cuda_batch_run(qld_batch_plan *plan, void *stream);
+int qld_cuda_batch_free(qld_batch_plan *plan);
+
+/*
  * Serving: a request loop over chromosome tables resident in HBM.
  *
  * qld_srv_create starts a server on `device` with a device output pool of

@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes as ct
 import os
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -33,6 +34,7 @@ OPT_WAIT_CYCLES, OPT_MEM_CAP = 7, 8
 EXPORTED = (
     "qld_cuda_init", "qld_cuda_release", "qld_cuda_last_error", "qld_cuda_set_option",
     "qld_cuda_ld", "qld_cuda_ld_device", "qld_cuda_ld_hits", "qld_cuda_ld_batch",
+    "qld_cuda_batch_plan", "qld_cuda_batch_run", "qld_cuda_batch_free",
     "qld_cuda_ld_device_part", "qld_cuda_split_rows",
     "qld_cuda_count_states", "qld_cuda_count_states_device", "qld_cuda_vcf_pack",
     "qld_cuda_ld_band",
@@ -119,6 +121,9 @@ def load_library(path: str = LIB_PATH) -> ct.CDLL:
     lib.qld_cuda_ld.argtypes = [vp, vp, vp, i, vp, vp, i, i, i, i, vp, vp]
     lib.qld_cuda_ld_device.argtypes = [vp, ct.POINTER(_LdArgs), vp]
     lib.qld_cuda_ld_batch.argtypes = [vp, ct.POINTER(_LdArgs), i, vp]
+    lib.qld_cuda_batch_plan.argtypes = [vp, ct.POINTER(_LdArgs), i, ct.POINTER(vp)]
+    lib.qld_cuda_batch_run.argtypes = [vp, vp]
+    lib.qld_cuda_batch_free.argtypes = [vp]
     lib.qld_cuda_ld_device_part.argtypes = [vp, ct.POINTER(_LdArgs), i, i, ct.POINTER(i),
                                             ct.POINTER(i), vp]
     lib.qld_cuda_split_rows.argtypes = [i, i, i, i, i, i, i, ct.POINTER(i), ct.POINTER(i)]
@@ -172,9 +177,13 @@ class Context:
         self.h = h
         self.device = device
         self._pinned: dict[int, int] = {}
+        self._plans: weakref.WeakSet = weakref.WeakSet()
 
     def close(self):
         if getattr(self, "h", None):
+            for plan in list(self._plans):   # qld_cuda_release frees them
+                plan.h = None
+            self._plans.clear()
             for p in list(self._pinned):
                 self.lib.qld_cuda_host_free(self.h, ct.c_void_p(p))
             self._pinned.clear()
@@ -410,10 +419,8 @@ class Context:
                                                      ct.byref(r0), ct.byref(r1), _stream(stream)))
         return r0.value, r1.value
 
-    def ld_batch(self, jobs, stream=None):
-        """Enqueue many tasks in one launch.  `jobs`: sequence of dicts with
-        the ld_device keyword names (A, bcA, m, lda, B, bcB, n, ldb, K, S,
-        symmetric, r2, ldr, counts=None, ldc=0)."""
+    @staticmethod
+    def _ld_args(jobs):
         arr = (_LdArgs * len(jobs))()
         for i, j in enumerate(jobs):
             arr[i] = _LdArgs(_p(j["A"]), _p(j["bcA"]), int(j["m"]), int(j["lda"]),
@@ -421,7 +428,25 @@ class Context:
                              int(j.get("ldb", j["lda"])), int(j["K"]), int(j["S"]),
                              int(bool(j["symmetric"])), _p(j["r2"]), int(j["ldr"]),
                              _p(j.get("counts")), int(j.get("ldc", 0)))
+        return arr
+
+    def ld_batch(self, jobs, stream=None):
+        """Enqueue many tasks in one launch.  `jobs`: sequence of dicts with
+        the ld_device keyword names (A, bcA, m, lda, B, bcB, n, ldb, K, S,
+        symmetric, r2, ldr, counts=None, ldc=0)."""
+        arr = self._ld_args(jobs)
         self._check(self.lib.qld_cuda_ld_batch(self.h, arr, len(jobs), _stream(stream)))
+
+    def batch_plan(self, jobs) -> "BatchPlan":
+        """qld_cuda_batch_plan: the batched call over `jobs` (as ld_batch)
+        captured once as a CUDA graph; BatchPlan.run() replays it.  The jobs'
+        device tensors must outlive the plan."""
+        arr = self._ld_args(jobs)
+        h = ct.c_void_p()
+        self._check(self.lib.qld_cuda_batch_plan(self.h, arr, len(jobs), ct.byref(h)))
+        plan = BatchPlan(self, h)
+        self._plans.add(plan)
+        return plan
 
     def ld_band(self, A, bcA, *, S: int, band: int, r2_out=None, counts=False):
         """Windowed LD from host arrays: r2 (m, band), r2[i, d] = r^2(i, i+1+d)."""
@@ -447,6 +472,37 @@ class Context:
 
     def sync(self, stream=None):
         self._check(self.lib.qld_cuda_sync(self.h, _stream(stream)))
+
+
+class BatchPlan:
+    """A batched call captured as a CUDA graph (qld_cuda_batch_plan)."""
+
+    def __init__(self, ctx: Context, h):
+        self.ctx = ctx
+        self.h = h
+
+    def run(self, stream=None):
+        """Replay on `stream` (asynchronous: Context.sync collects it)."""
+        if not self.h:
+            raise QldError(ERR_INVALID, "batch plan is closed")
+        self.ctx._check(self.ctx.lib.qld_cuda_batch_run(self.h, _stream(stream)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.qld_cuda_batch_free(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def split_rows(m, n, K, symmetric, kernel, part, nparts):

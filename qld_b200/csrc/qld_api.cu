@@ -79,8 +79,23 @@ struct qld_ctx {
     DevBuf vText, vSites, vValid, vSlash, vRoff, vRnd, vScratch, vWords, vBc, vLen, vKeep, vErr;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
     size_t prof_used = 0;
+    bool capturing = false;           // a batch plan is being captured: no profiling events
+    std::vector<qld_batch_plan *> plans;   // live plans, freed by qld_cuda_release
     qld_stats stats{};
     PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+};
+
+// A batched call captured once: its device job table and ticket counter, and
+// the executable graph of its launch sequence.
+struct qld_batch_plan {
+    qld_ctx *ctx = nullptr;
+    BatchJob *d_jobs = nullptr;
+    unsigned long long *d_queue = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;   // null: the plan has no work
+    cudaEvent_t done = nullptr;       // recorded after every replay
+    long long counts_launches = 0, kernel_launches = 0;   // per replay
+    int last_kernel = 0;
 };
 
 namespace {
@@ -274,7 +289,7 @@ int band_rows_for(qld_ctx *c, const Task &t) {
 // (*end receives the closing event, recorded by the caller after the launch).
 int prof_begin(qld_ctx *c, cudaStream_t st, cudaEvent_t *end) {
     *end = nullptr;
-    if (!c->profile) return QLD_OK;
+    if (!c->profile || c->capturing) return QLD_OK;
     if (c->prof_used == c->prof.size()) {
         cudaEvent_t a, b;
         CUDA_TRY(c, cudaEventCreate(&a));
@@ -555,6 +570,160 @@ const KernelShape &split_shape(int variant) {
            : variant == QLD_KERNEL_MMA ? kMmaShape : kPopcShape;
 }
 
+// A batched task that runs as its own launch (not the 4-bit kernel, or past
+// 2^24 samples), with its outputs.
+struct RoutedTask {
+    Task t;
+    float *r2;
+    long long ldr;
+    uint32_t *counts;
+    long long ldc;
+};
+
+// The host half of a batched call: checks every task, routes it (the kernel
+// qld_cuda_ld_device would give it), and fills `hj` with the job table of the
+// 4-bit tasks -- tensor maps built, most expensive first so the queue ends on
+// small items -- and `routed` with the others.  `items` = output tiles of hj.
+int prepare_batch(qld_ctx *c, const qld_ld_args *jobs, int njobs, std::vector<BatchJob> &hj,
+                  std::vector<RoutedTask> &routed, long long &items) {
+    const KernelShape &ks = kBatchShape;
+    std::vector<long long> tiles(njobs), cost(njobs);
+    std::vector<int> order;
+    order.reserve(njobs);
+    routed.clear();
+    for (int j = 0; j < njobs; ++j) {
+        qld_ld_args a = jobs[j];
+        if (a.symmetric) { a.B = a.A; a.bcB = a.bcA; a.n = a.m; a.ldb = a.lda; }
+        if (a.m < 0 || a.n < 0 || a.K < 1 || a.S < 1 || a.lda < a.K || a.ldb < a.K ||
+            (a.lda & 1) || (a.ldb & 1) || a.ldr < a.m || (a.counts && a.ldc < a.m) || !a.A ||
+            !a.B || !a.bcA || !a.bcB || !a.r2 || !aligned16(a.A) || !aligned16(a.B))
+            return set_err(c, QLD_ERR_INVALID, "batch job %d: bad sizes, strides or pointers", j);
+        Task t{a.A, a.bcA, a.m, a.lda, a.B, a.bcB, a.n, a.ldb, a.K, a.S, a.symmetric, 0};
+        const int variant = variant_of(c, t);
+        if (!exact_for(variant, t))
+            return set_err(c, QLD_ERR_UNSUPPORTED,
+                           "batch job %d: the forced kernel is not exact for K*64 = %lld samples",
+                           j, (long long)a.K * 64);
+        tiles[j] = (a.m == 0 || a.n == 0) ? 0 : tile_count(t, ks.bm, ks.bn, 0, a.n);
+        if (variant != QLD_KERNEL_FP4 || (long long)a.K * 64 > kBatchMaxSamples) {
+            if (tiles[j] > 0) routed.push_back({t, a.r2, a.ldr, a.counts, a.ldc});
+            continue;
+        }
+        cost[j] = tiles[j] * (long long)a.K;
+        order.push_back(j);
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return cost[x] > cost[y]; });
+    const int nb = (int)order.size();
+    hj.resize(nb);
+    items = 0;
+    for (int i = 0; i < nb; ++i) {
+        const int j = order[i];
+        qld_ld_args a = jobs[j];
+        if (a.symmetric) { a.B = a.A; a.bcB = a.bcA; a.n = a.m; a.ldb = a.lda; }
+        BatchJob &J = hj[i];
+        memset(&J, 0, sizeof J);
+        J.bcA = a.bcA; J.bcB = a.bcB; J.r2 = a.r2; J.counts = a.counts;
+        J.ldr = a.ldr; J.ldc = a.ldc; J.item0 = items;
+        J.m = a.m; J.n = a.n; J.K = a.K; J.S = a.S; J.symmetric = a.symmetric;
+        if (tiles[j] > 0) {
+            int rc;
+            if ((rc = make_tmap(c, &J.tmA, a.A, a.m, a.K, a.lda, ks.box_words, ks.box_rows_a,
+                                ks.swizzle)) ||
+                (rc = make_tmap(c, &J.tmB, a.B, a.n, a.K, a.ldb, ks.box_words, ks.box_rows_b,
+                                ks.swizzle)))
+                return rc;
+        }
+        items += tiles[j];
+    }
+    return QLD_OK;
+}
+
+// The launch sequence of a batched call on `st`: ticket reset and the
+// persistent launch over the nb jobs at d_jobs (when they have items), then
+// the routed tasks' own launches.
+int enqueue_batch(qld_ctx *c, const BatchJob *d_jobs, int nb, long long items,
+                  unsigned long long *d_queue, const std::vector<RoutedTask> &routed,
+                  cudaStream_t st) {
+    int rc;
+    if (items > 0) {
+        CUDA_TRY(c, cudaMemsetAsync(d_queue, 0, sizeof(unsigned long long), st));
+        BatchParams bp{};
+        bp.jobs = d_jobs;
+        bp.njobs = nb;
+        bp.nitems = items;
+        bp.queue = d_queue;
+        bp.status = c->d_status;
+        bp.timeout_cycles = c->timeout_cycles;
+        cudaEvent_t e1 = nullptr;
+        if ((rc = prof_begin(c, st, &e1))) return rc;
+        cudaError_t e = launch_batch(bp, c->r2_mode, 0, st);
+        if (e != cudaSuccess)
+            return set_err(c, QLD_ERR_CUDA, "batched launch failed: %s", cudaGetErrorString(e));
+        if (e1) CUDA_TRY(c, cudaEventRecord(e1, st));
+        c->stats.counts_launches++;
+        c->stats.kernel_launches++;
+        c->stats.last_kernel = QLD_KERNEL_FP4;
+    }
+    for (const RoutedTask &r : routed)
+        if ((rc = launch_counts(c, r.t, 0, r.t.n, r.r2, r.ldr, r.counts, r.ldc, 0, st)))
+            return rc;
+    return QLD_OK;
+}
+
+void destroy_plan(qld_batch_plan *p) {
+    if (p->done) cudaEventSynchronize(p->done);   // replays still in flight
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->done) cudaEventDestroy(p->done);
+    if (p->d_jobs) cudaFree(p->d_jobs);
+    if (p->d_queue) cudaFree(p->d_queue);
+    delete p;
+}
+
+// Upload the plan's job table and capture its launch sequence (relaxed
+// capture mode: the launchers' attribute and occupancy queries are not
+// stream work) into an executable graph.  The capture's launches are not
+// counted in the statistics; every replay adds them.
+int build_plan(qld_ctx *c, qld_batch_plan *p, const std::vector<BatchJob> &hj, long long items,
+               const std::vector<RoutedTask> &routed) {
+    if (items == 0 && routed.empty()) return QLD_OK;
+    const size_t jb = sizeof(BatchJob) * (hj.empty() ? 1 : hj.size());
+    if (cudaMalloc(&p->d_jobs, jb) != cudaSuccess ||
+        cudaMalloc(&p->d_queue, sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, QLD_ERR_NOMEM, "batch plan: cudaMalloc of the job table failed");
+    }
+    if (!hj.empty())
+        CUDA_TRY(c, cudaMemcpy(p->d_jobs, hj.data(), sizeof(BatchJob) * hj.size(),
+                               cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming));
+    cudaStream_t cs = nullptr;
+    CUDA_TRY(c, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    const qld_stats saved = c->stats;
+    int rc = QLD_OK;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+    if (e == cudaSuccess) {
+        c->capturing = true;
+        rc = enqueue_batch(c, p->d_jobs, (int)hj.size(), items, p->d_queue, routed, cs);
+        c->capturing = false;
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(cs, &g);   // ends the capture on every path
+        p->graph = g;
+    }
+    p->counts_launches = c->stats.counts_launches - saved.counts_launches;
+    p->kernel_launches = c->stats.kernel_launches - saved.kernel_launches;
+    p->last_kernel = c->stats.last_kernel;
+    c->stats = saved;
+    cudaStreamDestroy(cs);
+    if (rc) return rc;
+    if (e != cudaSuccess || !p->graph)
+        return set_err(c, QLD_ERR_CUDA, "batch plan: stream capture failed: %s",
+                       cudaGetErrorString(e));
+    CUDA_TRY(c, cudaGraphInstantiate(&p->exec, p->graph, 0));
+    return QLD_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -617,6 +786,8 @@ int qld_cuda_release(qld_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->copy) cudaStreamSynchronize(c->copy);
     if (c->h2d) cudaStreamSynchronize(c->h2d);
+    for (qld_batch_plan *p : c->plans) destroy_plan(p);
+    c->plans.clear();
     for (cudaEvent_t e : c->h2d_ev) cudaEventDestroy(e);
     DevBuf *bufs[] = {&c->dA,       &c->dB,       &c->dbcA,     &c->dbcB,     &c->dOut[0],
                       &c->dOut[1],  &c->dCnt[0],  &c->dCnt[1],  &c->dJobs,    &c->dQueue,
@@ -1224,93 +1395,70 @@ int qld_cuda_ld_batch(qld_ctx *c, const qld_ld_args *jobs, int njobs, void *stre
     if (!c || (njobs > 0 && !jobs) || njobs < 0) return QLD_ERR_INVALID;
     if (njobs == 0) return QLD_OK;
     CUDA_TRY(c, cudaSetDevice(c->device));
-    const KernelShape &ks = kBatchShape;
-    std::vector<long long> tiles(njobs), cost(njobs);
-    std::vector<int> order;
-    std::vector<Task> routed;
-    std::vector<int> routed_job;
-    order.reserve(njobs);
-    for (int j = 0; j < njobs; ++j) {
-        qld_ld_args a = jobs[j];
-        if (a.symmetric) { a.B = a.A; a.bcB = a.bcA; a.n = a.m; a.ldb = a.lda; }
-        if (a.m < 0 || a.n < 0 || a.K < 1 || a.S < 1 || a.lda < a.K || a.ldb < a.K ||
-            (a.lda & 1) || (a.ldb & 1) || a.ldr < a.m || (a.counts && a.ldc < a.m) || !a.A ||
-            !a.B || !a.bcA || !a.bcB || !a.r2 || !aligned16(a.A) || !aligned16(a.B))
-            return set_err(c, QLD_ERR_INVALID, "batch job %d: bad sizes, strides or pointers", j);
-        Task t{a.A, a.bcA, a.m, a.lda, a.B, a.bcB, a.n, a.ldb, a.K, a.S, a.symmetric, 0};
-        const int variant = variant_of(c, t);
-        if (!exact_for(variant, t))
-            return set_err(c, QLD_ERR_UNSUPPORTED,
-                           "batch job %d: the forced kernel is not exact for K*64 = %lld samples",
-                           j, (long long)a.K * 64);
-        tiles[j] = (a.m == 0 || a.n == 0) ? 0 : tile_count(t, ks.bm, ks.bn, 0, a.n);
-        if (variant != QLD_KERNEL_FP4 || (long long)a.K * 64 > kBatchMaxSamples) {
-            if (tiles[j] > 0) {
-                routed.push_back(t);
-                routed_job.push_back(j);
-            }
-            continue;
-        }
-        cost[j] = tiles[j] * (long long)a.K;
-        order.push_back(j);
-    }
-    // Most expensive tasks first, so the queue ends on small items.
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int x, int y) { return cost[x] > cost[y]; });
-    const int nb = (int)order.size();
-    c->hJobs.resize(nb > 0 ? nb : 1);
+    std::vector<RoutedTask> routed;
     long long items = 0;
-    for (int i = 0; i < nb; ++i) {
-        const int j = order[i];
-        qld_ld_args a = jobs[j];
-        if (a.symmetric) { a.B = a.A; a.bcB = a.bcA; a.n = a.m; a.ldb = a.lda; }
-        BatchJob &J = c->hJobs[i];
-        memset(&J, 0, sizeof J);
-        J.bcA = a.bcA; J.bcB = a.bcB; J.r2 = a.r2; J.counts = a.counts;
-        J.ldr = a.ldr; J.ldc = a.ldc; J.item0 = items;
-        J.m = a.m; J.n = a.n; J.K = a.K; J.S = a.S; J.symmetric = a.symmetric;
-        if (tiles[j] > 0) {
-            int rc;
-            if ((rc = make_tmap(c, &J.tmA, a.A, a.m, a.K, a.lda, ks.box_words, ks.box_rows_a,
-                                ks.swizzle)) ||
-                (rc = make_tmap(c, &J.tmB, a.B, a.n, a.K, a.ldb, ks.box_words, ks.box_rows_b,
-                                ks.swizzle)))
-                return rc;
-        }
-        items += tiles[j];
-    }
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     int rc;
+    if ((rc = prepare_batch(c, jobs, njobs, c->hJobs, routed, items))) return rc;
+    const int nb = (int)c->hJobs.size();
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     if (items > 0) {
         if ((rc = ensure(c, c->dJobs, sizeof(BatchJob) * (size_t)nb)) ||
             (rc = ensure(c, c->dQueue, sizeof(unsigned long long))))
             return rc;
         CUDA_TRY(c, cudaMemcpyAsync(c->dJobs.p, c->hJobs.data(), sizeof(BatchJob) * (size_t)nb,
                                     cudaMemcpyHostToDevice, st));
-        CUDA_TRY(c, cudaMemsetAsync(c->dQueue.p, 0, sizeof(unsigned long long), st));
-        BatchParams bp{};
-        bp.jobs = static_cast<const BatchJob *>(c->dJobs.p);
-        bp.njobs = nb;
-        bp.nitems = items;
-        bp.queue = static_cast<unsigned long long *>(c->dQueue.p);
-        bp.status = c->d_status;
-        bp.timeout_cycles = c->timeout_cycles;
-        cudaEvent_t e1 = nullptr;
-        if ((rc = prof_begin(c, st, &e1))) return rc;
-        cudaError_t e = launch_batch(bp, c->r2_mode, 0, st);
-        if (e != cudaSuccess)
-            return set_err(c, QLD_ERR_CUDA, "batched launch failed: %s", cudaGetErrorString(e));
-        if (e1) CUDA_TRY(c, cudaEventRecord(e1, st));
-        c->stats.counts_launches++;
-        c->stats.kernel_launches++;
-        c->stats.last_kernel = QLD_KERNEL_FP4;
     }
-    for (size_t i = 0; i < routed.size(); ++i) {
-        const qld_ld_args &a = jobs[routed_job[i]];
-        if ((rc = launch_counts(c, routed[i], 0, routed[i].n, a.r2, a.ldr, a.counts, a.ldc, 0,
-                                st)))
-            return rc;
+    return enqueue_batch(c, static_cast<const BatchJob *>(c->dJobs.p), nb, items,
+                         static_cast<unsigned long long *>(c->dQueue.p), routed, st);
+}
+
+int qld_cuda_batch_plan(qld_ctx *c, const qld_ld_args *jobs, int njobs, qld_batch_plan **out) {
+    if (!c || !out || (njobs > 0 && !jobs) || njobs < 0) return QLD_ERR_INVALID;
+    *out = nullptr;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    std::vector<BatchJob> hj;
+    std::vector<RoutedTask> routed;
+    long long items = 0;
+    int rc;
+    if ((rc = prepare_batch(c, jobs, njobs, hj, routed, items))) return rc;
+    qld_batch_plan *p = new (std::nothrow) qld_batch_plan();
+    if (!p) return set_err(c, QLD_ERR_NOMEM, "batch plan: out of host memory");
+    p->ctx = c;
+    if ((rc = build_plan(c, p, hj, items, routed))) {
+        destroy_plan(p);
+        return rc;
     }
+    c->plans.push_back(p);
+    *out = p;
+    return QLD_OK;
+}
+
+int qld_cuda_batch_run(qld_batch_plan *p, void *stream) {
+    if (!p || !p->ctx) return QLD_ERR_INVALID;
+    qld_ctx *c = p->ctx;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    if (!p->exec) return QLD_OK;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    cudaEvent_t e1 = nullptr;
+    int rc;
+    if ((rc = prof_begin(c, st, &e1))) return rc;
+    CUDA_TRY(c, cudaGraphLaunch(p->exec, st));
+    if (e1) CUDA_TRY(c, cudaEventRecord(e1, st));
+    CUDA_TRY(c, cudaEventRecord(p->done, st));
+    c->stats.counts_launches += p->counts_launches;
+    c->stats.kernel_launches += p->kernel_launches;
+    c->stats.last_kernel = p->last_kernel;
+    return QLD_OK;
+}
+
+int qld_cuda_batch_free(qld_batch_plan *p) {
+    if (!p) return QLD_OK;
+    qld_ctx *c = p->ctx;
+    if (c) {
+        c->plans.erase(std::remove(c->plans.begin(), c->plans.end(), p), c->plans.end());
+        cudaSetDevice(c->device);
+    }
+    destroy_plan(p);
     return QLD_OK;
 }
 
