@@ -257,6 +257,37 @@ def kernel_roofline(ctx, variant, bitops, kern_ms, dev, int8_context=True):
             "peak_source": "measured: qld_cuda_measure_popc_peak (register-only AND+POPC)"}
 
 
+def pair_tiles(m, n, symmetric, bm=256, bn=240):
+    """Output tiles of the SM-pair 4-bit kernel for one task (its tile list:
+    every bm x bn tile of A rows x B rows, in a single region those holding a
+    pair a >= b)."""
+    ta, tb = -(-m // bm), -(-n // bn)
+    if not symmetric:
+        return ta * tb
+    return sum(min((bm * a + bm - 1) // bn, tb - 1) + 1 for a in range(ta))
+
+
+def smem_roofline(m, n, K, symmetric, kern_ms, sm_mhz, sms=148):
+    """Shared-memory roofline of the SM-pair 4-bit kernel: per CTA and
+    256-sample stage its 248 rows (128 A + 120 B) each take 32 B of TMA
+    writes (packed words), 32 B of unpack reads, 128 B of E2M1 stores and
+    128 B of tensor-core operand reads -- 320 B per row, the minimum of this
+    layout -- over two CTAs per tile and 2 * ceil(K / 8) stages per tile;
+    against 128 B per clock per SM at the sampled SM clock (nominal)."""
+    if not kern_ms or not sm_mhz:
+        return None
+    stages = 2 * (-(-K // 8))
+    nbytes = 2 * pair_tiles(m, n, symmetric) * stages * 248 * 320
+    achieved = nbytes / (kern_ms * 1e-3) / 1e12
+    peak = sms * 128 * sm_mhz * 1e6 / 1e12
+    return {"bytes_per_launch": nbytes, "achieved": achieved, "peak": peak, "unit": "TB/s",
+            "frac": achieved / peak,
+            "peak_source": "nominal: 128 B/clk per SM x %d SMs at the sampled %.0f MHz" %
+                           (sms, sm_mhz),
+            "per_stage": "per CTA and 256-sample stage: 248 rows x (32 B TMA + 32 B unpack "
+                         "read + 128 B E2M1 store + 128 B tensor-core read)"}
+
+
 def measured_traffic(variant, workload, sm_pair=0, r2_mode="exact"):
     """DRAM bytes per launch of the counts kernel from the ncu capture
     summarised under profiles/ (None when no capture covers this case).
@@ -552,7 +583,7 @@ def ours_arm(args, rank, world, local_rank):
     import numpy as np
     import torch
 
-    from qld_b200 import synth
+    from qld_b200 import api, synth
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -625,6 +656,8 @@ def ours_arm(args, rank, world, local_rank):
     roof["hbm_frac_of_measured"] = (alg_bytes / (kern_ms * 1e-3) / 1e9) / mp["hbm_gbs"]
     roof["hbm_peak_gbs"] = mp["hbm_gbs"]
     roof["hbm_peak_source"] = mp["source"]
+    if variant == api.KERNEL_FP4 and sm_pair in (0, 2) and not split and K * 64 <= 1 << 24:
+        roof["shared_memory"] = smem_roofline(m, m, K, True, kern_ms, clocks.get("sm_mhz"))
 
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
@@ -701,6 +734,7 @@ def section_reference_mode(args, Tp, bc, m, lda, K, S, out, flush, st, local_ran
     """The headline region with r^2 in QLD_R2_REFERENCE mode (bit-identical to
     qLD-compute's get_pairwise_ld_score; the drop-in's default), automatic
     kernel choice."""
+    from qld_b200 import api
     ctx = new_context(local_rank, args, r2_mode="reference")
 
     def step():
@@ -718,6 +752,9 @@ def section_reference_mode(args, Tp, bc, m, lda, K, S, out, flush, st, local_ran
            "roofline": dict(kernel_roofline(ctx, stats.last_kernel, pairs * 64 * K, kern_ms,
                                             None, int8_context=False), kernel_ms=kern_ms),
            "clocks": clocks}
+    if stats.last_kernel == api.KERNEL_FP4 and args.sm_pair in (0, 2):
+        res["roofline"]["shared_memory"] = smem_roofline(m, m, K, True, kern_ms,
+                                                         clocks.get("sm_mhz"))
     if not args.no_parity:
         res["parity"] = region_parity(ctx, Tp, bc, m, lda, K, S, out, st, "reference", seed=12)
     ctx.close()

@@ -62,3 +62,15 @@ def test_band_pair_count():
 def test_host_cpu_reports_cores():
     model, phys, logical = bench.host_cpu()
     assert 1 <= phys <= logical and isinstance(model, str)
+
+
+def test_pair_tiles_and_shared_memory_roofline():
+    # the kernel's tile list: 7,419 tiles on the 29,817-SNP region, 579 on 8,192
+    assert bench.pair_tiles(29817, 29817, True) == 7419
+    assert bench.pair_tiles(8192, 8192, True) == 579
+    assert bench.pair_tiles(300, 500, False) == 2 * 3
+    r = bench.smem_roofline(29817, 29817, 260, True, 2.415, 1965.0)
+    assert r["bytes_per_launch"] == 2 * 7419 * 66 * 248 * 320
+    assert abs(r["peak"] - 148 * 128 * 1965e6 / 1e12) < 1e-9
+    assert 0.8 < r["frac"] < 0.9
+    assert bench.smem_roofline(100, 100, 4, True, 0.0, 1965.0) is None
