@@ -409,6 +409,55 @@ def cpu_reference_rate(T_np, S, seconds_target=8.0, factoring=None, ms=None):
     return ms * (ms - 1) / 2 / t, threads, desc, kind
 
 
+_FACTORING = {}   # the headline's best (JC, IC) BLIS split, reused by the sections
+
+
+def cpu_reference_tasks(tasks):
+    """The reference's stock -blis path over `tasks`, each (A, B or None, S)
+    host tables: per task BLIS cblas_dsyrk (B None: a single region) or
+    cblas_dgemm counts, then get_pairwise_ld_score on one thread, one task
+    after another as an -inputList run does.  Bit counts are made before the
+    clock starts (qLD makes them while loading).  Returns (seconds, threads,
+    path)."""
+    oracle = _oracle()
+    _, phys, logical = host_cpu()
+    prepared = [(A, oracle.bitcounts(A), B, None if B is None else oracle.bitcounts(B), S)
+                for A, B, S in tasks]
+    total = 0.0
+    if oracle.blis_available():
+        jc, ic = _FACTORING.get("blis", (1, phys))
+        _blis_threads(jc, ic)
+        for A, bcA, B, bcB, S in prepared:
+            _, _, tg, tl = oracle.ref_blis_counts_ld(A, bcA, S, B=B, bcB=bcB)
+            total += tg + tl
+        return total, jc * ic, (f"qLD-compute -blis path per task: BLIS 0.1.8 binary_gemm "
+                                f"cblas_dsyrk / cblas_dgemm (BLIS_JC_NT={jc}, BLIS_IC_NT={ic}) + "
+                                f"get_pairwise_ld_score (1 thread)")
+    for A, bcA, B, bcB, S in prepared:
+        t0 = time.perf_counter()
+        C = oracle.ref_counts_ukr(A, B, lower_only=B is None, threads=logical)
+        oracle.ref_ld_score(bcA, bcA if B is None else bcB, C, S, threads=1)
+        total += time.perf_counter() - t0
+    return total, logical, ("stand-in (BLIS not built): bin_gemm_2x2 in a BLIS-style loop + "
+                            "get_pairwise_ld_score (1 thread)")
+
+
+def cpu_sampled_baseline(make_tasks, sizes, seconds_target=6.0):
+    """cpu_baseline of a section: make_tasks(size) -> (tasks, pairs, description)
+    for a growing sample size; the first size is a probe whose time sets the
+    final size (time taken as proportional to size, capped at sizes[1])."""
+    model, phys, _ = host_cpu()
+    probe, cap = sizes
+    tasks, pairs, _ = make_tasks(probe)
+    t, _, _ = cpu_reference_tasks(tasks)
+    size = max(probe, min(cap, int(probe * seconds_target / max(t, 1e-3))))
+    tasks, pairs, desc = make_tasks(size)
+    t, threads, path = cpu_reference_tasks(tasks)
+    return {"value": pairs / t, "unit": "pairs/s", "cores": threads, "kind": "reference",
+            "path": path, "sample": f"{desc}: {pairs} pairs in {t:.2f} s; {model}, "
+                                    f"{phys} physical cores"}
+
+
 def best_blis_factoring(T_np, S):
     """The fastest (JC, IC) split of the host's physical cores for the counts,
     tried on a small sample (the reference's README leaves BLIS threading to
@@ -706,6 +755,8 @@ def ours_arm(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu:
         T_np = T.cpu().numpy().view(np.uint64)
         fac = best_blis_factoring(T_np, S)
+        if fac:
+            _FACTORING["blis"] = fac
         v, cores, desc, kind = cpu_reference_rate(T_np, S, factoring=fac)
         line["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": cores, "kind": "reference",
                                 "path": kind, "sample": desc}
@@ -900,6 +951,19 @@ def section_windowed(args, local_rank, flush, m_full=None):
                       "d2h_bytes_per_step": m * W * 4,
                       "api": "qld_cuda_ld_band (pinned host buffers, streamed)"}
         del Th, bch, outh
+    if not args.no_cpu:
+        b0 = (m // 2) // 256 * 256
+
+        def tasks(nb):
+            # one rectangle of a split_region-style tiling of the band: B rows
+            # [b0, b0 + nb) against the A rows [b0 + 1, b0 + nb - 1 + W] their
+            # band pairs need; nb * W band pairs
+            A = T[b0 + 1:b0 + nb + W].cpu().numpy().view(np.uint64)
+            B = T[b0:b0 + nb].cpu().numpy().view(np.uint64)
+            return ([(A, B, S)], nb * W,
+                    f"one band tile: B rows [{b0}, {b0 + nb}) x A rows [{b0 + 1}, "
+                    f"{b0 + nb + W - 1}] (rectangle computed whole, band pairs counted)")
+        res["cpu_baseline"] = cpu_sampled_baseline(tasks, (128, 8192))
     ctx.close()
     return res
 
@@ -1053,6 +1117,24 @@ def section_batched(args, local_rank, flush):
     if not args.no_parity:
         # the graph replay ran last: its outputs are what the jobs hold now
         out["parity"] = batch_parity(jobs, seed=15, mode=args.r2_mode)
+    if not args.no_cpu:
+        import numpy as np
+
+        def host(t, rows, K):
+            return np.ascontiguousarray(t[:rows, :K].cpu().numpy().view(np.uint64))
+
+        def tasks(count):
+            # every (njobs // count)-th job, as one -inputList task each
+            stride = max(1, len(jobs) // count)
+            picked = jobs[::stride]
+            ts, p = [], 0
+            for j in picked:
+                A = host(j["A"], j["m"], j["K"])
+                B = None if j["symmetric"] else host(j["B"], j["n"], j["K"])
+                ts.append((A, B, j["S"]))
+                p += j["m"] * (j["m"] - 1) // 2 if j["symmetric"] else j["m"] * j["n"]
+            return ts, p, f"every {stride}th of the {len(jobs)} tasks ({len(picked)} tasks)"
+        out["cpu_baseline"] = cpu_sampled_baseline(tasks, (16, len(jobs)))
     ctx.close()
     del jobs
     return out
@@ -1199,6 +1281,26 @@ def section_served(args, local_rank, flush=None, check_queries=12):
         par["sample"] = (f"{check_queries} more queries from the same distribution: 3 B rows "
                          "of each r2 block x all its A rows; device summaries vs the block")
         out["parity"] = par
+    if not args.no_cpu:
+        qrng = np.random.default_rng(6)
+        cpu_qs = []
+        for _ in range(64):   # queries from the same distribution, their own draw
+            c = int(qrng.integers(0, 22))
+            la, lb = (int(x) for x in qrng.integers(100, 20_001, 2))
+            a0 = int(qrng.integers(0, sizes[c] - la + 1))
+            b0 = int(qrng.integers(0, sizes[c] - lb + 1))
+            cpu_qs.append((c, a0, a0 + la, b0, b0 + lb))
+
+        def tasks(count):
+            ts, p = [], 0
+            for c, a0, a1, b0, b1 in cpu_qs[:count]:
+                T = tables[c][0]
+                A = T[a0:a1].cpu().numpy().view(np.uint64)
+                B = T[b0:b1].cpu().numpy().view(np.uint64)
+                ts.append((A, B, H))
+                p += (a1 - a0) * (b1 - b0)
+            return ts, p, f"{count} queries of the same distribution, one task each"
+        out["cpu_baseline"] = cpu_sampled_baseline(tasks, (2, 64))
     srv.close()
     del tables
     return out

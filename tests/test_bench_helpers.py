@@ -74,3 +74,19 @@ def test_pair_tiles_and_shared_memory_roofline():
     assert abs(r["peak"] - 148 * 128 * 1965e6 / 1e12) < 1e-9
     assert 0.8 < r["frac"] < 0.9
     assert bench.smem_roofline(100, 100, 4, True, 0.0, 1965.0) is None
+
+
+def test_sampled_cpu_baseline_runs_the_reference_path():
+    import numpy as np
+    rng = np.random.default_rng(3)
+    T = rng.integers(0, 2 ** 63, size=(300, 5), dtype=np.int64).view(np.uint64)
+    calls = []
+
+    def tasks(size):
+        calls.append(size)
+        return [(T[:size], None, 300), (T[:size], T[size:2 * size], 300)], \
+            size * (size - 1) // 2 + size * size, f"{size} rows"
+    r = bench.cpu_sampled_baseline(tasks, (20, 100), seconds_target=0.01)
+    assert calls[0] == 20 and 20 <= calls[1] <= 100
+    assert r["kind"] == "reference" and r["value"] > 0 and r["cores"] >= 1
+    assert r["sample"].startswith(f"{calls[1]} rows")
