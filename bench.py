@@ -115,7 +115,7 @@ def arm_config(args, world):
     """The `config` of the headline line; both arms print the same dict."""
     cfg = workload_config(args.workload)
     cfg["parallelism"] = (f"tile-row split x{world} (one region, no collective)"
-                          if args.split and world > 1 else
+                          if args.split else
                           f"replicas x{world} (independent regions, no collective)")
     cfg["l2"] = "512 MB flush write between timed steps"
     if args.snps:
@@ -638,7 +638,7 @@ def ours_arm(args, rank, world, local_rank):
     torch.cuda.set_device(dev)
     cfg = arm_config(args, world)
 
-    split = args.split and world > 1
+    split = args.split   # at N = 1 a one-part split: the same path over the whole region
     T, S = make_table(args.workload, dev, seed_offset=0 if split else rank)
     if args.snps:
         T = T[:args.snps].contiguous()

@@ -158,10 +158,16 @@ __device__ __forceinline__ float pair_r2_exact(uint32_t cnt, const ARow &ra, con
 // Exact zeros need no test: a zero row's factors are 0, so q = 0.
 // The earlier FP64 form (Newton reciprocal of den from rcp.approx.f64 with a
 // rounding test in FP64) spent its time in FP64 conversions and the MUFU.
+// fl32(cab / S) for integer cab <= S <= 2^24 (exact in FP32), by Markstein's
+// correction of RN(cab * RN(1/S)): the correctly rounded quotient.
+__device__ __forceinline__ float ref_quotient_ff(float cab, const ARowR &A) {
+    const float q0 = __fmul_rn(cab, A.rSf);
+    return __fmaf_rn(__fmaf_rn(-q0, A.Sf, cab), A.rSf, q0);
+}
+
 __device__ __forceinline__ float r2_reference_ff(float cab, const ARowR &A, float4 B,
                                                  bool &redo) {
-    const float q0 = __fmul_rn(cab, A.rSf);
-    const float v3 = __fmaf_rn(__fmaf_rn(-q0, A.Sf, cab), A.rSf, q0);
+    const float v3 = ref_quotient_ff(cab, A);
     const float p12 = __fmul_rn(A.k.x, B.x);
     const float e = __fmaf_rn(A.k.x, B.x, -p12);
     const float d = __fsub_rn(v3, p12);
@@ -188,14 +194,16 @@ __device__ __forceinline__ float r2_reference_ff(float cab, const ARowR &A, floa
 // default NaN 0xFFC00000 (gemm_cpu.c:363-389); that needs x alone, with the
 // reference's float rounding, and no FP64 division.  Empty SNPs keep the
 // zero rule; bit counts above S and the rare rounding cases run the literal
-// sequence.
+// sequence.  q = fl32((float)cab / S), the reference's v3.
+__device__ __forceinline__ float r2_fixed(float q, float vA, float vB) {
+    const float d = __fsub_rn(q, __fmul_rn(vA, vB));
+    return __fmul_rn(d, d) == 0.0f ? __uint_as_float(0xFFC00000u) : 123.456f;
+}
+
 __device__ __forceinline__ float r2_flagged(uint32_t cab, const RowRef &A, const RowRef &B,
-                                            int S) {
+                                            int S, float q) {
     if (A.v == 0.0f || B.v == 0.0f) return 0.0f;
-    if (A.v <= 1.0f && B.v <= 1.0f && (A.v == 1.0f || B.v == 1.0f)) {
-        const float d = __fsub_rn(__fdiv_rn((float)cab, (float)S), __fmul_rn(A.v, B.v));
-        return __fmul_rn(d, d) == 0.0f ? __uint_as_float(0xFFC00000u) : 123.456f;
-    }
+    if (A.v <= 1.0f && B.v <= 1.0f && (A.v == 1.0f || B.v == 1.0f)) return r2_fixed(q, A.v, B.v);
     return r2_reference(cab, A, B, S);
 }
 
@@ -235,21 +243,43 @@ __device__ __forceinline__ void chunk_ref(uint32_t (&v)[CW], const ARowR &ra, co
     }
     if (!a_ok) redo = 0;
     if (__any_sync(0xffffffffu, redo != 0)) {
-        RowRef rA;
-        rA.c = ra.c;
-        rA.v = ra.k.x;
-        rA.one_minus = __dsub_rn(1.0, (double)ra.k.x);
+        // A lane whose A row is a fixed SNP (v = 1) has all its pairs flagged:
+        // they take r2_flagged's fixed-SNP rule here in one pass, with
+        // r2_reference_ff's quotient, instead of one trip each through the
+        // warp-wide loop below (columns with bit counts above S stay flagged).
+        const bool a_fixed = S <= (1 << 24) && ra.k.x == 1.0f && redo != 0u;
+        if (__any_sync(0xffffffffu, a_fixed) && a_fixed) {
 #pragma unroll
-        for (int t = 0; t < CW; ++t) {
-            const bool rd = (redo >> t) & 1u;
-            if (__any_sync(0xffffffffu, rd) && rd) {
-                const float4 cb = f.f[bl0 + t];
-                RowRef rb;
-                rb.c = cb.x != 0.0f;        // only the zero rule reads it
-                rb.v = cb.x;
-                rb.one_minus = __dsub_rn(1.0, (double)cb.x);
-                const uint32_t cnt = FLOATCNT ? (uint32_t)__uint_as_float(v[t]) : v[t] >> SHIFT;
-                v[t] = __float_as_uint(r2_flagged(cnt, rA, rb, S));
+            for (int t = 0; t < CW; ++t) {
+                const float vb = f.f[bl0 + t].x;
+                if (((redo >> t) & 1u) && vb <= 1.0f) {
+                    const float cf = FLOATCNT ? __uint_as_float(v[t]) : (float)(v[t] >> SHIFT);
+                    v[t] = __float_as_uint(
+                        vb == 0.0f ? 0.0f : r2_fixed(ref_quotient_ff(cf, ra), 1.0f, vb));
+                    redo &= ~(1u << t);
+                }
+            }
+        }
+        if (__any_sync(0xffffffffu, redo != 0)) {
+            RowRef rA;
+            rA.c = ra.c;
+            rA.v = ra.k.x;
+            rA.one_minus = __dsub_rn(1.0, (double)ra.k.x);
+#pragma unroll
+            for (int t = 0; t < CW; ++t) {
+                const bool rd = (redo >> t) & 1u;
+                if (__any_sync(0xffffffffu, rd) && rd) {
+                    const float4 cb = f.f[bl0 + t];
+                    RowRef rb;
+                    rb.c = cb.x != 0.0f;        // only the zero rule reads it
+                    rb.v = cb.x;
+                    rb.one_minus = __dsub_rn(1.0, (double)cb.x);
+                    const uint32_t cnt =
+                        FLOATCNT ? (uint32_t)__uint_as_float(v[t]) : v[t] >> SHIFT;
+                    const float q = S <= (1 << 24) ? ref_quotient_ff((float)cnt, ra)
+                                                   : __fdiv_rn((float)cnt, (float)S);
+                    v[t] = __float_as_uint(r2_flagged(cnt, rA, rb, S, q));
+                }
             }
         }
     }

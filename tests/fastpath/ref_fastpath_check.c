@@ -65,10 +65,11 @@ static float ff_r2(uint32_t cab, uint32_t ca, uint32_t cb, int S) {
     if (redo) {
         if (!(A.v > 0 && A.v < 1 && B.v > 0 && B.v < 1)) ++fb_spec; else if (tiny) ++fb_tiny; else ++fb_amb;
         ++fallbacks;
-        /* the device's r2_flagged: zero rule, fixed SNP (v = 1: den = +0), else the sequence */
+        /* the device's r2_flagged (and chunk_ref's pass over fixed A rows): zero rule,
+         * fixed SNP (v = 1: den = +0) from the fast path's quotient v3, else the sequence */
         if (A.v == 0.0f || B.v == 0.0f) r = 0.0f;
         else if (A.v <= 1.0f && B.v <= 1.0f && (A.v == 1.0f || B.v == 1.0f)) {
-            volatile float q = (float)cab / (float)S, p = A.v * B.v;
+            volatile float q = v3, p = A.v * B.v;
             volatile float dd = q - p, xx = dd * dd;
             r = xx == 0.0f ? b2f(0xFFC00000u) : 123.456f;
         } else r = ref_r2(cab, ca, cb, S);

@@ -56,3 +56,23 @@ def test_parts_equal_the_whole_task(gpu_ctx, kernel, m, n, N, sym, nparts):
     assert np.array_equal(wcnt.cpu().numpy()[mask], scnt.cpu().numpy()[mask])
     want = oracle.counts(T[:m], None if sym else T[m:])
     assert np.array_equal(scnt.cpu().numpy().view(np.uint32)[mask], want[mask])
+
+
+def test_bench_split_path_runs_at_one_gpu():
+    """bench.py --split at N = 1 runs the split path (qld_cuda_ld_device_part,
+    one part) over the whole region and reports it as such."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--split", "--snps",
+                          "4096", "--steps", "2", "--warmup", "1", "--no-e2e", "--no-cpu",
+                          "--no-parity", "--sections", "none"],
+                         capture_output=True, text=True, timeout=600, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads([ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1])
+    assert line["split_rows"] == [0, 4096]
+    assert line["scaling"] == "strong" and line["value"] > 0
+    assert line["config"]["parallelism"].startswith("tile-row split x1")
+    assert line["gpu_launches"] >= 2
