@@ -354,7 +354,7 @@ k_ld_batch(const BatchParams bp) {
         const int et = tid - FIRST_EPI_WARP * 32;
         const int ew = warp - FIRST_EPI_WARP;
         const int q = warp & 3;             // TMEM lane quarter
-        const int colh = ew >> 2;           // chunks colh, colh + 2, colh + 4, colh + 6
+        const int colh = ew >> 2;           // chunks colh, colh + 2, ...
         if (et == 0) *epi_fail = 0;
         named_bar_sync(1, EPI_THREADS);
         for (int qi = 0;; ++qi) {
@@ -394,7 +394,8 @@ k_ld_batch(const BatchParams bp) {
                 const epi::ARowF raf = epi::make_arow_f32(ca, J.S);
                 const uint32_t tbase =
                     tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)ab * ACC_STRIDE;
-                // columns past the tile's 240 B rows are read but not written
+                // columns of the last 32-column chunk past the tile's 240 B rows
+                // are read but not written
                 const int n_tile = it.tb * BN + BN < J.n ? it.tb * BN + BN : J.n;
                 const int dlo = diag_lo(J.symmetric, 0), dhi = diag_hi(0);
                 epi::SumAcc acc;
@@ -403,7 +404,7 @@ k_ld_batch(const BatchParams bp) {
                 // 199 ms on the 4,096-task mix; exact mode: 70.5 against 71.7 ms)
                 constexpr int CW = MODE == R2_EXACT ? 32 : 16;
 #pragma unroll 1
-                for (int c = colh; c < 256 / CW; c += 2) {
+                for (int c = colh; c < (BN + CW - 1) / CW; c += 2) {   // the tile's chunks
                     uint32_t v[CW];
                     __syncwarp();
                     tc_ld_32x32b<CW>(tbase + (uint32_t)(c * CW), v);

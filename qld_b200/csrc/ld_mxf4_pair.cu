@@ -32,8 +32,8 @@
 //                reference r^2); six, at the 80 registers 22 warps leave, 4 %
 //                slower.
 //   warps 12-19  epilogue: warp w reads TMEM lane quarter w % 4 of the
-//                accumulator buffer the tile used, eight of its sixteen
-//                16-column chunks, applies the r^2 epilogue (gemm_cpu.c:343-404) and
+//                accumulator buffer the tile used, every other one of its
+//                fifteen 16-column chunks, applies the r^2 epilogue (gemm_cpu.c:343-404) and
 //                stores; they arrive on rank 0's "accumulator empty" barrier.
 // Every wait is bounded.  No thread returns early: both CTAs meet at the
 // cluster barriers at start and end on every path, including after a
@@ -62,10 +62,9 @@ constexpr int UB_BYTES = HN * 128;       // 15 KB
 constexpr int UNPACK_WARPS = 10, EPI_WARPS = 8;
 constexpr int FIRST_UNPACK_WARP = 2;
 constexpr int FIRST_EPI_WARP = FIRST_UNPACK_WARP + UNPACK_WARPS;
-constexpr int UNPACKERS = UNPACK_WARPS * 32;
 constexpr int EPILOGUE = EPI_WARPS * 32;
 constexpr int THREADS = (FIRST_EPI_WARP + EPI_WARPS) * 32;   // 640
-constexpr int GROUP_THREADS = UNPACKERS / 2;                 // unpackers per stage
+constexpr int GROUP_THREADS = UNPACK_WARPS * 32 / 2;         // unpackers per stage
 constexpr int NTASK = HM + HN;                               // row tasks
 constexpr int TASKS = (NTASK + GROUP_THREADS - 1) / GROUP_THREADS;
 constexpr uint32_t TMEM_COLS = 512;
@@ -275,7 +274,7 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         const int et = tid - FIRST_EPI_WARP * 32;
         const int ew = warp - FIRST_EPI_WARP;
         const int q = warp & 3;                 // TMEM lane quarter
-        const int colh = ew >> 2;               // chunks colh, colh + 2, colh + 4, colh + 6
+        const int colh = ew >> 2;               // chunks colh, colh + 2, ... (< 15)
         bool failed = false;
         int cur_t = 0, cur_base = 0;
         for (int it = 0; it < my_tiles; ++it) {
@@ -308,12 +307,11 @@ k_ld_mxf4_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 const epi::ARowF raf = epi::make_arow_f32(ca, p.S);
                 const uint32_t tbase =
                     tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)ab * ACC_STRIDE;
-                // columns past the tile's 240 B rows are read but not written
                 const int n_tile = tb * BN + BN < p.n ? tb * BN + BN : p.n;
                 // 16-column chunks: fewer live registers than 32 (2.41 / 2.66 ms
-                // against 2.43 / 2.75 ms, exact / reference r^2)
+                // against 2.43 / 2.75 ms, exact / reference r^2), the tile's 15
 #pragma unroll 1
-                for (int c = colh; c < 16; c += 2) {
+                for (int c = colh; c < BN / 16; c += 2) {
                     uint32_t v[16];
                     __syncwarp();
                     tc_ld_32x32b_x16(tbase + (uint32_t)(c * 16), v);
