@@ -258,8 +258,8 @@ const KernelShape &mma_shape(qld_ctx *c, const Task &t, int b0, int b1) {
 // The 4-bit kernel on SM pairs or single SMs (same 256 x 240 tiles).  The
 // pair kernel overlaps each tile's epilogue with the next tile's MMAs and
 // finishes a tile on two SMs in half the time: the faster one in both r^2
-// modes (a single region of 29,817 SNPs x 16,622 samples: 2.49 against
-// 3.16 ms exact, 2.82 against 4.14 ms reference).
+// modes (a single region of 29,817 SNPs x 16,622 samples: 2.40 against
+// 3.16 ms exact, 2.63 against 4.14 ms reference).
 const KernelShape &fp4_shape(qld_ctx *c, const Task &t, int b0, int b1) {
     (void)b0; (void)b1;
     if (c->sm_pair == 0)
