@@ -24,10 +24,11 @@
 // the slot on rank 0's barrier when done with its item.  A ticket past the
 // last item pushes an end marker.
 //
-// Roles per CTA (576 threads): warp 0 queue (rank 0) and TMA of the CTA's
-// rows, warp 1 TMEM and (rank 0) the MMAs, warps 2-9 unpack in two groups
-// taking alternate 256-sample stages (each thread whole rows), warps 10-17
-// epilogue (two per TMEM lane quarter).  TMEM: two 240-column accumulators
+// Roles per CTA (576 threads in R2_EXACT, 704 in R2_REFERENCE): warp 0 queue
+// (rank 0) and TMA of the CTA's rows, warp 1 TMEM and (rank 0) the MMAs,
+// warps 2-9 unpack in two groups taking alternate 256-sample stages (each
+// thread whole rows), warps 10-17 (10-21) epilogue, two (three) per TMEM lane
+// quarter.  TMEM: two 240-column accumulators
 // (columns 0 and 256), so a tile's epilogue overlaps the next tile's MMAs,
 // and the scale factors at columns 496-511.  Every wait is bounded and no
 // thread returns early: both CTAs meet at the cluster barriers at start and
@@ -55,11 +56,8 @@ constexpr int UA_BYTES = HM * 128;          // 16 KB: 256 E2M1 per row
 constexpr int UB_BYTES = HN * 128;          // 15 KB
 constexpr int UNPACK_WARPS = 8;
 constexpr int GROUP_THREADS = UNPACK_WARPS * 32 / 2;
-constexpr int EPI_WARPS = 8;
-constexpr int EPI_THREADS = EPI_WARPS * 32;
 constexpr int FIRST_UNPACK_WARP = 2;
 constexpr int FIRST_EPI_WARP = FIRST_UNPACK_WARP + UNPACK_WARPS;
-constexpr int THREADS = (FIRST_EPI_WARP + EPI_WARPS) * 32;   // 576
 constexpr int NROWS = HM + HN;                                // row tasks per stage
 constexpr int TASKS = (NROWS + GROUP_THREADS - 1) / GROUP_THREADS;
 constexpr uint32_t TMEM_COLS = 512;
@@ -72,7 +70,19 @@ constexpr uint16_t BOTH = 0x3;                               // CTA mask of a co
 constexpr int QSLOTS = 4;                                    // item ring depth
 // arrivals on rank 0's slot-free barrier per item: rank 0's MMA thread,
 // unpack and epilogue warps; rank 1's TMA thread, unpack and epilogue warps
-constexpr int ITEM_USERS = 2 * (1 + UNPACK_WARPS + EPI_WARPS);
+// Epilogue warps per r^2 mode: eight in R2_EXACT, twelve in R2_REFERENCE,
+// whose longer per-pair sequence leaves items below ~6,000 samples waiting
+// on their epilogue (4,096-task mix, reference mode: 87.7 against 95.0 ms;
+// exact mode with twelve: 72.1 against 69.2 ms, its 32-column chunks spill
+// at the 80 registers 704 threads leave).
+template <int MODE>
+struct Roles {
+    static constexpr int EPI_WARPS = MODE == R2_REFERENCE ? 12 : 8;
+    static constexpr int EPI_THREADS = EPI_WARPS * 32;
+    static constexpr int THREADS = (FIRST_EPI_WARP + EPI_WARPS) * 32;   // 576 or 704
+    static constexpr int ITEM_USERS = 2 * (1 + UNPACK_WARPS + EPI_WARPS);
+    static_assert(EPI_WARPS % 4 == 0 && EPI_THREADS >= COLS_N, "epilogue split");
+};
 
 // Shared-memory layout per r^2 mode: R2_EXACT needs 8 bytes of column
 // factors per column (epi::ColsF), R2_REFERENCE 16 (epi::ColsR); both leave
@@ -97,7 +107,7 @@ struct Smem {
                   "swizzled stages must start on 1024-byte boundaries");
 };
 static_assert(ACC_STRIDE + BN <= SF_COL && SF_COL + 16 <= TMEM_COLS, "TMEM map");
-static_assert(TASKS == 2 && SUB == 2 && UST % 2 == 0 && EPI_THREADS == COLS_N, "work split");
+static_assert(TASKS == 2 && SUB == 2 && UST % 2 == 0, "work split");
 
 struct Item {
     int job, ta, tb, np;   // job < 0: end of the queue
@@ -123,9 +133,10 @@ __device__ __forceinline__ Item decode_item(const BatchJob *jobs, int njobs, lon
 }
 
 template <int MODE>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Roles<MODE>::THREADS, 1)
 k_ld_batch(const BatchParams bp) {
     using L = Smem<MODE>;
+    using R = Roles<MODE>;
     constexpr int PST = L::PST;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -166,12 +177,12 @@ k_ld_batch(const BatchParams bp) {
         }
         for (int s = 0; s < 2; ++s) {
             mbar_init(smem_u32(&accfull[s]), 1);
-            mbar_init(smem_u32(&accempty[s]), 2 * EPI_WARPS);   // both CTAs' epilogues
+            mbar_init(smem_u32(&accempty[s]), 2 * R::EPI_WARPS);   // both CTAs' epilogues
         }
         mbar_init(smem_u32(mma_done), 1);
         for (int s = 0; s < QSLOTS; ++s) {
             mbar_init(smem_u32(&ifull[s]), 1);
-            mbar_init(smem_u32(&iempty[s]), ITEM_USERS);
+            mbar_init(smem_u32(&iempty[s]), R::ITEM_USERS);
         }
         fence_barrier_init();
     }
@@ -354,9 +365,9 @@ k_ld_batch(const BatchParams bp) {
         const int et = tid - FIRST_EPI_WARP * 32;
         const int ew = warp - FIRST_EPI_WARP;
         const int q = warp & 3;             // TMEM lane quarter
-        const int colh = ew >> 2;           // chunks colh, colh + 2, ...
+        const int colh = ew >> 2;           // chunks colh, colh + EPI_WARPS / 4, ...
         if (et == 0) *epi_fail = 0;
-        named_bar_sync(1, EPI_THREADS);
+        named_bar_sync(1, R::EPI_THREADS);
         for (int qi = 0;; ++qi) {
             const bool got_item = wait_item(qi);
             if (!__all_sync(0xffffffffu, got_item) && lane == 0) {
@@ -364,11 +375,11 @@ k_ld_batch(const BatchParams bp) {
                 *epi_fail = 1;
             }
             const Item it = items[qi % QSLOTS];
-            named_bar_sync(1, EPI_THREADS);
+            named_bar_sync(1, R::EPI_THREADS);
             if (*epi_fail || it.job < 0) break;
             const BatchJob &J = bp.jobs[it.job];
             const int ab = qi & 1;
-            {   // every column factor the chunks read; 0 past the tile and the task
+            if (et < COLS_N) {   // every column factor the chunks read; 0 past the tile and the task
                 const int b = it.tb * BN + et;
                 const uint32_t cb = (et < BN && b < J.n) ? J.bcB[b] : 0u;
                 if constexpr (MODE == R2_EXACT)
@@ -376,7 +387,7 @@ k_ld_batch(const BatchParams bp) {
                 else
                     epi::store_col_ref(colsr, et, cb, J.S);
             }
-            named_bar_sync(1, EPI_THREADS);
+            named_bar_sync(1, R::EPI_THREADS);
             bool ready = mbar_wait(smem_u32(&accfull[ab]), (qi >> 1) & 1, limit, bp.status);
             ready = __all_sync(0xffffffffu, ready);
             if (!ready) {
@@ -404,7 +415,7 @@ k_ld_batch(const BatchParams bp) {
                 // 199 ms on the 4,096-task mix; exact mode: 70.5 against 71.7 ms)
                 constexpr int CW = MODE == R2_EXACT ? 32 : 16;
 #pragma unroll 1
-                for (int c = colh; c < (BN + CW - 1) / CW; c += 2) {   // the tile's chunks
+                for (int c = colh; c < (BN + CW - 1) / CW; c += R::EPI_WARPS / 4) {   // the tile's chunks
                     uint32_t v[CW];
                     __syncwarp();
                     tc_ld_32x32b<CW>(tbase + (uint32_t)(c * CW), v);
@@ -429,7 +440,7 @@ k_ld_batch(const BatchParams bp) {
             }
             __syncwarp();
             if (lane == 0) release_item(qi);
-            named_bar_sync(1, EPI_THREADS);   // column factors may be rewritten
+            named_bar_sync(1, R::EPI_THREADS);   // column factors may be rewritten
         }
     }
 
@@ -467,7 +478,7 @@ cudaError_t launch_mode(const BatchParams &bp, int max_ctas, cudaStream_t st) {
             return e;
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(2 * (sms / 2), 1, 1);
-        cfg.blockDim = dim3(THREADS, 1, 1);
+        cfg.blockDim = dim3(Roles<MODE>::THREADS, 1, 1);
         cfg.dynamicSmemBytes = Smem<MODE>::BYTES;
         int n = 0;
         if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess || n <= 0) {
@@ -479,7 +490,7 @@ cudaError_t launch_mode(const BatchParams &bp, int max_ctas, cudaStream_t st) {
     long long pairs = bp.nitems < g_max_pairs ? bp.nitems : g_max_pairs;
     if (max_ctas > 0 && 2 * pairs > max_ctas) pairs = max_ctas / 2;
     if (pairs <= 0) return cudaSuccess;
-    kern<<<(int)(2 * pairs), THREADS, Smem<MODE>::BYTES, st>>>(bp);
+    kern<<<(int)(2 * pairs), Roles<MODE>::THREADS, Smem<MODE>::BYTES, st>>>(bp);
     return cudaGetLastError();
 }
 
